@@ -1,0 +1,179 @@
+/*
+ * corrct_b200 — C ABI of the B200 (sm_100a) attenuation-corrected XRF projection path.
+ *
+ * Every entry point takes plain device pointers, sizes, and a CUDA stream handle
+ * (a cudaStream_t passed as void*; NULL = legacy default stream).  The caller owns
+ * every buffer; the library never allocates or frees device memory on these paths
+ * (scratch space is passed in as a workspace).  Calls are stream-ordered, return an
+ * int status (CCT_OK = 0), and keep no hidden state other than the thread-local
+ * message returned by cct_last_error().
+ *
+ * Layouts (row-major, C order, n = volume side = detector width):
+ *   volume     [S][n][n]            float32
+ *   sinogram   [S][D][A][n]         float32   (S slices, D detectors, A angles)
+ *   maps       [S][A][D][n][n]      float32 or bfloat16
+ * which per slice are the reference's own shapes: volume (n, n) and sinogram
+ * (n_det, A, n) (corrct: src/corrct/projectors.py:591-594), maps (A, n_det, n, n)
+ * (corrct: src/corrct/physics/attenuation.py:134).
+ */
+#ifndef CORRCT_B200_H
+#define CORRCT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CCT_ABI_VERSION 1
+
+/* Status codes. */
+#define CCT_OK 0
+#define CCT_ERR_VALUE 1       /* bad shape, geometry or argument (Python: ValueError) */
+#define CCT_ERR_CUDA 2        /* CUDA runtime error (Python: RuntimeError) */
+#define CCT_ERR_UNSUPPORTED 3 /* valid but unsupported combination (Python: NotImplementedError) */
+
+/* Map storage types. */
+#define CCT_DTYPE_F32 0
+#define CCT_DTYPE_BF16 1
+
+/* Back-projection modes. */
+#define CCT_BP_REFERENCE 0 /* scikit-image iradon discretisation, no maps, no weights
+                              (corrct: src/corrct/projectors.py:619-622, _projector_backends.py:335-359) */
+#define CCT_BP_SYMMETRIC 1 /* iradon discretisation x weights x maps
+                              (corrct: src/corrct/projectors.py:533-568, 608-618) */
+#define CCT_BP_ADJOINT 2   /* exact transpose of cct_fp (no reference counterpart) */
+
+/* Geometry of a batch of slices that share n, the angles and the detectors. */
+typedef struct cct_xrf_desc {
+  int32_t n;          /* square volume side and detector width in pixels (>= 2) */
+  int32_t n_angles;   /* A >= 1 */
+  int32_t n_det;      /* D >= 1 fluorescence detectors (maps per angle) */
+  int32_t n_slices;   /* S >= 1 */
+  int32_t maps_dtype; /* CCT_DTYPE_F32 or CCT_DTYPE_BF16 */
+  int32_t reserved;
+  const float* fp_matrix; /* device [A][6]: per-angle inverse map of scikit-image radon,
+                             (M00, M01, M02, M10, M11, M12): col_in = M00*c + M01*r + M02,
+                             row_in = M10*c + M11*r + M12, entries as radon builds them in float32 */
+  const float* bp_trig;   /* device [A][2]: (cos, sin) of each angle as iradon evaluates them (float32) */
+  const float* weights;   /* device [A][D]: w_det[d] * w_angle[a][d], or NULL for all ones */
+} cct_xrf_desc;
+
+/* Library identity. */
+int cct_abi_version(void);
+const char* cct_last_error(void);
+
+/* Kernels never trap: an internal bound that valid inputs cannot exceed raises a device flag
+   instead.  *value = the flag (0 = clean); clear != 0 resets it.  Synchronous. */
+int cct_device_error(int32_t clear, int32_t* value);
+
+/*
+ * Forward projection.  maps == NULL: uncorrected projection (D must be 1), the
+ * scikit-image backend's fp (corrct: src/corrct/_projector_backends.py:312-333).
+ * maps != NULL: attenuated projection sino[s][d][a] = w[a][d] * radon_a(vol[s] * maps[s][a][d])
+ * (corrct: src/corrct/projectors.py:502-531, 570-596).
+ */
+int cct_fp(const cct_xrf_desc* desc, const float* vol, const void* maps, float* sino, void* stream);
+
+/*
+ * Back projection, mode = CCT_BP_*.  Replaces ProjectorAttenuationXRF.bp / bp_angle
+ * (corrct: src/corrct/projectors.py:533-568, 598-622) and ProjectorBackendSKimage.bp
+ * (corrct: src/corrct/_projector_backends.py:335-359).  maps may be NULL for
+ * CCT_BP_REFERENCE and CCT_BP_ADJOINT (uncorrected transpose).
+ */
+int cct_bp(const cct_xrf_desc* desc, int32_t mode, const float* sino, const void* maps, float* vol,
+           void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Attenuation maps: maps[s][a][d] = exp(-L_in(theta_a)) * mean_k exp(-L_out(theta_a + phi_d + s_k)),
+ * with L the reference's pad / rotate / half-voxel cumulative sum / rotate-back line integral
+ * (corrct: src/corrct/_projector_backends.py:43-99, src/corrct/physics/attenuation.py:105-180).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct cct_maps_desc {
+  int32_t n;          /* volume side */
+  int32_t n_angles;   /* A */
+  int32_t n_det;      /* D */
+  int32_t n_slices;   /* S */
+  int32_t n_sub;      /* emitted sub-angles per detector (>= 1) */
+  int32_t maps_dtype; /* CCT_DTYPE_F32 or CCT_DTYPE_BF16 */
+  int32_t has_in;     /* incident attenuation present */
+  int32_t has_out;    /* emitted attenuation present */
+  const double* rot_in;  /* device [A][2][6]: scikit-image rotate inverse maps of the padded image,
+                            [0] = rotate(-phi), [1] = rotate(+phi), same entry order as fp_matrix */
+  const double* rot_out; /* device [A][D][n_sub][2][6], emitted directions (phi includes + pi) */
+} cct_maps_desc;
+
+/* Workspace bytes needed to process `angles_per_pass` angles per pass (>= 1). */
+int cct_maps_workspace_size(const cct_maps_desc* desc, int32_t angles_per_pass, size_t* bytes);
+
+/* Compute maps.  mu_in / mu_out: device [S][n][n] float32 (NULL when absent).  The number of
+   angles per pass is the largest that fits in workspace_bytes. */
+int cct_compute_maps(const cct_maps_desc* desc, const float* mu_in, const float* mu_out, void* maps,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Device-resident solver steps for a batch of slices (update equations of corrct's MLEM,
+ * SIRT and PDHG: src/corrct/solvers.py:688-805, 867-984, 1060-1206).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct cct_solver_state {
+  float* x;              /* [S][n][n] iterate, updated in place */
+  float* x_relax;        /* [S][n][n] PDHG over-relaxed iterate (NULL otherwise) */
+  const float* b;        /* [S][D][A][n] data */
+  const float* tau;      /* [S][n][n], or [n][n] when tau_shared (MLEM: A^T 1; SIRT/PDHG: scaling) */
+  const float* sigma;    /* [S][D][A][n] SIRT/PDHG data-space scaling, NULL for MLEM */
+  float* sino_buf;       /* [S][D][A][n] workspace (MLEM ratio, SIRT residual, PDHG dual) */
+  float* vol_buf;        /* [S][n][n] workspace */
+  float* tv_dual;        /* [S][2][n][n] PDHG TV dual (NULL otherwise) */
+  double* partials;      /* workspace, cct_solver_partials_count() doubles */
+  double* residuals;     /* [S] residual norm of the last evaluated iterate */
+  int32_t* active;       /* [S] 1 while a slice iterates, 0 once it met its tolerance */
+  int32_t* iterations;   /* [S] iterations performed (counted like SolutionInfo.iterations) */
+  const double* tolerance; /* [S] stop when tolerance > residual; NULL = never stop early */
+  const float* x_mask;   /* [n][n] solution mask shared by all slices, or NULL */
+  float lower_limit;
+  float upper_limit;
+  int32_t has_lower;
+  int32_t has_upper;
+  float background;      /* data background added to A x (0 with has_background = 0) */
+  int32_t has_background;
+  float tv_lambda;       /* PDHG isotropic TV weight */
+  int32_t tau_shared;
+  double* residual_history; /* [S][history_len] residual of every iteration (SolutionInfo.residuals), or NULL */
+  int32_t history_len;
+} cct_solver_state;
+
+/* Number of doubles the `partials` workspace must hold. */
+int cct_solver_partials_count(const cct_xrf_desc* desc, int64_t* count);
+
+/* One MLEM iteration with the KL residual stopping test (corrct: src/corrct/solvers.py:777-803).
+   Equivalent to cct_mlem_fp followed by cct_mlem_update. */
+int cct_mlem_step(const cct_xrf_desc* desc, const void* maps, cct_solver_state* st, void* stream);
+
+/* First half of an MLEM iteration: attenuated fp of x with the fused epilogue
+   ratio = b / max(Ax + bg, eps) into sino_buf, the FP64 KL residual, the iteration count and
+   the stopping test (corrct: src/corrct/solvers.py:779-796). */
+int cct_mlem_fp(const cct_xrf_desc* desc, const void* maps, cct_solver_state* st, void* stream);
+
+/* Second half: x *= A^T(ratio) / tau, clip, mask, for slices still active
+   (corrct: src/corrct/solvers.py:798-803). */
+int cct_mlem_update(const cct_xrf_desc* desc, cct_solver_state* st, void* stream);
+
+/* One SIRT iteration with the l2 residual (corrct: src/corrct/solvers.py:951-982). */
+int cct_sirt_step(const cct_xrf_desc* desc, const void* maps, int32_t bp_mode, cct_solver_state* st,
+                  void* stream);
+
+/* One PDHG iteration, KL data term + isotropic TV2D (corrct: src/corrct/solvers.py:1165-1206). */
+int cct_pdhg_step(const cct_xrf_desc* desc, const void* maps, int32_t bp_mode, cct_solver_state* st,
+                  void* stream);
+
+/* Norms in FP64 per slice: out[s] = sum |v| (ord 1) or sum v^2 (ord 2) over `count` elements of
+   slice s of v (slices `count` apart).  Replaces np.linalg.norm on solver arrays. */
+int cct_reduce_norm(const float* v, int64_t count, int32_t n_slices, int32_t ord, double* out,
+                    double* partials, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CORRCT_B200_H */

@@ -1,0 +1,428 @@
+"""Standalone numpy port of the reference's attenuation-corrected XRF projection path.
+
+TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).  Every function names the
+reference ``file:line`` (paths inside the ``corrct`` project) whose behaviour it
+restates.  The scikit-image primitives come from ``oracle.skimage_restated``.
+All arithmetic follows the dtype of the inputs: float64 inputs give the FP64
+oracle; float32 inputs reproduce the reference's default float32 run.
+
+This module is checked against golden fixtures produced by the reference's own
+Python (``tests/golden/make_golden.py``); it is what the GPU parity tests
+compare against at sizes beyond the fixtures, and what the CPU-baseline legs of
+``bench.py`` time.
+"""
+
+from __future__ import annotations
+
+import concurrent.futures as cf
+from collections.abc import Sequence
+
+import numpy as np
+from numpy.typing import NDArray
+
+from . import skimage_restated as skr
+
+EPS32 = np.finfo(np.float32).eps  # solvers.py:20, data_terms.py:19
+
+
+# --------------------------------------------------------------------------------------
+# Geometry helpers
+# --------------------------------------------------------------------------------------
+
+
+def backend_angles(angles_rot_rad: Sequence[float] | NDArray) -> tuple[NDArray, NDArray]:
+    """Backend angles: float32 radians and float32 degrees.
+
+    ``_projector_backends.py:148`` casts the angles to float32 and
+    ``_projector_backends.py:299`` converts them with ``np.rad2deg``.
+    """
+    rad = np.array(angles_rot_rad, ndmin=1, dtype=np.float32)
+    return rad, np.rad2deg(rad)
+
+
+def padded_size(n: int) -> tuple[int, int]:
+    """Padding of ``compute_attenuation``: returns (edge, padded size) (``_projector_backends.py:75-77``)."""
+    min_size = np.ceil(np.sqrt(2.0 * n * n))
+    edge = int(np.ceil((min_size - n) / 2))
+    return edge, n + 2 * edge
+
+
+# --------------------------------------------------------------------------------------
+# Attenuation maps
+# --------------------------------------------------------------------------------------
+
+
+def compute_attenuation(vol: NDArray, angle_rad: float, invert: bool = False) -> NDArray:
+    """exp(-line integral) map of one 2-D slice for one direction.
+
+    Restates ``_projector_backends.py:43-99``: zero-pad to the diagonal
+    (``:62-65, 75-77, 83``), rotate by ``-angle`` (``:68``), add the rolled copy
+    and cumulate half of it along rows (``:70-71``), rotate back (``:73``), crop
+    (``:95``) and exponentiate (``:97``).  ``invert`` adds pi (``:79-80``).
+    """
+    n = vol.shape[-1]
+    edge, _ = padded_size(n)
+    if invert:
+        angle_rad += np.pi
+    rot_angle_deg = np.rad2deg(angle_rad)
+    cum = np.pad(vol, ((edge, edge), (edge, edge)), mode="constant")
+    cum = skr.rotate(cum, -rot_angle_deg, order=1, clip=False)
+    cum += np.roll(cum, 1, axis=-2)
+    cum = np.cumsum(cum / 2, axis=-2)
+    cum = skr.rotate(cum, rot_angle_deg, order=1, clip=False)
+    cum = cum[edge:-edge, edge:-edge]
+    return np.exp(-cum)
+
+
+def detector_sub_angles(surface_mm2: float, distance_mm: float, sub_sampling: int) -> NDArray:
+    """Sub-angle offsets of a finite detector (``physics/xrf.py:243-258``, ``attenuation.py:111-114``)."""
+    if surface_mm2 > 0.0:
+        half_edge = np.sqrt(surface_mm2) / 2
+        half_angle = np.arctan2(half_edge, distance_mm)
+        sub = np.linspace(-half_angle, half_angle, sub_sampling + 1)
+        return np.convolve(sub, np.ones(2), "valid") / 2
+    return np.zeros(1)
+
+
+def compute_maps(
+    mu_in: NDArray | None,
+    mu_out: NDArray | None,
+    angles_rot_rad: NDArray,
+    angles_det_rad: Sequence[float] | NDArray = (np.pi / 2,),
+    dtype=np.float64,
+    detector_surfaces_mm2: Sequence[float] | None = None,
+    detector_distances_mm: Sequence[float] | None = None,
+    emitted_sub_sampling: int = 1,
+    workers: int = 1,
+) -> NDArray:
+    """Attenuation maps ``(A, D, N, N)`` = exp(-L_in) * mean_s exp(-L_out).
+
+    Restates ``AttenuationVolume.compute_maps`` (``physics/attenuation.py:122-180``)
+    with ``_compute_attenuation_angle_in`` (``:105-106``) and
+    ``_compute_attenuation_angle_out`` (``:108-120``).  ``angles_rot_rad`` are the
+    (float32) backend angles the projector passes in (``projectors.py:462``).
+    ``workers > 1`` spreads angles over a thread pool like the reference
+    (``attenuation.py:139-158``); results do not depend on it.
+    """
+    angles_rot_rad = np.array(angles_rot_rad, ndmin=1)
+    det_angles = np.array(angles_det_rad, ndmin=1, dtype=np.float64)
+    n_det = len(det_angles)
+    surfaces = np.zeros(n_det) if detector_surfaces_mm2 is None else np.array(detector_surfaces_mm2, ndmin=1)
+    distances = np.ones(n_det) if detector_distances_mm is None else np.array(detector_distances_mm, ndmin=1)
+    ref = mu_in if mu_in is not None else mu_out
+    if ref is None:
+        raise ValueError("No attenuation volumes were given.")
+    n_ang = len(angles_rot_rad)
+    maps = np.ones([n_ang, n_det, *ref.shape], dtype=dtype)
+
+    def one_angle(ii: int) -> None:
+        a = angles_rot_rad[ii]
+        if mu_in is not None:
+            maps[ii] *= compute_attenuation(mu_in, a, invert=False)[None, ...]
+        if mu_out is not None:
+            angle_det = a + det_angles
+            atts = np.zeros(maps.shape[1:], dtype=dtype)
+            for dd, ad in enumerate(angle_det):
+                subs = detector_sub_angles(surfaces[dd], distances[dd], emitted_sub_sampling)
+                for a_s in subs:
+                    atts[dd] += compute_attenuation(mu_out, ad + a_s, invert=True)
+                atts[dd] /= len(subs)
+            maps[ii] *= atts
+
+    if workers > 1:
+        with cf.ThreadPoolExecutor(max_workers=workers) as ex:
+            list(ex.map(one_angle, range(n_ang)))
+    else:
+        for ii in range(n_ang):
+            one_angle(ii)
+    return maps
+
+
+# --------------------------------------------------------------------------------------
+# Projections
+# --------------------------------------------------------------------------------------
+
+
+def fp_angle(vol: NDArray, angle_deg32: np.floating) -> NDArray:
+    """One sinogram line: ``skt.radon(vol, [deg])`` squeezed (``_projector_backends.py:333``)."""
+    return np.squeeze(skr.radon(vol, np.asarray([angle_deg32])))
+
+
+def bp_angle(line: NDArray, angle_deg32: np.floating, n: int) -> NDArray:
+    """One-line back projection ``iradon(...)*2/pi`` (``_projector_backends.py:358-359``)."""
+    vol = skr.iradon(line[:, np.newaxis], np.asarray([angle_deg32]), output_size=n, filter_name=None, circle=False)
+    return vol * 2 / np.pi
+
+
+def fp_uncorrected(vol: NDArray, angles_deg32: NDArray, workers: int = 1) -> NDArray:
+    """Sinogram ``(A, N)`` of ``ProjectorBackendSKimage.fp`` (``_projector_backends.py:326-331``)."""
+    out = np.empty((len(angles_deg32), vol.shape[-1]), dtype=vol.dtype)
+
+    def one(ii: int) -> None:
+        out[ii] = fp_angle(vol, angles_deg32[ii])
+
+    _run(one, len(angles_deg32), workers)
+    return out
+
+
+def bp_uncorrected(sino: NDArray, angles_deg32: NDArray, n: int, workers: int = 1) -> NDArray:
+    """Volume ``(N, N)`` of ``ProjectorBackendSKimage.bp`` (``_projector_backends.py:352-359``)."""
+    parts = np.empty((len(angles_deg32), n, n), dtype=sino.dtype)
+
+    def one(ii: int) -> None:
+        parts[ii] = skr.iradon(
+            sino[ii, :, np.newaxis], np.asarray([angles_deg32[ii]]), output_size=n, filter_name=None, circle=False
+        )
+
+    _run(one, len(angles_deg32), workers)
+    return parts.sum(axis=0) * 2 / np.pi
+
+
+def _run(func, count: int, workers: int) -> None:
+    if workers > 1:
+        with cf.ThreadPoolExecutor(max_workers=workers) as ex:
+            list(ex.map(func, range(count)))
+    else:
+        for ii in range(count):
+            func(ii)
+
+
+def _weights(n_ang: int, n_det: int, weights_det, weights_angles) -> NDArray:
+    """Per (angle, detector) weight ``w_det[d] * w_ang[a, d]`` (``projectors.py:439-459, 516``)."""
+    wd = np.ones(n_det) if weights_det is None else np.array(weights_det, ndmin=1, dtype=np.float64)
+    if n_det > 1 and len(wd) == 1:
+        wd = np.tile(wd, [n_det])
+    wa = np.ones((n_ang, n_det)) if weights_angles is None else np.array(weights_angles)
+    return wd[None, :] * wa
+
+
+def fp_xrf(
+    vol: NDArray,
+    maps: NDArray,
+    angles_deg32: NDArray,
+    weights_det=None,
+    weights_angles=None,
+    workers: int = 1,
+) -> NDArray:
+    """Attenuated forward projection (``ProjectorAttenuationXRF.fp``, ``projectors.py:502-531, 570-596``).
+
+    Returns ``(D, A, N)``, squeezed to ``(A, N)`` for a single detector.
+    """
+    n_ang, n_det = maps.shape[:2]
+    w = _weights(n_ang, n_det, weights_det, weights_angles)
+    out = np.empty((n_det, n_ang, vol.shape[-1]), dtype=np.result_type(vol, maps))
+
+    def one(ii: int) -> None:
+        temp = vol * maps[ii]
+        for dd in range(n_det):
+            out[dd, ii] = w[ii, dd] * fp_angle(temp[dd], angles_deg32[ii])
+
+    _run(one, n_ang, workers)
+    return out[0] if n_det == 1 else out
+
+
+def bp_xrf(
+    sino: NDArray,
+    maps: NDArray,
+    angles_deg32: NDArray,
+    weights_det=None,
+    weights_angles=None,
+    is_symmetric: bool = False,
+    workers: int = 1,
+) -> NDArray:
+    """Back projection of ``ProjectorAttenuationXRF.bp`` (``projectors.py:533-568, 598-622``).
+
+    Default (``is_symmetric=False``): plain per-detector back projections summed,
+    with neither maps nor weights (``:619-622``).  Symmetric: per angle, weighted
+    per-detector back projections multiplied by the maps (``:553-568``).
+    """
+    n_ang, n_det = maps.shape[:2]
+    n = maps.shape[-1]
+    sino = np.reshape(sino, [n_det, n_ang, -1])
+    if not is_symmetric:
+        return np.sum(np.stack([bp_uncorrected(sino[d], angles_deg32, n, workers) for d in range(n_det)]), axis=0)
+    w = _weights(n_ang, n_det, weights_det, weights_angles)
+    parts = np.empty((n_ang, n, n), dtype=np.result_type(sino, maps))
+
+    def one(ii: int) -> None:
+        acc = np.stack([w[ii, d] * bp_angle(sino[d, ii], angles_deg32[ii], n) for d in range(n_det)])
+        acc *= maps[ii]
+        parts[ii] = acc.sum(axis=0)
+
+    _run(one, n_ang, workers)
+    return parts.sum(axis=0)
+
+
+def fp_xrf_adjoint(
+    sino: NDArray, maps: NDArray | None, angles_deg32: NDArray, n: int, weights_det=None, weights_angles=None
+) -> NDArray:
+    """Exact transpose of ``fp_xrf`` (scatter of every bilinear tap).
+
+    No reference counterpart: the reference's back projection is the unmatched
+    ``iradon`` discretisation.  This is the definition the GPU ``adjoint`` mode is
+    tested against.  ``maps=None`` gives the transpose of the uncorrected fp.
+    """
+    n_ang = len(angles_deg32)
+    n_det = 1 if maps is None else maps.shape[1]
+    sino = np.reshape(sino, [n_det, n_ang, n])
+    w = _weights(n_ang, n_det, weights_det, weights_angles)
+    out = np.zeros((n, n), dtype=np.float64)
+    rr, cc = np.mgrid[:n, :n]
+    for ii in range(n_ang):
+        m = skr.radon_matrix(angles_deg32[ii], n).astype(np.float64)
+        cols_in = m[0, 0] * cc + m[0, 1] * rr + m[0, 2]
+        rows_in = m[1, 0] * cc + m[1, 1] * rr + m[1, 2]
+        r0, c0 = np.floor(rows_in), np.floor(cols_in)
+        r1, c1 = np.ceil(rows_in), np.ceil(cols_in)
+        dr, dc = rows_in - r0, cols_in - c0
+        for dd in range(n_det):
+            vals = np.broadcast_to(sino[dd, ii][None, :] * w[ii, dd], (n, n))
+            acc = np.zeros((n, n))
+            for rt, ct, wt in (
+                (r0, c0, (1 - dr) * (1 - dc)),
+                (r0, c1, (1 - dr) * dc),
+                (r1, c0, dr * (1 - dc)),
+                (r1, c1, dr * dc),
+            ):
+                ri, ci = rt.astype(np.int64), ct.astype(np.int64)
+                ok = (ri >= 0) & (ri < n) & (ci >= 0) & (ci < n)
+                np.add.at(acc, (ri[ok], ci[ok]), (vals * wt)[ok])
+            out += acc if maps is None else acc * maps[ii, dd]
+    return out
+
+
+# --------------------------------------------------------------------------------------
+# Data terms, TV, solvers (update equations of solvers.py)
+# --------------------------------------------------------------------------------------
+
+
+def kl_residual(ax: NDArray, b: NDArray, sigma=1.0, background=None, mask=None) -> NDArray:
+    """``DataFidelity_KL.compute_residual`` with the proximal (``data_terms.py:720-739``)."""
+    proj = ax if background is None else ax + background
+    proj = np.fmax(proj, EPS32)
+    res = np.fmax(proj, EPS32) * sigma
+    sigma_data = 4 * sigma * np.fmax(b, 0.0)
+    res = (1 + res - np.sqrt((res - 1) ** 2 + sigma_data)) / 2
+    if mask is not None:
+        res = res * mask
+    return -res
+
+
+def kl_residual_norm(res: NDArray) -> float:
+    """l1 norm of the KL residual (``data_terms.py:741-742``)."""
+    return float(np.linalg.norm(res.flatten(), ord=1))
+
+
+def l2_residual(ax: NDArray, b: NDArray, background=None, mask=None) -> NDArray:
+    """``DataFidelityBase.compute_residual`` (``data_terms.py:136-161``)."""
+    proj = ax if background is None else ax + background
+    res = b - proj
+    if mask is not None:
+        res = res * mask
+    return res
+
+
+def gradient(x: NDArray) -> NDArray:
+    """``TransformGradient.gradient`` with edge padding (``operators.py:796-816``)."""
+    d = []
+    for ax in (-2, -1):
+        pad = [(0, 0)] * x.ndim
+        pad[ax] = (0, 1)
+        d.append(np.diff(np.pad(x, pad, mode="edge"), n=1, axis=ax))
+    return np.stack(d, axis=0)
+
+
+def divergence(q: NDArray) -> NDArray:
+    """``TransformGradient.divergence`` with edge padding (``operators.py:818-844``)."""
+    d = []
+    for ii, ax in enumerate((-2, -1)):
+        pad = [(0, 0)] * (q.ndim - 1)
+        pad[ax] = (1, 0)
+        d.append(np.diff(np.pad(q[ii], pad, mode="edge"), n=1, axis=ax))
+    return np.sum(np.stack(d, axis=0), axis=0)
+
+
+def diagonal_scaling(fp, bp, b: NDArray, x_shape, reg_tau: float = 0.0, relax_tau: float = 1.0, relax_sigma: float = 1.0):
+    """``compute_diagonal_scaling`` (``solvers.py:60-117``) for one TV regularizer contribution ``reg_tau``."""
+    tau = np.abs(bp(np.ones_like(b)))
+    tau = tau + reg_tau
+    tau[(tau / np.max(tau)) < 1e-5] = 1
+    tau = relax_tau / tau
+    sigma = np.abs(fp(np.ones(x_shape, dtype=tau.dtype)))
+    sigma[(sigma / np.max(sigma)) < 1e-5] = 1.0
+    sigma = relax_sigma / sigma
+    return sigma, tau
+
+
+def mlem(fp, bp, b: NDArray, iterations: int, x0=None, tolerance=None, lower_limit=None, upper_limit=None, x_mask=None):
+    """MLEM update loop of ``solvers.py:725-805`` (KL data term, no background).
+
+    Returns (x, residuals list).
+    """
+    b = np.array(b)
+    tau = bp(np.ones_like(b))
+    x = np.ones_like(tau) if x0 is None else np.array(x0).copy()
+    if x_mask is not None:
+        x *= x_mask
+    residuals = []
+    for _ in range(iterations):
+        ax = fp(x)
+        if tolerance is not None:
+            r = kl_residual_norm(kl_residual(ax, b))
+            residuals.append(r)
+            if tolerance > r:
+                break
+        ax = ax.clip(EPS32, None)
+        upd = bp(b / ax)
+        x *= upd / tau
+        if lower_limit is not None or upper_limit is not None:
+            x = x.clip(lower_limit, upper_limit)
+        if x_mask is not None:
+            x *= x_mask
+    return x, residuals
+
+
+def sirt(fp, bp, b: NDArray, iterations: int, x_shape, relaxation: float = 1.95, x0=None, lower_limit=None, upper_limit=None, x_mask=None):
+    """SIRT update loop of ``solvers.py:895-984`` (l2 data term, no regularizer)."""
+    sigma, tau = diagonal_scaling(fp, bp, b, x_shape, relax_tau=relaxation)
+    x = np.zeros_like(tau) if x0 is None else np.array(x0).copy()
+    for _ in range(iterations):
+        res = l2_residual(fp(x), b)
+        x += bp(res * sigma) * tau
+        if lower_limit is not None or upper_limit is not None:
+            x = x.clip(lower_limit, upper_limit)
+        if x_mask is not None:
+            x *= x_mask
+    return x
+
+
+def pdhg_kl_tv(fp, bp, b: NDArray, iterations: int, x_shape, lam: float, relaxation: float = 0.95, lower_limit=None, upper_limit=None, x_mask=None):
+    """PDHG with KL data term and isotropic TV2D (``solvers.py:1099-1206``).
+
+    Dual KL prox ``data_terms.py:682-692``; TV via ``Regularizer_Grad``
+    (``regularizers.py:260-273``, sigma = 0.5, tau contribution 2*ndims = 4) with
+    the l12 dual prox (``data_terms.py:549-555, 607-608``).
+    """
+    b = np.array(b)
+    sigma, tau = diagonal_scaling(fp, bp, b, x_shape, reg_tau=4.0, relax_tau=relaxation, relax_sigma=relaxation)
+    x = np.zeros(x_shape, dtype=tau.dtype)
+    x_relax = x.copy()
+    sigma_data = 4 * sigma * np.fmax(b, 0.0)
+    p = np.zeros_like(b)
+    q = np.zeros((2, *x_shape), dtype=tau.dtype)
+    for _ in range(iterations):
+        p += fp(x_relax) * sigma
+        p[:] = (1 + p - np.sqrt((p - 1) ** 2 + sigma_data)) / 2
+        q += 0.5 * gradient(x_relax)
+        qn = np.linalg.norm(q, ord=2, axis=0, keepdims=True)
+        q /= np.fmax(qn, lam)
+        q *= lam
+        upd = bp(p) - divergence(q)
+        x_new = x - upd * tau
+        if lower_limit is not None or upper_limit is not None:
+            x_new = x_new.clip(lower_limit, upper_limit)
+        if x_mask is not None:
+            x_new *= x_mask
+        x_relax = x_new + (x_new - x)
+        x = x_new
+    return x

@@ -1,0 +1,169 @@
+"""ctypes binding of ``libcorrct_b200.so`` (declared in ``include/corrct_b200.h``).
+
+The library is loaded lazily on first use.  There is no CPU fallback: a missing
+library or a missing CUDA device raises immediately.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcorrct_b200.so")
+
+CCT_OK = 0
+CCT_ERR_VALUE = 1
+CCT_ERR_CUDA = 2
+CCT_ERR_UNSUPPORTED = 3
+
+CCT_DTYPE_F32 = 0
+CCT_DTYPE_BF16 = 1
+
+CCT_BP_REFERENCE = 0
+CCT_BP_SYMMETRIC = 1
+CCT_BP_ADJOINT = 2
+
+c_float_p = ctypes.c_void_p  # device pointers are passed as integers
+
+
+class XrfDesc(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32),
+        ("n_angles", ctypes.c_int32),
+        ("n_det", ctypes.c_int32),
+        ("n_slices", ctypes.c_int32),
+        ("maps_dtype", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("fp_matrix", ctypes.c_void_p),
+        ("bp_trig", ctypes.c_void_p),
+        ("weights", ctypes.c_void_p),
+    ]
+
+
+class MapsDesc(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32),
+        ("n_angles", ctypes.c_int32),
+        ("n_det", ctypes.c_int32),
+        ("n_slices", ctypes.c_int32),
+        ("n_sub", ctypes.c_int32),
+        ("maps_dtype", ctypes.c_int32),
+        ("has_in", ctypes.c_int32),
+        ("has_out", ctypes.c_int32),
+        ("rot_in", ctypes.c_void_p),
+        ("rot_out", ctypes.c_void_p),
+    ]
+
+
+class SolverState(ctypes.Structure):
+    _fields_ = [
+        ("x", ctypes.c_void_p),
+        ("x_relax", ctypes.c_void_p),
+        ("b", ctypes.c_void_p),
+        ("tau", ctypes.c_void_p),
+        ("sigma", ctypes.c_void_p),
+        ("sino_buf", ctypes.c_void_p),
+        ("vol_buf", ctypes.c_void_p),
+        ("tv_dual", ctypes.c_void_p),
+        ("partials", ctypes.c_void_p),
+        ("residuals", ctypes.c_void_p),
+        ("active", ctypes.c_void_p),
+        ("iterations", ctypes.c_void_p),
+        ("tolerance", ctypes.c_void_p),
+        ("x_mask", ctypes.c_void_p),
+        ("lower_limit", ctypes.c_float),
+        ("upper_limit", ctypes.c_float),
+        ("has_lower", ctypes.c_int32),
+        ("has_upper", ctypes.c_int32),
+        ("background", ctypes.c_float),
+        ("has_background", ctypes.c_int32),
+        ("tv_lambda", ctypes.c_float),
+        ("tau_shared", ctypes.c_int32),
+        ("residual_history", ctypes.c_void_p),
+        ("history_len", ctypes.c_int32),
+    ]
+
+
+# name -> (restype, argtypes); every symbol declared in include/corrct_b200.h
+SIGNATURES = {
+    "cct_abi_version": (ctypes.c_int, []),
+    "cct_last_error": (ctypes.c_char_p, []),
+    "cct_device_error": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+    "cct_fp": (ctypes.c_int, [ctypes.POINTER(XrfDesc), c_float_p, c_float_p, c_float_p, ctypes.c_void_p]),
+    "cct_bp": (
+        ctypes.c_int,
+        [ctypes.POINTER(XrfDesc), ctypes.c_int32, c_float_p, c_float_p, c_float_p, ctypes.c_void_p],
+    ),
+    "cct_maps_workspace_size": (
+        ctypes.c_int,
+        [ctypes.POINTER(MapsDesc), ctypes.c_int32, ctypes.POINTER(ctypes.c_size_t)],
+    ),
+    "cct_compute_maps": (
+        ctypes.c_int,
+        [ctypes.POINTER(MapsDesc), c_float_p, c_float_p, c_float_p, c_float_p, ctypes.c_size_t, ctypes.c_void_p],
+    ),
+    "cct_solver_partials_count": (ctypes.c_int, [ctypes.POINTER(XrfDesc), ctypes.POINTER(ctypes.c_int64)]),
+    "cct_mlem_step": (
+        ctypes.c_int,
+        [ctypes.POINTER(XrfDesc), c_float_p, ctypes.POINTER(SolverState), ctypes.c_void_p],
+    ),
+    "cct_mlem_fp": (
+        ctypes.c_int,
+        [ctypes.POINTER(XrfDesc), c_float_p, ctypes.POINTER(SolverState), ctypes.c_void_p],
+    ),
+    "cct_mlem_update": (ctypes.c_int, [ctypes.POINTER(XrfDesc), ctypes.POINTER(SolverState), ctypes.c_void_p]),
+    "cct_sirt_step": (
+        ctypes.c_int,
+        [ctypes.POINTER(XrfDesc), c_float_p, ctypes.c_int32, ctypes.POINTER(SolverState), ctypes.c_void_p],
+    ),
+    "cct_pdhg_step": (
+        ctypes.c_int,
+        [ctypes.POINTER(XrfDesc), c_float_p, ctypes.c_int32, ctypes.POINTER(SolverState), ctypes.c_void_p],
+    ),
+    "cct_reduce_norm": (
+        ctypes.c_int,
+        [c_float_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, c_float_p, c_float_p, ctypes.c_void_p],
+    ),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load() -> ctypes.CDLL:
+    """Load the shared library (once) and bind the C signatures."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python -m pycorrectedemissionct_b200.build` "
+                    "(there is no CPU fallback)"
+                )
+            lib = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            if lib.cct_abi_version() != 1:
+                raise RuntimeError("libcorrct_b200.so ABI version mismatch")
+            _lib = lib
+    return _lib
+
+
+def check(status: int) -> None:
+    """Map a status code to the reference's exception types."""
+    if status == CCT_OK:
+        return
+    msg = load().cct_last_error().decode(errors="replace")
+    if status == CCT_ERR_VALUE:
+        raise ValueError(msg)
+    if status == CCT_ERR_UNSUPPORTED:
+        raise NotImplementedError(msg)
+    raise RuntimeError(f"CUDA error: {msg}")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(load(), name)(*args))

@@ -1,0 +1,249 @@
+"""Device-resident core of the XRF path: batched fp / bp / maps / solver steps on torch CUDA tensors.
+
+Everything here calls ``libcorrct_b200.so`` through the C ABI; torch only provides
+device memory and the current CUDA stream.  Inputs must already be CUDA tensors;
+there is no CPU path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib, geometry
+
+MAPS_DTYPES = {"float32": (torch.float32, _lib.CCT_DTYPE_F32), "bfloat16": (torch.bfloat16, _lib.CCT_DTYPE_BF16)}
+
+BP_MODES = {"reference": _lib.CCT_BP_REFERENCE, "symmetric": _lib.CCT_BP_SYMMETRIC, "adjoint": _lib.CCT_BP_ADJOINT}
+
+DEFAULT_MAPS_WORKSPACE = 256 << 20
+
+
+def require_cuda(device=None) -> torch.device:
+    """The CUDA device to run on; raises when CUDA is unavailable (no CPU fallback)."""
+    if not torch.cuda.is_available():
+        raise RuntimeError("corrct_b200 needs a CUDA device (B200, sm_100a); no CPU fallback exists")
+    if device is None:
+        return torch.device("cuda", torch.cuda.current_device())
+    device = torch.device(device)
+    if device.type != "cuda":
+        raise ValueError(f"corrct_b200 runs on CUDA devices only, got {device}")
+    return device
+
+
+def stream_handle(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _check_tensor(t: torch.Tensor, shape: tuple, dtype: torch.dtype, device: torch.device, name: str) -> None:
+    if not isinstance(t, torch.Tensor) or t.device != device:
+        raise ValueError(f"{name} must be a CUDA tensor on {device}")
+    if tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
+    if t.dtype != dtype:
+        raise ValueError(f"{name} has dtype {t.dtype}, expected {dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+class XrfCore:
+    """Geometry tables on the device plus batched projection entry points.
+
+    Parameters
+    ----------
+    n : int
+        Volume side (square) and detector width.
+    angles_rot_rad : array-like
+        Rotation angles (cast to float32 like the reference backend).
+    n_det : int
+        Fluorescence detectors (maps per angle).
+    weights : (A, D) array or None
+        ``w_det[d] * w_angle[a, d]`` applied by the attenuated fp and the symmetric bp.
+    """
+
+    def __init__(self, n: int, angles_rot_rad, n_det: int = 1, weights=None, device=None):
+        self.device = require_cuda(device)
+        self.n = int(n)
+        self.n_det = int(n_det)
+        self.angles_rad32, self.angles_deg32 = geometry.backend_angles(angles_rot_rad)
+        self.n_angles = len(self.angles_rad32)
+        self.fp_mat_np = geometry.fp_matrices(self.angles_deg32, self.n)
+        self.trig_np = geometry.bp_trig(self.angles_deg32)
+        self.fp_mat = torch.from_numpy(self.fp_mat_np).to(self.device)
+        self.trig = torch.from_numpy(self.trig_np).to(self.device)
+        self.set_weights(weights)
+
+    def set_weights(self, weights) -> None:
+        if weights is None:
+            self.weights = None
+            self.weights_np = None
+        else:
+            w = np.asarray(weights, dtype=np.float32).reshape(self.n_angles, self.n_det)
+            self.weights_np = w
+            self.weights = torch.from_numpy(np.ascontiguousarray(w)).to(self.device)
+
+    # ------------------------------------------------------------------ descriptors
+    def desc(self, n_slices: int, maps_dtype: int = _lib.CCT_DTYPE_F32, angles: slice | None = None) -> _lib.XrfDesc:
+        d = _lib.XrfDesc()
+        d.n = self.n
+        d.n_det = self.n_det
+        d.n_slices = int(n_slices)
+        d.maps_dtype = maps_dtype
+        if angles is None:
+            d.n_angles = self.n_angles
+            d.fp_matrix = self.fp_mat.data_ptr()
+            d.bp_trig = self.trig.data_ptr()
+            d.weights = _ptr(self.weights)
+        else:
+            a0, a1 = angles.start, angles.stop
+            d.n_angles = a1 - a0
+            d.fp_matrix = self.fp_mat[a0:a1].data_ptr()
+            d.bp_trig = self.trig[a0:a1].data_ptr()
+            d.weights = None if self.weights is None else self.weights[a0:a1].data_ptr()
+        return d
+
+    # ------------------------------------------------------------------ projections
+    def fp(
+        self,
+        vol: torch.Tensor,
+        maps: torch.Tensor | None = None,
+        out: torch.Tensor | None = None,
+        angles: slice | None = None,
+    ) -> torch.Tensor:
+        """Batched forward projection: vol (S, n, n) -> sino (S, D, A', n).
+
+        ``angles`` (a contiguous slice) restricts the projection to those angles; ``maps``
+        then holds only those angles: (S, A', D, n, n).
+        """
+        n = self.n
+        s = vol.shape[0]
+        na = self.n_angles if angles is None else angles.stop - angles.start
+        _check_tensor(vol, (s, n, n), torch.float32, self.device, "vol")
+        mdt = _lib.CCT_DTYPE_F32
+        if maps is not None:
+            mdt = self._check_maps(maps, s, na)
+        elif self.n_det != 1:
+            raise ValueError("an uncorrected projection needs a single detector")
+        if out is None:
+            out = torch.empty((s, self.n_det, na, n), dtype=torch.float32, device=self.device)
+        _check_tensor(out, (s, self.n_det, na, n), torch.float32, self.device, "sino")
+        desc = self.desc(s, mdt, angles)
+        _lib.call("cct_fp", ctypes.byref(desc), vol.data_ptr(), _ptr(maps), out.data_ptr(), stream_handle(self.device))
+        return out
+
+    def bp(
+        self,
+        sino: torch.Tensor,
+        mode: str = "reference",
+        maps: torch.Tensor | None = None,
+        out: torch.Tensor | None = None,
+        angles: slice | None = None,
+    ) -> torch.Tensor:
+        """Batched back projection: sino (S, D, A', n) -> vol (S, n, n)."""
+        n = self.n
+        s = sino.shape[0]
+        na = self.n_angles if angles is None else angles.stop - angles.start
+        _check_tensor(sino, (s, self.n_det, na, n), torch.float32, self.device, "sino")
+        if mode not in BP_MODES:
+            raise ValueError(f"Unknown back-projection mode {mode!r}; expected one of {sorted(BP_MODES)}")
+        mdt = _lib.CCT_DTYPE_F32
+        if maps is not None:
+            mdt = self._check_maps(maps, s, na)
+        if out is None:
+            out = torch.empty((s, n, n), dtype=torch.float32, device=self.device)
+        _check_tensor(out, (s, n, n), torch.float32, self.device, "vol")
+        desc = self.desc(s, mdt, angles)
+        _lib.call(
+            "cct_bp", ctypes.byref(desc), BP_MODES[mode], sino.data_ptr(), _ptr(maps), out.data_ptr(),
+            stream_handle(self.device),
+        )
+        return out
+
+    def _check_maps(self, maps: torch.Tensor, s: int, n_angles: int | None = None) -> int:
+        shape = (s, self.n_angles if n_angles is None else n_angles, self.n_det, self.n, self.n)
+        if maps.dtype == torch.bfloat16:
+            _check_tensor(maps, shape, torch.bfloat16, self.device, "maps")
+            return _lib.CCT_DTYPE_BF16
+        _check_tensor(maps, shape, torch.float32, self.device, "maps")
+        return _lib.CCT_DTYPE_F32
+
+    def partials_count(self, n_slices: int) -> int:
+        c = ctypes.c_int64(0)
+        desc = self.desc(n_slices)
+        _lib.call("cct_solver_partials_count", ctypes.byref(desc), ctypes.byref(c))
+        return int(c.value)
+
+
+def compute_maps(
+    mu_in: torch.Tensor | None,
+    mu_out: torch.Tensor | None,
+    angles_rad32,
+    det_angles=(np.pi / 2,),
+    surfaces_mm2=None,
+    distances_mm=None,
+    sub_sampling: int = 1,
+    maps_dtype: str = "float32",
+    workspace: torch.Tensor | None = None,
+    workspace_bytes: int = DEFAULT_MAPS_WORKSPACE,
+    out: torch.Tensor | None = None,
+) -> torch.Tensor:
+    """Attenuation maps (S, A, D, n, n) on the device from mu_in / mu_out (S, n, n) float32."""
+    ref = mu_in if mu_in is not None else mu_out
+    if ref is None:
+        raise ValueError("No attenuation volumes were given.")
+    device = require_cuda(ref.device)
+    s, n = ref.shape[0], ref.shape[-1]
+    for name, t in (("mu_in", mu_in), ("mu_out", mu_out)):
+        if t is not None:
+            _check_tensor(t, (s, n, n), torch.float32, device, name)
+    if maps_dtype not in MAPS_DTYPES:
+        raise ValueError(f"maps_dtype must be one of {sorted(MAPS_DTYPES)}")
+    tdt, cdt = MAPS_DTYPES[maps_dtype]
+    rot_in, rot_out, n_sub = geometry.attenuation_rotations(
+        angles_rad32, det_angles, n, surfaces_mm2, distances_mm, sub_sampling
+    )
+    n_ang, n_det = rot_out.shape[0], rot_out.shape[1]
+    rot_in_d = torch.from_numpy(np.ascontiguousarray(rot_in)).to(device)
+    rot_out_d = torch.from_numpy(np.ascontiguousarray(rot_out)).to(device)
+    desc = _lib.MapsDesc()
+    desc.n, desc.n_angles, desc.n_det, desc.n_slices = n, n_ang, n_det, s
+    desc.n_sub, desc.maps_dtype = n_sub, cdt
+    desc.has_in, desc.has_out = int(mu_in is not None), int(mu_out is not None)
+    desc.rot_in, desc.rot_out = rot_in_d.data_ptr(), rot_out_d.data_ptr()
+    need = ctypes.c_size_t(0)
+    _lib.call("cct_maps_workspace_size", ctypes.byref(desc), 1, ctypes.byref(need))
+    if workspace is None:
+        nbytes = max(int(need.value), min(int(workspace_bytes), int(need.value) * n_ang))
+        workspace = torch.empty(nbytes, dtype=torch.uint8, device=device)
+    if out is None:
+        maps = torch.empty((s, n_ang, n_det, n, n), dtype=tdt, device=device)
+    else:
+        _check_tensor(out, (s, n_ang, n_det, n, n), tdt, device, "out")
+        maps = out
+    compute_maps.last_passes = -(-n_ang // max(1, (workspace.numel() * workspace.element_size()) // int(need.value)))
+    _lib.call(
+        "cct_compute_maps", ctypes.byref(desc), _ptr(mu_in), _ptr(mu_out), maps.data_ptr(), workspace.data_ptr(),
+        workspace.numel() * workspace.element_size(), stream_handle(device),
+    )
+    # torch's caching allocator reuses the freed matrices / workspace only for work queued
+    # later on the same stream, so dropping them here is safe
+    return maps
+
+
+def reduce_norm(v: torch.Tensor, ord: int = 2) -> torch.Tensor:
+    """Per-slice FP64 norm sums of a (S, ...) float32 CUDA tensor: sum |v| (ord 1) or sum v^2 (ord 2)."""
+    device = require_cuda(v.device)
+    if v.dtype != torch.float32 or not v.is_contiguous():
+        raise ValueError("reduce_norm needs a contiguous float32 tensor")
+    s = v.shape[0]
+    count = v.numel() // s
+    out = torch.empty(s, dtype=torch.float64, device=device)
+    partials = torch.empty(s * 1024, dtype=torch.float64, device=device)
+    _lib.call("cct_reduce_norm", v.data_ptr(), count, s, ord, out.data_ptr(), partials.data_ptr(), stream_handle(device))
+    return out

@@ -1,0 +1,251 @@
+// C ABI entry points: argument validation, status codes, launches.
+
+#include <cstring>
+#include <string>
+
+#include "cct_common.cuh"
+#include "cct_internal.cuh"
+
+namespace cct {
+int launch_maps(const cct_maps_desc* d, const float* mu_in, const float* mu_out, void* maps, void* work,
+                size_t work_bytes, cudaStream_t st);
+int64_t maps_bytes_per_angle(const cct_maps_desc* d);
+void launch_residual_step(const double* partials, int64_t per_slice, int n_slices, double* residuals, int* active,
+                          int* iterations, const double* tolerance, double* history, int history_len,
+                          cudaStream_t st);
+void launch_tv_dual(const float* x_relax, float* q, int n, int n_slices, float lam, const int* active,
+                    cudaStream_t st);
+void launch_norm(const float* v, int64_t count, int n_slices, int ord, double* out, double* partials,
+                 cudaStream_t st);
+}  // namespace cct
+
+static thread_local std::string g_last_error;
+
+void cct_set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
+static int check_launch() {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    cct_set_last_error(cudaGetErrorString(e));
+    return CCT_ERR_CUDA;
+  }
+  return CCT_OK;
+}
+
+static int validate_desc(const cct_xrf_desc* d) {
+  CCT_REQUIRE(d != nullptr, "descriptor is NULL");
+  CCT_REQUIRE(d->n >= 2 && d->n <= 8192, "volume side n must be in [2, 8192]");
+  CCT_REQUIRE(d->n_angles >= 1 && d->n_det >= 1 && d->n_slices >= 1, "n_angles, n_det and n_slices must be >= 1");
+  CCT_REQUIRE((int64_t)d->n_angles * d->n_det <= 65535, "n_angles * n_det must be <= 65535");
+  CCT_REQUIRE(d->n_slices <= 65535, "n_slices must be <= 65535");
+  CCT_REQUIRE(d->maps_dtype == CCT_DTYPE_F32 || d->maps_dtype == CCT_DTYPE_BF16, "maps_dtype must be F32 or BF16");
+  CCT_REQUIRE(d->fp_matrix != nullptr && d->bp_trig != nullptr, "fp_matrix and bp_trig are required");
+  return CCT_OK;
+}
+
+static cct::FpArgs make_fp_args(const cct_xrf_desc* d, const float* vol, const void* maps, float* out) {
+  cct::FpArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.n = d->n; a.n_angles = d->n_angles; a.n_det = d->n_det; a.n_slices = d->n_slices;
+  a.maps_dtype = d->maps_dtype; a.epi = cct::FP_EPI_STORE;
+  a.fp_matrix = d->fp_matrix; a.weights = d->weights; a.vol = vol; a.maps = maps; a.out = out;
+  return a;
+}
+
+static cct::BpArgs make_bp_args(const cct_xrf_desc* d, int mode, const float* sino, const void* maps, float* out) {
+  cct::BpArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.n = d->n; a.n_angles = d->n_angles; a.n_det = d->n_det; a.n_slices = d->n_slices;
+  a.maps_dtype = d->maps_dtype; a.mode = mode; a.epi = cct::BP_EPI_STORE;
+  a.fp_matrix = d->fp_matrix; a.bp_trig = d->bp_trig; a.weights = d->weights;
+  a.sino = sino; a.maps = maps; a.out = out;
+  return a;
+}
+
+extern "C" {
+
+int cct_abi_version(void) { return CCT_ABI_VERSION; }
+
+const char* cct_last_error(void) { return g_last_error.c_str(); }
+
+int cct_fp(const cct_xrf_desc* desc, const float* vol, const void* maps, float* sino, void* stream) {
+  int rc = validate_desc(desc);
+  if (rc != CCT_OK) return rc;
+  CCT_REQUIRE(vol != nullptr && sino != nullptr, "vol and sino are required");
+  CCT_REQUIRE(maps != nullptr || desc->n_det == 1, "an uncorrected projection (maps == NULL) needs n_det == 1");
+  cct::FpArgs a = make_fp_args(desc, vol, maps, sino);
+  cct::launch_fp(a, reinterpret_cast<cudaStream_t>(stream));
+  return check_launch();
+}
+
+int cct_bp(const cct_xrf_desc* desc, int32_t mode, const float* sino, const void* maps, float* vol, void* stream) {
+  int rc = validate_desc(desc);
+  if (rc != CCT_OK) return rc;
+  CCT_REQUIRE(sino != nullptr && vol != nullptr, "sino and vol are required");
+  CCT_REQUIRE(mode == CCT_BP_REFERENCE || mode == CCT_BP_SYMMETRIC || mode == CCT_BP_ADJOINT, "unknown bp mode");
+  CCT_REQUIRE(mode != CCT_BP_SYMMETRIC || maps != nullptr, "the symmetric back projection needs maps");
+  CCT_REQUIRE(!(mode == CCT_BP_ADJOINT && maps == nullptr && desc->n_det != 1),
+              "an uncorrected adjoint (maps == NULL) needs n_det == 1");
+  cct::BpArgs a = make_bp_args(desc, mode, sino, maps, vol);
+  cct::launch_bp(a, reinterpret_cast<cudaStream_t>(stream));
+  return check_launch();
+}
+
+int cct_maps_workspace_size(const cct_maps_desc* desc, int32_t angles_per_pass, size_t* bytes) {
+  CCT_REQUIRE(desc != nullptr && bytes != nullptr, "descriptor and bytes are required");
+  CCT_REQUIRE(desc->n >= 2 && desc->n <= 8192, "volume side n must be in [2, 8192]");
+  CCT_REQUIRE(desc->n_angles >= 1 && desc->n_det >= 1 && desc->n_slices >= 1 && desc->n_sub >= 1,
+              "n_angles, n_det, n_slices and n_sub must be >= 1");
+  CCT_REQUIRE(angles_per_pass >= 1, "angles_per_pass must be >= 1");
+  CCT_REQUIRE(desc->has_in || desc->has_out, "No attenuation volumes were given.");
+  *bytes = (size_t)cct::maps_bytes_per_angle(desc) * (size_t)angles_per_pass;
+  return CCT_OK;
+}
+
+int cct_compute_maps(const cct_maps_desc* desc, const float* mu_in, const float* mu_out, void* maps,
+                     void* workspace, size_t workspace_bytes, void* stream) {
+  size_t need = 0;
+  int rc = cct_maps_workspace_size(desc, 1, &need);
+  if (rc != CCT_OK) return rc;
+  CCT_REQUIRE(desc->maps_dtype == CCT_DTYPE_F32 || desc->maps_dtype == CCT_DTYPE_BF16,
+              "maps_dtype must be F32 or BF16");
+  CCT_REQUIRE(!desc->has_in || (mu_in != nullptr && desc->rot_in != nullptr), "incident volume or matrices missing");
+  CCT_REQUIRE(!desc->has_out || (mu_out != nullptr && desc->rot_out != nullptr), "emitted volume or matrices missing");
+  CCT_REQUIRE(maps != nullptr && workspace != nullptr, "maps and workspace are required");
+  CCT_REQUIRE(workspace_bytes >= need, "workspace smaller than one angle pass (cct_maps_workspace_size)");
+  CCT_REQUIRE(desc->n_angles <= 65535 && desc->n_slices <= 65535, "too many angles or slices");
+  rc = cct::launch_maps(desc, mu_in, mu_out, maps, workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
+  if (rc != CCT_OK) return rc;
+  return check_launch();
+}
+
+int cct_device_error(int32_t clear, int32_t* value) {
+  CCT_REQUIRE(value != nullptr, "value is required");
+  int v = 0;
+  const int e = cct::read_device_error(clear, &v);
+  if (e != 0) {
+    cct_set_last_error(cudaGetErrorString((cudaError_t)e));
+    return CCT_ERR_CUDA;
+  }
+  *value = v;
+  return CCT_OK;
+}
+
+int cct_solver_partials_count(const cct_xrf_desc* desc, int64_t* count) {
+  int rc = validate_desc(desc);
+  if (rc != CCT_OK) return rc;
+  CCT_REQUIRE(count != nullptr, "count is required");
+  const int64_t bands = (desc->n + 63) / 64;
+  *count = (int64_t)desc->n_slices * bands * desc->n_angles * desc->n_det;
+  return CCT_OK;
+}
+
+static int validate_state(const cct_xrf_desc* d, const cct_solver_state* st) {
+  CCT_REQUIRE(st != nullptr, "solver state is NULL");
+  CCT_REQUIRE(st->x && st->b && st->tau && st->sino_buf && st->partials && st->residuals && st->active &&
+                  st->iterations,
+              "solver state is missing a required buffer");
+  (void)d;
+  return CCT_OK;
+}
+
+static cct::BpArgs make_solver_bp(const cct_xrf_desc* d, int mode, const void* maps, const cct_solver_state* st,
+                                  int epi) {
+  cct::BpArgs a = make_bp_args(d, mode, st->sino_buf, maps, st->vol_buf);
+  a.epi = epi;
+  a.x = st->x; a.x_relax = st->x_relax; a.tau = st->tau; a.tau_shared = st->tau_shared;
+  a.x_mask = st->x_mask; a.tv_dual = st->tv_dual;
+  a.lower = st->lower_limit; a.upper = st->upper_limit; a.has_lower = st->has_lower; a.has_upper = st->has_upper;
+  a.active = st->active;
+  return a;
+}
+
+int cct_mlem_fp(const cct_xrf_desc* desc, const void* maps, cct_solver_state* st, void* stream) {
+  int rc = validate_desc(desc);
+  if (rc != CCT_OK) return rc;
+  rc = validate_state(desc, st);
+  if (rc != CCT_OK) return rc;
+  CCT_REQUIRE(maps != nullptr || desc->n_det == 1, "an uncorrected MLEM (maps == NULL) needs n_det == 1");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  cct::FpArgs f = make_fp_args(desc, st->x, maps, st->sino_buf);
+  f.epi = cct::FP_EPI_MLEM; f.b = st->b; f.background = st->background; f.has_background = st->has_background;
+  f.partials = st->partials; f.active = st->active;
+  cct::launch_fp(f, s);
+  int64_t per_slice = 0;
+  cct_solver_partials_count(desc, &per_slice);
+  per_slice /= desc->n_slices;
+  cct::launch_residual_step(st->partials, per_slice, desc->n_slices, st->residuals, st->active, st->iterations,
+                            st->tolerance, st->residual_history, st->history_len, s);
+  return check_launch();
+}
+
+int cct_mlem_update(const cct_xrf_desc* desc, cct_solver_state* st, void* stream) {
+  int rc = validate_desc(desc);
+  if (rc != CCT_OK) return rc;
+  rc = validate_state(desc, st);
+  if (rc != CCT_OK) return rc;
+  // the reference's default XRF back projection ignores maps and weights (projectors.py:619-622)
+  cct::BpArgs b = make_solver_bp(desc, CCT_BP_REFERENCE, nullptr, st, cct::BP_EPI_MLEM);
+  cct::launch_bp(b, reinterpret_cast<cudaStream_t>(stream));
+  return check_launch();
+}
+
+int cct_mlem_step(const cct_xrf_desc* desc, const void* maps, cct_solver_state* st, void* stream) {
+  const int rc = cct_mlem_fp(desc, maps, st, stream);
+  if (rc != CCT_OK) return rc;
+  return cct_mlem_update(desc, st, stream);
+}
+
+int cct_sirt_step(const cct_xrf_desc* desc, const void* maps, int32_t bp_mode, cct_solver_state* st, void* stream) {
+  int rc = validate_desc(desc);
+  if (rc != CCT_OK) return rc;
+  rc = validate_state(desc, st);
+  if (rc != CCT_OK) return rc;
+  CCT_REQUIRE(st->sigma != nullptr, "SIRT needs sigma");
+  CCT_REQUIRE(bp_mode == CCT_BP_REFERENCE || bp_mode == CCT_BP_SYMMETRIC, "SIRT bp_mode must be REFERENCE or SYMMETRIC");
+  CCT_REQUIRE(bp_mode != CCT_BP_SYMMETRIC || maps != nullptr, "the symmetric back projection needs maps");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  cct::FpArgs f = make_fp_args(desc, st->x, maps, st->sino_buf);
+  f.epi = cct::FP_EPI_SIRT; f.b = st->b; f.sigma = st->sigma; f.background = st->background;
+  f.has_background = st->has_background; f.partials = st->partials; f.active = st->active;
+  cct::launch_fp(f, s);
+  int64_t per_slice = 0;
+  cct_solver_partials_count(desc, &per_slice);
+  per_slice /= desc->n_slices;
+  cct::launch_residual_step(st->partials, per_slice, desc->n_slices, st->residuals, st->active, st->iterations,
+                            st->tolerance, st->residual_history, st->history_len, s);
+  cct::BpArgs b = make_solver_bp(desc, bp_mode, maps, st, cct::BP_EPI_SIRT);
+  cct::launch_bp(b, s);
+  return check_launch();
+}
+
+int cct_pdhg_step(const cct_xrf_desc* desc, const void* maps, int32_t bp_mode, cct_solver_state* st, void* stream) {
+  int rc = validate_desc(desc);
+  if (rc != CCT_OK) return rc;
+  rc = validate_state(desc, st);
+  if (rc != CCT_OK) return rc;
+  CCT_REQUIRE(st->sigma != nullptr && st->x_relax != nullptr && st->tv_dual != nullptr,
+              "PDHG needs sigma, x_relax and tv_dual");
+  CCT_REQUIRE(bp_mode == CCT_BP_REFERENCE || bp_mode == CCT_BP_SYMMETRIC, "PDHG bp_mode must be REFERENCE or SYMMETRIC");
+  CCT_REQUIRE(bp_mode != CCT_BP_SYMMETRIC || maps != nullptr, "the symmetric back projection needs maps");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  cct::FpArgs f = make_fp_args(desc, st->x_relax, maps, st->sino_buf);
+  f.epi = cct::FP_EPI_PDHG; f.b = st->b; f.sigma = st->sigma; f.background = st->background;
+  f.has_background = st->has_background; f.active = st->active;
+  cct::launch_fp(f, s);
+  cct::launch_tv_dual(st->x_relax, st->tv_dual, desc->n, desc->n_slices, st->tv_lambda, st->active, s);
+  cct::BpArgs b = make_solver_bp(desc, bp_mode, maps, st, cct::BP_EPI_PDHG);
+  cct::launch_bp(b, s);
+  return check_launch();
+}
+
+int cct_reduce_norm(const float* v, int64_t count, int32_t n_slices, int32_t ord, double* out, double* partials,
+                    void* stream) {
+  CCT_REQUIRE(v != nullptr && out != nullptr && partials != nullptr, "v, out and partials are required");
+  CCT_REQUIRE(count >= 1 && n_slices >= 1 && n_slices <= 65535, "count and n_slices must be >= 1");
+  CCT_REQUIRE(ord == 1 || ord == 2, "ord must be 1 or 2");
+  cct::launch_norm(v, count, n_slices, ord, out, partials, reinterpret_cast<cudaStream_t>(stream));
+  return check_launch();
+}
+
+}  // extern "C"

@@ -1,0 +1,137 @@
+// Internal launch arguments and fused epilogues shared by the projection and solver kernels.
+#pragma once
+
+#include "cct_common.cuh"
+
+namespace cct {
+
+constexpr float EPS32 = 1.1920928955078125e-07f;  // np.finfo(np.float32).eps (corrct solvers.py:20)
+
+// Sample position of output (col c, row r) under a radon inverse map; every kernel that
+// needs the position of a forward-projection sample evaluates exactly this expression.
+__device__ __forceinline__ float sample_x(float ma, float mb, float mc, float c, float r) {
+  return fmaf(mb, r, fmaf(ma, c, mc));
+}
+
+enum FpEpilogue : int { FP_EPI_STORE = 0, FP_EPI_MLEM = 1, FP_EPI_SIRT = 2, FP_EPI_PDHG = 3 };
+enum BpEpilogue : int { BP_EPI_STORE = 0, BP_EPI_MLEM = 1, BP_EPI_SIRT = 2, BP_EPI_PDHG = 3 };
+
+struct FpArgs {
+  int n, n_angles, n_det, n_slices, maps_dtype, epi;
+  const float* fp_matrix;
+  const float* weights;
+  const float* vol;
+  const void* maps;
+  float* out;          // STORE: A x; MLEM: b / max(Ax + bg, eps); SIRT: (b - Ax - bg) * sigma; PDHG: dual p
+  const float* b;
+  const float* sigma;  // SIRT / PDHG
+  float background;
+  int has_background;
+  double* partials;    // per-CTA residual partial sums (MLEM, SIRT)
+  const int* active;
+};
+
+struct BpArgs {
+  int n, n_angles, n_det, n_slices, maps_dtype, mode, epi;
+  const float* fp_matrix;
+  const float* bp_trig;
+  const float* weights;
+  const float* sino;
+  const void* maps;
+  float* out;              // STORE target
+  // fused solver epilogues
+  float* x;
+  float* x_relax;
+  const float* tau;
+  int tau_shared;
+  const float* x_mask;
+  const float* tv_dual;    // PDHG: updated TV dual [S][2][n][n]
+  float lower, upper;
+  int has_lower, has_upper;
+  const int* active;
+};
+
+// Fused forward-projection epilogue for one final value `ax` = (A x)[idx].
+// Returns this element's contribution to the slice residual (FP64).
+template <int EPI>
+__device__ __forceinline__ double fp_epilogue(const FpArgs& a, int64_t idx, float ax) {
+  if (EPI == FP_EPI_STORE) {
+    a.out[idx] = ax;
+    return 0.0;
+  } else if (EPI == FP_EPI_MLEM) {
+    // corrct solvers.py:787-796 and data_terms.py:720-742 (KL, sigma = 1)
+    const float bb = a.b[idx];
+    const float proj = a.has_background ? ax + a.background : ax;
+    const float clipped = fmaxf(proj, EPS32);
+    a.out[idx] = bb / clipped;
+    const double r = (double)clipped;
+    const double sd = 4.0 * fmax((double)bb, 0.0);
+    const double res = (1.0 + r - sqrt((r - 1.0) * (r - 1.0) + sd)) * 0.5;
+    return fabs(res);
+  } else if (EPI == FP_EPI_SIRT) {
+    // corrct data_terms.py:136-161 (l2 residual), solvers.py:954-977
+    const float proj = a.has_background ? ax + a.background : ax;
+    const float res = a.b[idx] - proj;
+    a.out[idx] = res * a.sigma[idx];
+    return (double)res * (double)res;
+  } else {
+    // PDHG dual update + KL prox (corrct data_terms.py:262-276, 682-692)
+    const float proj = a.has_background ? ax + a.background : ax;
+    const double sg = (double)a.sigma[idx];
+    const double p = (double)a.out[idx] + (double)proj * sg;
+    const double sd = 4.0 * sg * fmax((double)a.b[idx], 0.0);
+    a.out[idx] = (float)((1.0 + p - sqrt((p - 1.0) * (p - 1.0) + sd)) * 0.5);
+    return 0.0;
+  }
+}
+
+__device__ __forceinline__ float apply_limits(const BpArgs& a, float v) {
+  // x.clip(lower, upper): numpy clip is min(max(v, lower), upper)
+  if (a.has_lower) v = fmaxf(v, a.lower);
+  if (a.has_upper) v = fminf(v, a.upper);
+  return v;
+}
+
+// Fused back-projection epilogue for pixel (s, i, j) with back-projected value `v`.
+template <int EPI>
+__device__ __forceinline__ void bp_epilogue(const BpArgs& a, int s, int i, int j, float v) {
+  const int64_t n2 = (int64_t)a.n * a.n;
+  const int64_t pix = (int64_t)i * a.n + j;
+  const int64_t idx = (int64_t)s * n2 + pix;
+  if (EPI == BP_EPI_STORE) {
+    a.out[idx] = v;
+    return;
+  }
+  const float tau = a.tau[(a.tau_shared ? 0 : (int64_t)s * n2) + pix];
+  float x = a.x[idx];
+  if (EPI == BP_EPI_MLEM) {
+    // x *= upd / tau  (corrct solvers.py:798-803)
+    x = x * (v / tau);
+  } else if (EPI == BP_EPI_SIRT) {
+    // x += upd * tau  (corrct solvers.py:977)
+    x = x + v * tau;
+  } else {
+    // PDHG primal step (corrct solvers.py:1179-1190): x_new = x - (A^T p - div q) * tau,
+    // div with edge padding (operators.py:818-844)
+    const float* q = a.tv_dual + (int64_t)s * 2 * n2;
+    const float q0 = q[pix], q1 = q[n2 + pix];
+    const float d0 = (i > 0) ? q0 - q[pix - a.n] : 0.f;
+    const float d1 = (j > 0) ? q1 - q[n2 + pix - 1] : 0.f;
+    const float upd = v - (d0 + d1);
+    float xn = x - upd * tau;
+    xn = apply_limits(a, xn);
+    if (a.x_mask != nullptr) xn *= a.x_mask[pix];
+    a.x_relax[idx] = xn + (xn - x);
+    a.x[idx] = xn;
+    return;
+  }
+  x = apply_limits(a, x);
+  if (a.x_mask != nullptr) x *= a.x_mask[pix];
+  a.x[idx] = x;
+}
+
+void launch_fp(const FpArgs& a, cudaStream_t st);
+int read_device_error(int clear, int* value);
+void launch_bp(const BpArgs& a, cudaStream_t st);
+
+}  // namespace cct

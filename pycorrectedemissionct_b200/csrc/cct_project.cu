@@ -1,0 +1,456 @@
+// Forward and back projection kernels of the XRF path (sm_100a).
+//
+// Forward projection (scikit-image radon discretisation, corrct:
+// src/corrct/_projector_backends.py:312-333, attenuated form projectors.py:502-531):
+//   sino[s][d][a][c] = w[a][d] * sum_r bilin(vol[s] * maps[s][a][d], M_a (c, r))
+// One CTA owns (slice, angle, detector, band of 64 detector bins) and walks the
+// column band in chunks of 64 rows.  For each chunk the bounding box of the
+// rotated chunk is staged in shared memory as z = vol * map (coalesced float4
+// loads of both, zero outside the image, odd row stride so lanes on different
+// rows hit different banks), then each thread samples 16 rows of one column
+// from shared memory.  Column sums stay in registers; the CTA writes final
+// values, so the result is deterministic and needs no atomics or partial sums.
+// The map of every angle is read from HBM once; the volume is L2-resident.
+//
+// Back projection (scikit-image iradon, filter None, corrct:
+// src/corrct/_projector_backends.py:335-359): one CTA owns a 32x32 pixel tile and
+// loops over all (detector, angle) lines in chunks of 32; each chunk stages, per
+// line, the <= 48 detector bins the tile can reach as (value, slope) pairs, and
+// every pixel does one shared-memory lookup and one FMA per line.  np.interp's
+// left=0 / right=0 edges are discontinuous, so lines whose range comes within
+// 0.01 bin of an edge take a checked path that decides edge cases in double
+// precision exactly as numpy does.
+
+#include "cct_common.cuh"
+#include "cct_internal.cuh"
+
+namespace cct {
+
+// Raised (never trapped) if a staged box would exceed its shared-memory bound; valid
+// rotation matrices cannot reach it.  Read through cct_device_error().
+__device__ int g_box_overflow = 0;
+
+// ------------------------------------------------------------------------------------------
+// Forward projection
+// ------------------------------------------------------------------------------------------
+constexpr int FP_TC = 64;                          // detector bins per CTA
+constexpr int FP_TR = 64;                          // rows per staged chunk
+constexpr int FP_THREADS = 256;
+constexpr int FP_RGROUPS = FP_THREADS / FP_TC;     // 4 row groups
+constexpr int FP_RPT = FP_TR / FP_RGROUPS;         // 16 rows per thread per chunk
+// Rotated 64x64 chunk: extent <= 64*sqrt(2) = 90.6, +1/+2 tap margins, +3 for float4
+// alignment of the left edge, rounded up to a multiple of 4.
+constexpr int FP_BOX_W = 100;
+constexpr int FP_BOX_H = 96;
+constexpr int FP_STRIDE = FP_BOX_W + 1;            // odd stride: conflict-free steep-angle lanes
+
+template <int EPI, bool HAS_MAPS, int MAPS_DTYPE>
+__global__ void __launch_bounds__(FP_THREADS) fp_kernel(FpArgs args) {
+  __shared__ float z[FP_BOX_H * FP_STRIDE];
+  __shared__ float red[FP_THREADS];
+  __shared__ double red_d[FP_TC / 32];
+
+  const int n = args.n;
+  const int band = blockIdx.x;
+  const int ad = blockIdx.y;
+  const int s = blockIdx.z;
+  if (args.active != nullptr && args.active[s] == 0) return;
+  const int a = ad / args.n_det;
+  const int d = ad - a * args.n_det;
+
+  const float* M = args.fp_matrix + 6 * a;
+  const float m00 = M[0], m01 = M[1], m02 = M[2], m10 = M[3], m11 = M[4], m12 = M[5];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int cl = tid & (FP_TC - 1);
+  const int rg = tid / FP_TC;
+  const int c0 = band * FP_TC;
+  const int c = c0 + cl;
+  const int c_last = min(c0 + FP_TC, n) - 1;
+
+  const float* vol = args.vol + (int64_t)s * n * n;
+  const int64_t map_off = (((int64_t)s * args.n_angles + a) * args.n_det + d) * (int64_t)n * n;
+  const bool vec4 = (n & 3) == 0;
+
+  float acc = 0.f;
+  for (int r0 = 0; r0 < n; r0 += FP_TR) {
+    const int r_last = min(r0 + FP_TR, n) - 1;
+    // Bounding box of the chunk's sample positions (corners of the rotated rectangle).
+    const float fc0 = (float)c0, fc1 = (float)c_last, fr0 = (float)r0, fr1 = (float)r_last;
+    const float xa = sample_x(m00, m01, m02, fc0, fr0), xb = sample_x(m00, m01, m02, fc1, fr0);
+    const float xc = sample_x(m00, m01, m02, fc0, fr1), xd = sample_x(m00, m01, m02, fc1, fr1);
+    const float ya = sample_x(m10, m11, m12, fc0, fr0), yb = sample_x(m10, m11, m12, fc1, fr0);
+    const float yc = sample_x(m10, m11, m12, fc0, fr1), yd = sample_x(m10, m11, m12, fc1, fr1);
+    const float xmin = fminf(fminf(xa, xb), fminf(xc, xd)), xmax = fmaxf(fmaxf(xa, xb), fmaxf(xc, xd));
+    const float ymin = fminf(fminf(ya, yb), fminf(yc, yd)), ymax = fmaxf(fmaxf(ya, yb), fmaxf(yc, yd));
+    int bx0 = (int)floorf(xmin) - 1;
+    const int bx1 = (int)floorf(xmax) + 2;
+    const int by0 = (int)floorf(ymin) - 1;
+    const int by1 = (int)floorf(ymax) + 2;
+    bx0 &= ~3;  // floor to a multiple of 4 (two's complement) for aligned float4 loads
+    const int q4 = (bx1 - bx0) / 4 + 1;  // float4 columns
+    const int bh = by1 - by0 + 1;
+    if (4 * q4 > FP_BOX_W || bh > FP_BOX_H) {  // cannot happen for valid matrices; never trap
+      if (tid == 0) atomicExch(&g_box_overflow, 1);
+      return;
+    }
+
+    // Stage z = vol * map over the box (zeros outside the image).
+    for (int rr = warp; rr < bh; rr += FP_THREADS / 32) {
+      const int gy = by0 + rr;
+      const bool row_in = gy >= 0 && gy < n;
+      for (int q = lane; q < q4; q += 32) {
+        const int gx = bx0 + 4 * q;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (row_in) {
+          const int64_t off = (int64_t)gy * n + gx;
+          if (vec4 && gx >= 0 && gx + 3 < n) {
+            v = __ldg(reinterpret_cast<const float4*>(vol + off));
+            if (HAS_MAPS) {
+              if (MAPS_DTYPE == CCT_DTYPE_BF16) {
+                const uint2 raw = __ldg(reinterpret_cast<const uint2*>(
+                    reinterpret_cast<const __nv_bfloat16*>(args.maps) + map_off + off));
+                const __nv_bfloat162 lo = *reinterpret_cast<const __nv_bfloat162*>(&raw.x);
+                const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162*>(&raw.y);
+                const float2 flo = __bfloat1622float2(lo), fhi = __bfloat1622float2(hi);
+                v.x *= flo.x; v.y *= flo.y; v.z *= fhi.x; v.w *= fhi.y;
+              } else {
+                const float4 mv = __ldg(reinterpret_cast<const float4*>(
+                    reinterpret_cast<const float*>(args.maps) + map_off + off));
+                v.x *= mv.x; v.y *= mv.y; v.z *= mv.z; v.w *= mv.w;
+              }
+            }
+          } else if (!vec4 || (gx + 3 >= 0 && gx < n)) {
+            float e[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const int xx = gx + k;
+              float val = 0.f;
+              if (xx >= 0 && xx < n) {
+                val = __ldg(vol + off + k);
+                if (HAS_MAPS) val *= load_map(args.maps, MAPS_DTYPE, map_off + off + k);
+              }
+              e[k] = val;
+            }
+            v = make_float4(e[0], e[1], e[2], e[3]);
+          }
+        }
+        float* dst = z + rr * FP_STRIDE + 4 * q;
+        dst[0] = v.x; dst[1] = v.y; dst[2] = v.z; dst[3] = v.w;
+      }
+    }
+    __syncthreads();
+
+    if (c <= c_last) {
+      const int rb = r0 + rg * FP_RPT;
+      const int re = min(rb + FP_RPT, r_last + 1);
+      // Sample positions use exactly sample_x()'s expression so that the adjoint
+      // kernel (and the box corners) see bit-identical coordinates.
+      const float fc = (float)c;
+      const float pxc = fmaf(m00, fc, m02);
+      const float pyc = fmaf(m10, fc, m12);
+      const float* zb = z - by0 * FP_STRIDE - bx0;
+      float fr = (float)rb;
+#pragma unroll 4
+      for (int r = rb; r < re; ++r) {
+        const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
+        const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
+        const float* p = zb + fy.i * FP_STRIDE + fx.i;
+        const float t0 = p[0], t1 = p[1], b0 = p[FP_STRIDE], b1 = p[FP_STRIDE + 1];
+        const float top = fmaf(fx.f, t1 - t0, t0);
+        const float bot = fmaf(fx.f, b1 - b0, b0);
+        acc += fmaf(fy.f, bot - top, top);
+        fr += 1.f;
+      }
+    }
+    __syncthreads();
+  }
+
+  red[tid] = acc;
+  __syncthreads();
+  if (rg == 0) {
+    double part = 0.0;
+    if (c <= c_last) {
+      float total = red[cl] + red[cl + FP_TC] + red[cl + 2 * FP_TC] + red[cl + 3 * FP_TC];
+      if (args.weights != nullptr) total *= args.weights[a * args.n_det + d];
+      const int64_t idx = (((int64_t)s * args.n_det + d) * args.n_angles + a) * n + c;
+      part = fp_epilogue<EPI>(args, idx, total);
+    }
+    if (EPI != FP_EPI_STORE) {
+      part = warp_sum_double(part);
+      if (lane == 0) red_d[warp] = part;
+    }
+  }
+  if (EPI != FP_EPI_STORE) {
+    __syncthreads();
+    if (tid == 0) {
+      const int64_t per_slice = (int64_t)gridDim.x * gridDim.y;
+      args.partials[(int64_t)s * per_slice + (int64_t)blockIdx.y * gridDim.x + blockIdx.x] = red_d[0] + red_d[1];
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Back projection (reference iradon discretisation, optional maps x weights)
+// ------------------------------------------------------------------------------------------
+constexpr int BP_TILE = 32;
+constexpr int BP_THREADS = 256;
+constexpr int BP_PPT = BP_TILE * BP_TILE / BP_THREADS;  // 4 pixels per thread
+constexpr int BP_LINES = 32;                             // lines staged per chunk
+constexpr int BP_KW = 64;                                // staged pairs per line (>= 48 needed)
+constexpr float BP_EDGE_GUARD = 0.01f;
+
+enum : int { LINE_FAST = 0, LINE_CHECKED = 1, LINE_EMPTY = 2 };
+
+template <int EPI, bool SYM, int MAPS_DTYPE>
+__global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
+  __shared__ float2 pairs[BP_LINES][BP_KW];
+  __shared__ float4 linfo[BP_LINES];  // cos, sin, offset (K - kbase), weight
+  __shared__ int lkind[BP_LINES];
+  __shared__ int lkbase[BP_LINES];
+
+  const int n = args.n;
+  const int s = blockIdx.y;
+  if (args.active != nullptr && args.active[s] == 0) return;
+  const int tiles_j = (n + BP_TILE - 1) / BP_TILE;
+  const int ti = blockIdx.x / tiles_j;
+  const int tj = blockIdx.x - ti * tiles_j;
+  const int i0 = ti * BP_TILE, j0 = tj * BP_TILE;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int j = j0 + lane;
+  const int R = n / 2;      // iradon output radius (output_size // 2)
+  const int K = n / 2;      // detector offset (img_shape // 2)
+  const float t_left = (float)(-K), t_right = (float)(n - 1 - K);
+  const int n_lines = args.n_det * args.n_angles;
+  const float* sino = args.sino + (int64_t)s * n_lines * n;
+
+  // tile corners relative to the centre
+  // full tile (also pixels beyond n, which are computed and discarded) so every
+  // thread's lookup stays inside the staged range
+  const float cj0 = (float)(j0 - R), cj1 = (float)(j0 + BP_TILE - 1 - R);
+  const float ci0 = (float)(i0 - R), ci1 = (float)(i0 + BP_TILE - 1 - R);
+
+  float acc[BP_PPT];
+#pragma unroll
+  for (int k = 0; k < BP_PPT; ++k) acc[k] = 0.f;
+
+  for (int l0 = 0; l0 < n_lines; l0 += BP_LINES) {
+    // ---- stage up to BP_LINES lines: each warp fills 4 lines
+    for (int ll = warp; ll < BP_LINES; ll += BP_THREADS / 32) {
+      const int l = l0 + ll;
+      if (l >= n_lines) break;
+      const int d = l / args.n_angles;
+      const int a = l - d * args.n_angles;
+      const float cs = args.bp_trig[2 * a], sn = args.bp_trig[2 * a + 1];
+      // t = (j - R) cos - (i - R) sin at the four corners
+      const float t00 = fmaf(cj0, cs, -ci0 * sn), t01 = fmaf(cj1, cs, -ci0 * sn);
+      const float t10 = fmaf(cj0, cs, -ci1 * sn), t11 = fmaf(cj1, cs, -ci1 * sn);
+      const float tmin = fminf(fminf(t00, t01), fminf(t10, t11));
+      const float tmax = fmaxf(fmaxf(t00, t01), fmaxf(t10, t11));
+      int kind = LINE_FAST;
+      if (tmax < t_left - BP_EDGE_GUARD || tmin > t_right + BP_EDGE_GUARD) {
+        kind = LINE_EMPTY;
+      } else if (tmin < t_left + BP_EDGE_GUARD || tmax > t_right - BP_EDGE_GUARD) {
+        kind = LINE_CHECKED;
+      }
+      const int kbase = (int)floorf(tmin + (float)K) - 1;
+      float w = 1.f;
+      if (SYM && args.weights != nullptr) w = args.weights[a * args.n_det + d];
+      const float* line = sino + ((int64_t)d * args.n_angles + a) * n;
+      for (int q = lane; q < BP_KW; q += 32) {
+        const int kk = kbase + q;
+        const float v0 = (kk >= 0 && kk < n) ? __ldg(line + kk) : 0.f;
+        const float v1 = (kk + 1 >= 0 && kk + 1 < n) ? __ldg(line + kk + 1) : 0.f;
+        pairs[ll][q] = make_float2(w * v0, w * (v1 - v0));
+      }
+      if (lane == 0) {
+        linfo[ll] = make_float4(cs, sn, (float)(K - kbase), w);
+        lkind[ll] = kind;
+        lkbase[ll] = kbase;
+      }
+    }
+    __syncthreads();
+
+    // ---- accumulate
+    const int lines_here = min(BP_LINES, n_lines - l0);
+    for (int ll = 0; ll < lines_here; ++ll) {
+      const int kind = lkind[ll];
+      if (kind == LINE_EMPTY) continue;
+      const float4 inf = linfo[ll];
+      const float base = fmaf((float)(j - R), inf.x, inf.z);
+      const float2* pr = pairs[ll];
+      int a = 0, d = 0;
+      if (SYM) {
+        const int l = l0 + ll;
+        d = l / args.n_angles;
+        a = l - d * args.n_angles;
+      }
+#pragma unroll
+      for (int k = 0; k < BP_PPT; ++k) {
+        const int i = i0 + warp + 8 * k;
+        const float u = fmaf(-(float)(i - R), inf.y, base);
+        const FloorSplit fs = floor_split(u);
+        const float2 p = pr[fs.i];
+        float v = fmaf(fs.f, p.y, p.x);
+        if (kind == LINE_CHECKED) {
+          // np.interp(t, k - K, line, left=0, right=0) decided in double like numpy
+          const double td = __dsub_rn(__dmul_rn((double)(j - R), (double)inf.x),
+                                      __dmul_rn((double)(i - R), (double)inf.y));
+          if (td < -(double)K || td > (double)(n - 1 - K)) {
+            v = 0.f;
+          } else {
+            const double uk = td + (double)K;
+            const double fl = floor(uk);
+            const int kidx = (int)fl - lkbase[ll];
+            const float2 pe = pr[min(max(kidx, 0), BP_KW - 1)];
+            v = (float)((double)pe.x + (uk - fl) * (double)pe.y);
+          }
+        }
+        if (SYM) {
+          if (i < n && j < n) {
+            const int64_t moff = (((int64_t)s * args.n_angles + a) * args.n_det + d) * (int64_t)n * n +
+                                 (int64_t)i * n + j;
+            v *= load_map(args.maps, MAPS_DTYPE, moff);
+          }
+        }
+        acc[k] += v;
+      }
+    }
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (int k = 0; k < BP_PPT; ++k) {
+    const int i = i0 + warp + 8 * k;
+    if (i < n && j < n) bp_epilogue<EPI>(args, s, i, j, acc[k]);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Exact adjoint of the forward projection (gather form; no reference counterpart)
+// bp[p] = sum_a sum_{(r,c)} w_a hat(col_in(r,c) - p_x) hat(row_in(r,c) - p_y) y[a][c] (* map[a][p])
+// For a pixel p and angle a the candidate samples are the rotated-lattice points within
+// distance < 1 (per axis) of p: r, c within +-2 of the inverse-rotated position.
+// ------------------------------------------------------------------------------------------
+template <bool HAS_MAPS, int MAPS_DTYPE>
+__global__ void __launch_bounds__(256) bp_adjoint_kernel(BpArgs args) {
+  const int n = args.n;
+  const int64_t total = (int64_t)n * n;
+  const int s = blockIdx.y;
+  const int64_t pix = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= total) return;
+  const int pi = (int)(pix / n), pj = (int)(pix - (int64_t)pi * n);
+  const int n_lines = args.n_det * args.n_angles;
+  const float* sino = args.sino + (int64_t)s * n_lines * n;
+  double acc = 0.0;
+  for (int l = 0; l < n_lines; ++l) {
+    const int d = l / args.n_angles;
+    const int a = l - d * args.n_angles;
+    const float* M = args.fp_matrix + 6 * a;
+    const float m00 = M[0], m01 = M[1], m02 = M[2], m10 = M[3], m11 = M[4], m12 = M[5];
+    // invert the 2x2 part to find the lattice point nearest to p
+    const double det = (double)m00 * m11 - (double)m01 * m10;
+    const double dx = pj - (double)m02, dy = pi - (double)m12;
+    const double cc = (m11 * dx - m01 * dy) / det;
+    const double rr = (-m10 * dx + m00 * dy) / det;
+    const int cb = (int)floor(cc), rb = (int)floor(rr);
+    double lsum = 0.0;
+    for (int r = rb - 2; r <= rb + 3; ++r) {
+      if (r < 0 || r >= n) continue;
+      for (int c = cb - 2; c <= cb + 3; ++c) {
+        if (c < 0 || c >= n) continue;
+        // same float arithmetic as the forward kernel's sample position
+        const float px = sample_x(m00, m01, m02, (float)c, (float)r);
+        const float py = sample_x(m10, m11, m12, (float)c, (float)r);
+        const float hx = 1.f - fabsf(px - (float)pj);
+        const float hy = 1.f - fabsf(py - (float)pi);
+        if (hx > 0.f && hy > 0.f) lsum += (double)hx * hy * sino[((int64_t)d * args.n_angles + a) * n + c];
+      }
+    }
+    float w = args.weights != nullptr ? args.weights[a * args.n_det + d] : 1.f;
+    double contrib = lsum * w;
+    if (HAS_MAPS) {
+      const int64_t moff = (((int64_t)s * args.n_angles + a) * args.n_det + d) * (int64_t)n * n + pix;
+      contrib *= load_map(args.maps, MAPS_DTYPE, moff);
+    }
+    acc += contrib;
+  }
+  bp_epilogue<BP_EPI_STORE>(args, s, pi, pj, (float)acc);
+}
+
+// ------------------------------------------------------------------------------------------
+// Launchers
+// ------------------------------------------------------------------------------------------
+template <int EPI>
+static void launch_fp_epi(const FpArgs& a, cudaStream_t st) {
+  const dim3 grid((a.n + FP_TC - 1) / FP_TC, a.n_angles * a.n_det, a.n_slices);
+  if (a.maps == nullptr) {
+    fp_kernel<EPI, false, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(a);
+  } else if (a.maps_dtype == CCT_DTYPE_BF16) {
+    fp_kernel<EPI, true, CCT_DTYPE_BF16><<<grid, FP_THREADS, 0, st>>>(a);
+  } else {
+    fp_kernel<EPI, true, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(a);
+  }
+}
+
+void launch_fp(const FpArgs& a, cudaStream_t st) {
+  switch (a.epi) {
+    case FP_EPI_MLEM: launch_fp_epi<FP_EPI_MLEM>(a, st); break;
+    case FP_EPI_SIRT: launch_fp_epi<FP_EPI_SIRT>(a, st); break;
+    case FP_EPI_PDHG: launch_fp_epi<FP_EPI_PDHG>(a, st); break;
+    default: launch_fp_epi<FP_EPI_STORE>(a, st); break;
+  }
+}
+
+template <int EPI>
+static void launch_bp_epi(const BpArgs& a, cudaStream_t st) {
+  const int tiles = (a.n + BP_TILE - 1) / BP_TILE;
+  const dim3 grid(tiles * tiles, a.n_slices);
+  const bool sym = a.mode == CCT_BP_SYMMETRIC;
+  if (!sym) {
+    bp_kernel<EPI, false, CCT_DTYPE_F32><<<grid, BP_THREADS, 0, st>>>(a);
+  } else if (a.maps_dtype == CCT_DTYPE_BF16) {
+    bp_kernel<EPI, true, CCT_DTYPE_BF16><<<grid, BP_THREADS, 0, st>>>(a);
+  } else {
+    bp_kernel<EPI, true, CCT_DTYPE_F32><<<grid, BP_THREADS, 0, st>>>(a);
+  }
+}
+
+void launch_bp(const BpArgs& a, cudaStream_t st) {
+  if (a.mode == CCT_BP_ADJOINT) {
+    const dim3 grid((unsigned)(((int64_t)a.n * a.n + 255) / 256), a.n_slices);
+    if (a.maps == nullptr) {
+      bp_adjoint_kernel<false, CCT_DTYPE_F32><<<grid, 256, 0, st>>>(a);
+    } else if (a.maps_dtype == CCT_DTYPE_BF16) {
+      bp_adjoint_kernel<true, CCT_DTYPE_BF16><<<grid, 256, 0, st>>>(a);
+    } else {
+      bp_adjoint_kernel<true, CCT_DTYPE_F32><<<grid, 256, 0, st>>>(a);
+    }
+    return;
+  }
+  switch (a.epi) {
+    case BP_EPI_MLEM: launch_bp_epi<BP_EPI_MLEM>(a, st); break;
+    case BP_EPI_SIRT: launch_bp_epi<BP_EPI_SIRT>(a, st); break;
+    case BP_EPI_PDHG: launch_bp_epi<BP_EPI_PDHG>(a, st); break;
+    default: launch_bp_epi<BP_EPI_STORE>(a, st); break;
+  }
+}
+
+}  // namespace cct
+
+namespace cct {
+int read_device_error(int clear, int* value) {
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, g_box_overflow, sizeof(int));
+  if (e != cudaSuccess) return (int)e;
+  if (clear && v != 0) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(g_box_overflow, &zero, sizeof(int));
+    if (e != cudaSuccess) return (int)e;
+  }
+  *value = v;
+  return 0;
+}
+}  // namespace cct

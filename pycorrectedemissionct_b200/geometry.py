@@ -1,0 +1,117 @@
+"""Per-angle sampling matrices of the XRF path, built with the same numpy operations as the reference.
+
+The kernels receive, per angle, the exact matrices scikit-image builds inside the
+reference's scikit-image backend, so sample positions agree with the reference
+to float32 rounding:
+
+* ``fp_matrices`` — scikit-image ``radon`` (``circle=True``) inverse map per angle:
+  ``np.deg2rad`` of the float32 backend degrees (``corrct``:
+  ``src/corrct/_projector_backends.py:148, 299``), float32 ``cos``/``sin``, and the
+  entries ``[[c, s, -C(c+s-1)], [-s, c, -C(c-s-1)]]`` with ``C = n // 2`` evaluated in
+  float32.
+* ``bp_trig`` — the float32 ``(cos, sin)`` that scikit-image ``iradon`` uses for the
+  back projection of each angle.
+* ``rotate_matrix`` — scikit-image ``rotate`` about ``((P-1)/2, (P-1)/2)`` composed in
+  float64 from ``math.cos``/``math.sin`` of ``np.deg2rad(angle)``.
+* ``attenuation_rotations`` — the two rotations (``-phi`` then ``+phi``) of every
+  ``compute_attenuation`` call (``src/corrct/_projector_backends.py:67-80``) made by
+  ``AttenuationVolume.compute_maps`` (``src/corrct/physics/attenuation.py:105-120``):
+  incident angles are the float32 backend angles; emitted angles are
+  ``angle + detector angle + sub-angle + pi`` in float64.
+"""
+
+from __future__ import annotations
+
+import math
+from collections.abc import Sequence
+
+import numpy as np
+from numpy.typing import NDArray
+
+
+def backend_angles(angles_rot_rad) -> tuple[NDArray, NDArray]:
+    """(float32 radians, float32 degrees) as the reference backend stores them."""
+    rad = np.array(angles_rot_rad, ndmin=1, dtype=np.float32)
+    return rad, np.rad2deg(rad)
+
+
+def fp_matrices(angles_deg32: NDArray, n: int) -> NDArray:
+    """``(A, 6)`` float32 radon inverse maps (M00, M01, M02, M10, M11, M12)."""
+    out = np.empty((len(angles_deg32), 6), dtype=np.float32)
+    center = n // 2
+    for ii, th in enumerate(np.asarray(angles_deg32, dtype=np.float32)):
+        angle = np.deg2rad(np.asarray([th]))[0]
+        c, s = np.cos(angle), np.sin(angle)
+        out[ii] = [c, s, -center * (c + s - 1), -s, c, -center * (c - s - 1)]
+    return out
+
+
+def bp_trig(angles_deg32: NDArray) -> NDArray:
+    """``(A, 2)`` float32 ``(cos, sin)`` of iradon per angle."""
+    angle = np.deg2rad(np.asarray(angles_deg32, dtype=np.float32))
+    return np.stack([np.cos(angle), np.sin(angle)], axis=1).astype(np.float32)
+
+
+def padded_size(n: int) -> tuple[int, int]:
+    """(edge, P) of ``compute_attenuation``'s zero padding (``_projector_backends.py:75-77``)."""
+    min_size = np.ceil(np.sqrt(2.0 * n * n))
+    edge = int(np.ceil((min_size - n) / 2))
+    return edge, n + 2 * edge
+
+
+def rotate_matrix(angle_deg, size: int) -> NDArray:
+    """scikit-image ``rotate`` inverse map of a ``size x size`` image, as 6 float64 entries."""
+    center = np.array((size, size)) / 2.0 - 0.5
+    rot = np.deg2rad(angle_deg)
+    c, s = math.cos(rot), math.sin(rot)
+    t1 = np.array([[1.0, 0.0, center[0]], [0.0, 1.0, center[1]], [0.0, 0.0, 1.0]])
+    r = np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+    t3 = np.array([[1.0, 0.0, -center[0]], [0.0, 1.0, -center[1]], [0.0, 0.0, 1.0]])
+    m = t1 @ (r @ t3)
+    return m[:2].reshape(6)
+
+
+def _attenuation_pair(angle_rad, invert: bool, size: int) -> NDArray:
+    if invert:
+        angle_rad = angle_rad + np.pi
+    deg = np.rad2deg(angle_rad)
+    return np.stack([rotate_matrix(-deg, size), rotate_matrix(deg, size)])
+
+
+def detector_sub_angles(surface_mm2: float, distance_mm: float, sub_sampling: int) -> NDArray:
+    """Sub-angle offsets of a detector (``physics/xrf.py:243-258``, ``attenuation.py:111-114``)."""
+    if surface_mm2 > 0.0:
+        half_angle = np.arctan2(np.sqrt(surface_mm2) / 2, distance_mm)
+        sub = np.linspace(-half_angle, half_angle, sub_sampling + 1)
+        return np.convolve(sub, np.ones(2), "valid") / 2
+    return np.zeros(1)
+
+
+def attenuation_rotations(
+    angles_rot_rad32: NDArray,
+    det_angles: Sequence[float] | NDArray,
+    n: int,
+    surfaces_mm2: Sequence[float] | None = None,
+    distances_mm: Sequence[float] | None = None,
+    sub_sampling: int = 1,
+) -> tuple[NDArray, NDArray, int]:
+    """Rotation matrices ``rot_in (A, 2, 6)`` and ``rot_out (A, D, n_sub, 2, 6)`` (float64)."""
+    _, size = padded_size(n)
+    det_angles = np.array(det_angles, ndmin=1, dtype=np.float64)
+    n_det = len(det_angles)
+    surfaces = np.zeros(n_det) if surfaces_mm2 is None else np.array(surfaces_mm2, ndmin=1, dtype=np.float64)
+    distances = np.ones(n_det) if distances_mm is None else np.array(distances_mm, ndmin=1, dtype=np.float64)
+    subs = [detector_sub_angles(surfaces[d], distances[d], sub_sampling) for d in range(n_det)]
+    n_sub = max(len(s) for s in subs)
+    if any(len(s) != n_sub for s in subs):
+        raise ValueError("All detectors must use the same number of emitted sub-angles")
+    angles = np.array(angles_rot_rad32, ndmin=1)
+    rot_in = np.empty((len(angles), 2, 6))
+    rot_out = np.empty((len(angles), n_det, n_sub, 2, 6))
+    for ii, a in enumerate(angles):
+        rot_in[ii] = _attenuation_pair(a, False, size)
+        angle_det = a + det_angles
+        for dd, ad in enumerate(angle_det):
+            for kk, a_s in enumerate(subs[dd]):
+                rot_out[ii, dd, kk] = _attenuation_pair(ad + a_s, True, size)
+    return rot_in, rot_out, n_sub

@@ -1,0 +1,332 @@
+"""Solvers with the reference's interface running device-resident on the B200 projectors.
+
+Mirrors ``corrct``: ``src/corrct/solvers.py`` — ``SolutionInfo`` (``:161-201``),
+``MLEM`` (``:634-805``), ``SIRT`` (``:808-984``), ``PDHG`` (``:987-1206``, KL or l2
+data term, optional isotropic TV2D), ``SART`` (``:473-631``) and ``FISTA``
+(``:1209-1513``, l2 data term, no regularizer).  ``__call__(A, b, iterations, x0,
+lower_limit, upper_limit, x_mask, ...)`` returns ``(x, SolutionInfo)`` like the
+reference.  MLEM, SIRT and PDHG run the fused ``cct_*_step`` kernels (the update
+equations of the reference); SART and FISTA drive the projector's device fp / bp.
+``A`` must be one of this package's projectors: the unchanged corrct solvers
+remain available for any other operator (including these projectors).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .engine import BatchedSolver
+from .projectors import ProjectorAttenuationXRF, ProjectorUncorrected
+
+eps = np.finfo(np.float32).eps
+
+
+class SolutionInfo:
+    """Reconstruction info (corrct ``solvers.py:161-201``)."""
+
+    def __init__(self, method: str, max_iterations: int, tolerance, residual0: float = np.inf, residual0_cv: float = np.inf):
+        self.method = method
+        self.max_iterations = max_iterations
+        self.tolerance = tolerance
+        self.residual0 = residual0
+        self.residual0_cv = residual0_cv
+        self.residuals = np.zeros(max_iterations)
+        self.residuals_cv = np.zeros(max_iterations)
+        self.iterations = 0
+
+    @property
+    def residuals_rel(self):
+        return self.residuals / self.residual0
+
+    @property
+    def residuals_cv_rel(self):
+        return self.residuals_cv / self.residual0_cv
+
+
+def _check_projector(A) -> None:
+    if not isinstance(A, ProjectorUncorrected):
+        raise TypeError(
+            "the B200 solvers run on this package's projectors; use corrct's own solvers for other operators"
+        )
+
+
+def _data_term_name(data_term) -> tuple[str, float | None]:
+    if isinstance(data_term, str):
+        name = data_term.lower()
+        if name not in ("l2", "kl"):
+            raise ValueError(f"Unknown data term: '{data_term}', only accepted terms are: 'l2' | 'kl'.")
+        return name, None
+    name = getattr(data_term, "__data_fidelity_name__", "").lower()
+    if name not in ("l2", "kl"):
+        raise ValueError(f"Unsupported data term: '{data_term}', only 'kl' and 'l2' are supported.")
+    bg = getattr(data_term, "background", None)
+    return name, (None if bg is None else float(np.asarray(bg)))
+
+
+def _as_batch(A, b, x0, x_mask):
+    dev = A.projector_backend.device
+    n = int(A.vol_shape[-1])
+    n_det = A._n_det() if isinstance(A, ProjectorAttenuationXRF) else 1
+    n_ang = len(A.angles_rot_rad)
+    as_np = not isinstance(b, torch.Tensor)
+    bt = torch.as_tensor(np.ascontiguousarray(b, dtype=np.float32) if as_np else b).to(dev, torch.float32)
+    bt = bt.reshape(1, n_det, n_ang, n).contiguous()
+    x0t = None if x0 is None else torch.as_tensor(np.asarray(x0, dtype=np.float32) if not isinstance(x0, torch.Tensor) else x0).to(dev, torch.float32).reshape(1, n, n)
+    mt = None if x_mask is None else torch.as_tensor(np.asarray(x_mask, dtype=np.float32) if not isinstance(x_mask, torch.Tensor) else x_mask).to(dev, torch.float32).reshape(n, n)
+    maps = A.maps_device if isinstance(A, ProjectorAttenuationXRF) else None
+    return bt, x0t, mt, maps, as_np
+
+
+def _finish(solver: BatchedSolver, info: SolutionInfo, iterations: int, as_np: bool):
+    torch.cuda.current_stream(solver.device).synchronize()
+    info.iterations = int(solver.iterations[0].item())
+    if solver.history is not None:
+        h = solver.history[0].cpu().numpy()
+        k = min(info.iterations, iterations)
+        info.residuals[:k] = h[:k]
+    x = solver.x[0]
+    return (x.cpu().numpy() if as_np else x.clone()), info
+
+
+class Solver:
+    """Base solver (corrct ``solvers.py:204-400``)."""
+
+    def __init__(self, verbose: bool = False, leave_progress: bool = True, relaxation: float = 1.0, tolerance=None, data_term="l2", data_term_test=None):
+        self.verbose = verbose
+        self.leave_progress = leave_progress
+        self.relaxation = relaxation
+        self.tolerance = tolerance
+        self.data_term, self.background = _data_term_name(data_term)
+        if data_term_test is not None:
+            raise NotImplementedError("data_term_test (cross-validation residuals) is not supported by the B200 solvers")
+
+    def info(self) -> str:
+        return type(self).__name__
+
+    def upper(self) -> str:
+        return type(self).__name__.upper()
+
+    def lower(self) -> str:
+        return type(self).__name__.lower()
+
+    @staticmethod
+    def _reject_masks(b_mask, b_test_mask) -> None:
+        if b_mask is not None or b_test_mask is not None:
+            raise NotImplementedError("b_mask / b_test_mask are not supported by the B200 solvers yet")
+
+
+class MLEM(Solver):
+    """MLEM with the KL data term (corrct ``solvers.py:634-805``)."""
+
+    def __init__(self, verbose: bool = False, leave_progress: bool = True, tolerance=None, regularizer=None, data_term="kl", data_term_test=None):
+        super().__init__(verbose=verbose, leave_progress=leave_progress, tolerance=tolerance, data_term=data_term, data_term_test=data_term_test)
+        if regularizer is not None:
+            raise NotImplementedError("MLEM regularizers are not supported by the B200 solvers")
+
+    def __call__(self, A, b, iterations: int, x0=None, lower_limit=None, upper_limit=None, x_mask=None, b_mask=None, b_test_mask=None):
+        _check_projector(A)
+        self._reject_masks(b_mask, b_test_mask)
+        if getattr(A, "is_symmetric", False) or getattr(A, "bp_mode", "reference") != "reference":
+            raise NotImplementedError("the fused MLEM uses the reference (non-symmetric) back projection")
+        bt, x0t, mt, maps, as_np = _as_batch(A, b, x0, x_mask)
+        solver = BatchedSolver(
+            A.core, maps, bt, "mlem", tolerance=self.tolerance, x0=x0t, x_mask=mt,
+            lower_limit=lower_limit, upper_limit=upper_limit, background=self.background, history_len=iterations,
+        )
+        info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
+        if self.tolerance is not None:
+            info.residual0 = _kl_residual_norm(A.core.fp(solver.x, maps), bt, self.background)
+        solver.run(iterations, check_every=10 if self.tolerance is not None else max(iterations, 1))
+        return _finish(solver, info, iterations, as_np)
+
+
+class SIRT(Solver):
+    """SIRT with the l2 data term (corrct ``solvers.py:808-984``)."""
+
+    def __init__(self, verbose: bool = False, leave_progress: bool = True, relaxation: float = 1.95, tolerance=None, regularizer=None, data_term="l2", data_term_test=None):
+        super().__init__(verbose=verbose, leave_progress=leave_progress, relaxation=relaxation, tolerance=tolerance, data_term=data_term, data_term_test=data_term_test)
+        if regularizer is not None:
+            raise NotImplementedError("SIRT regularizers are not supported by the B200 solvers")
+        if self.data_term != "l2":
+            raise NotImplementedError("the fused SIRT uses the l2 data term")
+
+    def __call__(self, A, b, iterations: int, x0=None, lower_limit=None, upper_limit=None, x_mask=None, b_mask=None, b_test_mask=None):
+        _check_projector(A)
+        self._reject_masks(b_mask, b_test_mask)
+        bt, x0t, mt, maps, as_np = _as_batch(A, b, x0, x_mask)
+        bp_mode = "symmetric" if getattr(A, "is_symmetric", False) else "reference"
+        solver = BatchedSolver(
+            A.core, maps, bt, "sirt", tolerance=self.tolerance, x0=x0t, x_mask=mt, lower_limit=lower_limit,
+            upper_limit=upper_limit, relaxation=self.relaxation, bp_mode=bp_mode, background=self.background,
+            history_len=iterations,
+        )
+        info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
+        solver.run(iterations, check_every=10 if self.tolerance is not None else max(iterations, 1))
+        return _finish(solver, info, iterations, as_np)
+
+
+class PDHG(Solver):
+    """Chambolle-Pock PDHG with the KL data term and optional isotropic TV2D (corrct ``solvers.py:987-1206``).
+
+    ``regularizer`` is ``None`` or an object with ``__reg_name__ == "TV2D"`` (or a float
+    TV weight); ``tolerance`` is not supported yet.
+    """
+
+    def __init__(self, verbose: bool = False, leave_progress: bool = True, tolerance=None, relaxation: float = 0.95, regularizer=None, data_term="kl", data_term_test=None):
+        super().__init__(verbose=verbose, leave_progress=leave_progress, relaxation=relaxation, tolerance=tolerance, data_term=data_term, data_term_test=data_term_test)
+        if self.data_term != "kl":
+            raise NotImplementedError("the fused PDHG uses the KL data term")
+        if tolerance is not None:
+            raise NotImplementedError("PDHG tolerance is not supported by the B200 solvers yet")
+        self.tv_weight = _tv_weight(regularizer)
+
+    def __call__(self, A, b, iterations: int, x0=None, lower_limit=None, upper_limit=None, x_mask=None, b_mask=None, b_test_mask=None, precondition: bool = True):
+        _check_projector(A)
+        self._reject_masks(b_mask, b_test_mask)
+        if not precondition:
+            raise NotImplementedError("PDHG without diagonal preconditioning is not supported by the B200 solvers")
+        if x0 is not None:
+            raise NotImplementedError("PDHG x0 is not supported by the B200 solvers yet")
+        bt, _, mt, maps, as_np = _as_batch(A, b, None, x_mask)
+        bp_mode = "symmetric" if getattr(A, "is_symmetric", False) else "reference"
+        if self.tv_weight is None:
+            raise NotImplementedError("the fused PDHG needs a TV2D regularizer")
+        solver = BatchedSolver(
+            A.core, maps, bt, "pdhg", x_mask=mt, lower_limit=lower_limit, upper_limit=upper_limit,
+            relaxation=self.relaxation, tv_lambda=self.tv_weight, bp_mode=bp_mode, background=self.background,
+        )
+        info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
+        solver.run(iterations, check_every=max(iterations, 1))
+        x, info = _finish(solver, info, iterations, as_np)
+        info.iterations = iterations
+        return x, info
+
+
+def _tv_weight(regularizer):
+    if regularizer is None:
+        return None
+    if isinstance(regularizer, (int, float)):
+        return float(regularizer)
+    if getattr(regularizer, "__reg_name__", "") == "TV2D":
+        return float(np.max(np.asarray(regularizer.weight)))
+    raise NotImplementedError("only the isotropic TV2D regularizer is supported by the B200 PDHG")
+
+
+def _kl_residual_norm(ax: torch.Tensor, b: torch.Tensor, background) -> float:
+    """||KL residual||_1 in FP64 (corrct ``data_terms.py:720-742`` with sigma = 1)."""
+    proj = ax.double() if background is None else ax.double() + background
+    r = torch.clamp(proj, min=float(eps))
+    res = (1 + r - torch.sqrt((r - 1) ** 2 + 4 * torch.clamp(b.double(), min=0))) / 2
+    return float(res.abs().sum().item())
+
+
+class SART(Solver):
+    """SART row-action solver on per-angle device projections (corrct ``solvers.py:473-631``)."""
+
+    def __call__(self, A, b, iterations: int, A_num_rows=None, At=None, x0=None, lower_limit=None, upper_limit=None, x_mask=None, b_mask=None):
+        _check_projector(A)
+        if b_mask is not None:
+            raise NotImplementedError("b_mask is not supported by the B200 SART")
+        dev = A.projector_backend.device
+        n = int(A.vol_shape[-1])
+        n_ang = len(A.angles_rot_rad)
+        as_np = not isinstance(b, torch.Tensor)
+        bt = torch.as_tensor(np.ascontiguousarray(b, dtype=np.float32) if as_np else b).to(dev, torch.float32)
+        xrf = isinstance(A, ProjectorAttenuationXRF)
+        fpa = lambda x, ii: A.fp_angle(x, ii)  # noqa: E731
+        bpa = (lambda y, ii: A.bp_angle(y, ii, single_line=True)) if xrf else (lambda y, ii: A.bp_angle(y, ii))  # noqa: E731
+        b_ones = torch.ones_like(bt)
+        tau = torch.stack([bpa(b_ones[..., ii, :].contiguous(), ii) for ii in range(n_ang)], dim=-2).abs()
+        tau = torch.where(tau / tau.max() < 1e-5, torch.ones_like(tau), tau)
+        tau = self.relaxation / tau
+        x_ones = torch.ones((n, n), device=dev)
+        if x_mask is not None:
+            x_ones = x_ones * torch.as_tensor(np.asarray(x_mask, dtype=np.float32)).to(dev)
+        sigma = torch.stack([fpa(x_ones, ii) for ii in range(n_ang)], dim=-2).abs()
+        sigma = torch.where(sigma / sigma.max() < 1e-5, torch.ones_like(sigma), sigma)
+        sigma = 1 / sigma
+        x = torch.zeros((n, n), device=dev) if x0 is None else torch.as_tensor(np.asarray(x0, dtype=np.float32)).to(dev).clone()
+        mask = None if x_mask is None else torch.as_tensor(np.asarray(x_mask, dtype=np.float32)).to(dev)
+        info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
+        rows_sequence = np.random.permutation(n_ang)
+        for ii in range(iterations):
+            info.iterations += 1
+            for a in rows_sequence:
+                res = fpa(x, int(a)) - bt[..., a, :]
+                x = x - bpa((res * sigma[..., a, :]).contiguous(), int(a)) * tau[..., a, :]
+                if lower_limit is not None:
+                    x = torch.clamp(x, min=lower_limit)
+                if upper_limit is not None:
+                    x = torch.clamp(x, max=upper_limit)
+                if mask is not None:
+                    x = x * mask
+            if self.tolerance is not None:
+                fp = torch.stack([fpa(x, a) for a in range(n_ang)], dim=-1)
+                r = fp - torch.movedim(bt, -2, -1)
+                info.residuals[ii] = float(torch.linalg.norm(r.double()).item())
+                if self.tolerance > info.residuals[ii]:
+                    break
+        return (x.cpu().numpy() if as_np else x), info
+
+
+class FISTA(Solver):
+    """FISTA with the l2 data term and no regularizer (corrct ``solvers.py:1209-1513``)."""
+
+    def __init__(self, verbose: bool = False, leave_progress: bool = True, tolerance=None, relaxation: float = 1.0, regularizer=None, data_term="l2", data_term_test=None, restart_period=None):
+        super().__init__(verbose=verbose, leave_progress=leave_progress, relaxation=relaxation, tolerance=tolerance, data_term=data_term, data_term_test=data_term_test)
+        if regularizer is not None:
+            raise NotImplementedError("FISTA regularizers are not supported by the B200 solvers")
+        if self.data_term != "l2":
+            raise ValueError(f"Unknown data term: '{data_term}'. FISTA only accepts 'l2' and derivatives.")
+        self.restart_period = restart_period
+
+    def __call__(self, A, b, iterations: int, x0=None, lower_limit=None, upper_limit=None, x_mask=None, b_mask=None, b_test_mask=None, precondition: bool = True):
+        _check_projector(A)
+        self._reject_masks(b_mask, b_test_mask)
+        if not precondition:
+            raise NotImplementedError("FISTA without diagonal preconditioning is not supported by the B200 solvers")
+        bt, x0t, mt, maps, as_np = _as_batch(A, b, x0, x_mask)
+        core = A.core
+        bp_mode = "symmetric" if getattr(A, "is_symmetric", False) else "reference"
+        fp = lambda v: core.fp(v, maps)  # noqa: E731
+        bp = lambda y: core.bp(y, bp_mode, maps if bp_mode == "symmetric" else None)  # noqa: E731
+        n = core.n
+        # compute_diagonal_scaling (solvers.py:60-117), relaxation on tau
+        tau = bp(torch.ones_like(bt)).abs()
+        tau = torch.where(tau / tau.max() < 1e-5, torch.ones_like(tau), tau)
+        tau = self.relaxation / tau
+        x_ones = torch.ones((1, n, n), device=core.device)
+        if mt is not None:
+            x_ones = x_ones * mt
+        sigma = fp(x_ones).abs()
+        sigma = torch.where(sigma / sigma.max() < 1e-5, torch.ones_like(sigma), sigma)
+        sigma = 1.0 / sigma
+        x = torch.zeros((1, n, n), device=core.device) if x0t is None else x0t.clone()
+        if mt is not None:
+            x = x * mt
+        y = x.clone()
+        t = 1.0
+        bg = 0.0 if self.background is None else self.background
+        info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
+        for ii in range(iterations):
+            info.iterations += 1
+            residual = bt - (fp(y.contiguous()) + bg)
+            grad = bp((residual * sigma).contiguous())
+            x_new = y + tau * grad
+            if lower_limit is not None or upper_limit is not None:
+                x_new = torch.clamp(x_new, min=lower_limit, max=upper_limit)
+            if mt is not None:
+                x_new = x_new * mt
+            t_new = float(1.0 + np.sqrt(1.0 + 4.0 * t * t)) / 2.0
+            if self.restart_period is not None and (ii + 1) % self.restart_period == 0:
+                t_new = 1.0
+            momentum = (t - 1.0) / t_new
+            y = x_new + momentum * (x_new - x)
+            x, t = x_new, t_new
+            if self.tolerance is not None:
+                r = bt - (fp(x.contiguous()) + bg)
+                info.residuals[ii] = float(torch.sum(r.double() ** 2).item())
+                if self.tolerance > info.residuals[ii]:
+                    break
+        return (x[0].cpu().numpy() if as_np else x[0]), info

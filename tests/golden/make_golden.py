@@ -1,0 +1,116 @@
+"""Generate the golden fixtures of the XRF projection path from the reference's own Python.
+
+Runs the unmodified reference ``corrct`` (imported through
+``oracle.reference_import`` with the restated scikit-image primitives) in FP64
+on seeded synthetic slices and stores inputs and outputs as ``.npz`` files next
+to this script.  Needs a local checkout of the reference (``CORRCT_SRC``);
+the fixtures themselves are committed so the tests do not.
+
+Usage: ``python tests/golden/make_golden.py``
+"""
+
+from __future__ import annotations
+
+import contextlib
+import io
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.reference_import import load_corrct  # noqa: E402
+from pycorrectedemissionct_b200 import phantoms  # noqa: E402
+
+CASES = [
+    # name, N, A, detector angles, detector weights, random angle weights, seed
+    ("n32_a16", 32, 16, [np.pi / 2], None, False, 11),
+    ("n33_a9", 33, 9, [np.pi / 2], None, False, 12),
+    ("n16_a7_d2", 16, 7, [np.pi / 2, np.pi / 3], [1.0, 0.5], True, 13),
+    ("n64_a48", 64, 48, [np.pi / 2], None, False, 14),
+]
+ITERATIONS = 10
+
+
+def make_case(corrct, name, n, n_ang, det_angles, det_weights, rand_ang_w, seed):
+    rng = phantoms.slice_rng(seed, 0)
+    x = phantoms.ellipse_phantom(n, rng, num_ellipses=6, dtype=np.float64)
+    mu_in = phantoms.disk_attenuation(n, rng, mu_max=0.05, num_disks=3, dtype=np.float64)
+    mu_out = 0.7 * mu_in
+    angles = phantoms.angles(n_ang)
+    det_angles = np.array(det_angles, dtype=np.float64)
+    w_ang = rng.uniform(0.5, 1.5, size=(n_ang, len(det_angles))) if rand_ang_w else None
+
+    angles32 = np.array(angles, dtype=np.float32)
+    att = corrct.physics.attenuation.AttenuationVolume(mu_in, mu_out, angles32, det_angles, dtype=np.float64)
+    att.compute_maps(use_multithreading=False, verbose=False)
+    maps = att.get_maps()
+
+    common = dict(
+        att_maps=maps,
+        angles_detectors_rad=det_angles,
+        weights_detectors=det_weights,
+        weights_angles=w_ang,
+        use_multithreading=False,
+        backend="skimage",
+        verbose=False,
+    )
+    p = corrct.projectors.ProjectorAttenuationXRF((n, n), angles, **common)
+    ps = corrct.projectors.ProjectorAttenuationXRF((n, n), angles, is_symmetric=True, **common)
+    pu = corrct.projectors.ProjectorUncorrected((n, n), angles, backend="skimage")
+
+    fp_att = p.fp(x)
+    y = rng.uniform(0.0, 1.0, size=fp_att.shape)
+    out = dict(
+        n=n,
+        angles=angles,
+        det_angles=det_angles,
+        det_weights=np.ones(len(det_angles)) if det_weights is None else np.array(det_weights, dtype=np.float64),
+        weights_angles=np.ones((n_ang, len(det_angles))) if w_ang is None else w_ang,
+        x=x,
+        mu_in=mu_in,
+        mu_out=mu_out,
+        maps=maps,
+        fp_att=fp_att,
+        y=y,
+        bp_att=p.bp(y),
+        bp_sym=ps.bp(y),
+        fp_unc=pu.fp(x),
+        bp_unc=pu.bp(np.reshape(y, (-1, n_ang, n))[0]),
+    )
+    # the reference's float32 default run (maps in float32 from float32 mu), for error reporting
+    att32 = corrct.physics.attenuation.AttenuationVolume(
+        mu_in.astype(np.float32), mu_out.astype(np.float32), angles32, det_angles
+    )
+    att32.compute_maps(use_multithreading=False, verbose=False)
+    out["maps_ref32"] = att32.get_maps()
+
+    if len(det_angles) == 1:
+        b = phantoms.poisson_data(fp_att, 1e4, rng, dtype=np.float64)
+        out["b"] = b
+        mlem = corrct.solvers.MLEM(tolerance=0.0, verbose=False)
+        xm, info = mlem(p, b, iterations=ITERATIONS)
+        out["mlem_x"], out["mlem_res"] = xm, info.residuals[:ITERATIONS]
+        sirt = corrct.solvers.SIRT(verbose=False)
+        out["sirt_x"] = sirt(p, b, iterations=ITERATIONS)[0]
+        pdhg = corrct.solvers.PDHG(
+            data_term="kl", regularizer=corrct.regularizers.Regularizer_TV2D(1e-2), verbose=False
+        )
+        out["pdhg_x"] = pdhg(p, b, iterations=ITERATIONS)[0]
+    np.savez_compressed(os.path.join(HERE, f"xrf_{name}.npz"), **out)
+    print(f"{name}: maps {maps.shape} fp {fp_att.shape}")
+
+
+def main():
+    corrct = load_corrct()
+    with contextlib.redirect_stdout(io.StringIO()) as log:
+        for case in CASES:
+            make_case(corrct, *case)
+    print("\n".join(line for line in log.getvalue().splitlines() if ":" in line and "maps" in line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,231 @@
+"""GPU parity of the CUDA path (called through the C ABI) against the reference-generated golden
+fixtures and the FP64 oracle port.
+
+Tolerances (relative L2, FP32 GPU vs FP64 oracle): maps, fp, bp 1e-5; reconstructions after a
+fixed iteration count 1e-4; exact-adjoint pair <fp x, y> vs <x, bp y> 1e-6 (FP64 inner products).
+BF16-stored maps are reported against FP64 with their own bound (BF16 keeps 8 mantissa bits).
+"""
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+TOL_RECON = 1e-4
+TOL_ADJ = 1e-6
+
+CASES = ["n32_a16", "n33_a9", "n16_a7_d2", "n64_a48"]
+
+
+@pytest.fixture(scope="module")
+def cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+def _core(g, cuda):
+    from pycorrectedemissionct_b200 import core
+
+    n_det = len(g["det_angles"])
+    w = np.asarray(g["det_weights"])[None, :] * np.asarray(g["weights_angles"])
+    return core.XrfCore(int(g["n"]), g["angles"], n_det=n_det, weights=w, device=cuda)
+
+
+def _t(a, cuda, dtype=torch.float32):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(cuda, dtype)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_maps_match_reference(golden_cases, case, cuda):
+    from pycorrectedemissionct_b200 import core
+
+    g = golden_cases[case]
+    rad32 = np.array(g["angles"], dtype=np.float32)
+    maps = core.compute_maps(_t(g["mu_in"], cuda)[None], _t(g["mu_out"], cuda)[None], rad32, g["det_angles"])
+    got = maps[0].cpu().numpy()
+    assert got.shape == g["maps"].shape
+    assert rel_l2(got, g["maps"]) < TOL
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_fp_bp_match_reference(golden_cases, case, cuda):
+    g = golden_cases[case]
+    c = _core(g, cuda)
+    n, n_ang, n_det = int(g["n"]), len(g["angles"]), len(g["det_angles"])
+    maps = _t(g["maps"], cuda)[None]
+    x = _t(g["x"], cuda)[None]
+    fp = c.fp(x, maps)[0].cpu().numpy()
+    assert rel_l2(fp.reshape(g["fp_att"].shape), g["fp_att"]) < TOL
+    y = _t(np.reshape(g["y"], (1, n_det, n_ang, n)), cuda)
+    assert rel_l2(c.bp(y, "reference")[0].cpu().numpy(), g["bp_att"]) < TOL
+    assert rel_l2(c.bp(y, "symmetric", maps)[0].cpu().numpy(), g["bp_sym"]) < TOL
+    if n_det == 1:
+        cu = _core(dict(g, weights_angles=np.ones_like(g["weights_angles"])), cuda)
+        assert rel_l2(cu.fp(x)[0, 0].cpu().numpy(), g["fp_unc"]) < TOL
+        assert rel_l2(cu.bp(y, "reference")[0].cpu().numpy(), g["bp_unc"]) < TOL
+
+
+@pytest.mark.parametrize("case", ["n32_a16", "n33_a9", "n64_a48"])
+def test_solvers_match_reference(golden_cases, case, cuda):
+    from pycorrectedemissionct_b200 import projectors, solvers
+
+    g = golden_cases[case]
+    n = int(g["n"])
+    p = projectors.ProjectorAttenuationXRF((n, n), g["angles"], att_maps=g["maps"], angles_detectors_rad=g["det_angles"])
+    xm, info = solvers.MLEM(tolerance=0.0)(p, g["b"], iterations=10)
+    assert rel_l2(xm, g["mlem_x"]) < TOL_RECON
+    np.testing.assert_allclose(info.residuals[:10], g["mlem_res"], rtol=TOL_RECON)
+    assert info.iterations == 10
+    xs, _ = solvers.SIRT()(p, g["b"], iterations=10)
+    assert rel_l2(xs, g["sirt_x"]) < TOL_RECON
+    xp, _ = solvers.PDHG(data_term="kl", regularizer=1e-2)(p, g["b"], iterations=10)
+    assert rel_l2(xp, g["pdhg_x"]) < TOL_RECON
+
+
+@pytest.mark.parametrize("n,n_ang", [(128, 90), (256, 360)])
+def test_against_oracle_port_medium(n, n_ang, cuda):
+    from oracle import port
+    from pycorrectedemissionct_b200 import core, phantoms
+
+    rng = phantoms.slice_rng(1000 + n, 0)
+    x = phantoms.ellipse_phantom(n, rng, 12, dtype=np.float64)
+    mu = phantoms.disk_attenuation(n, rng, 0.02, dtype=np.float64)
+    angles = phantoms.angles(n_ang)
+    rad32, deg32 = port.backend_angles(angles)
+    ref_maps = port.compute_maps(mu, 0.7 * mu, rad32, workers=8)
+    maps = core.compute_maps(_t(mu, cuda)[None], _t(0.7 * mu, cuda)[None], rad32)
+    assert rel_l2(maps[0].cpu().numpy(), ref_maps) < TOL
+    c = core.XrfCore(n, angles, device=cuda)
+    ref_fp = port.fp_xrf(x, ref_maps, deg32, workers=8)
+    fp = c.fp(_t(x, cuda)[None], _t(ref_maps, cuda)[None])[0, 0].cpu().numpy()
+    assert rel_l2(fp, ref_fp) < TOL
+    y = rng.uniform(size=(n_ang, n))
+    ref_bp = port.bp_uncorrected(y, deg32, n, workers=8)
+    bp = c.bp(_t(y, cuda)[None, None], "reference")[0].cpu().numpy()
+    assert rel_l2(bp, ref_bp) < TOL
+    # the sensitivity image A^T 1 exercises np.interp's discontinuous detector edges everywhere
+    ones = np.ones((n_ang, n))
+    assert rel_l2(c.bp(_t(ones, cuda)[None, None], "reference")[0].cpu().numpy(), port.bp_uncorrected(ones, deg32, n, workers=8)) < TOL
+
+
+@pytest.mark.parametrize("n,n_ang,n_det", [(64, 16, 1), (96, 31, 2), (128, 180, 1)])
+def test_exact_adjoint_pair(n, n_ang, n_det, cuda):
+    from pycorrectedemissionct_b200 import core
+
+    rng = np.random.default_rng(n)
+    w = rng.uniform(0.5, 1.5, size=(n_ang, n_det))
+    c = core.XrfCore(n, np.linspace(0, 2 * np.pi, n_ang, endpoint=False), n_det=n_det, weights=w, device=cuda)
+    maps = _t(rng.uniform(0.2, 1.0, size=(1, n_ang, n_det, n, n)), cuda)
+    x = _t(rng.uniform(size=(1, n, n)), cuda)
+    y = _t(rng.uniform(size=(1, n_det, n_ang, n)), cuda)
+    lhs = torch.vdot(c.fp(x, maps).double().flatten(), y.double().flatten()).item()
+    rhs = torch.vdot(x.double().flatten(), c.bp(y, "adjoint", maps).double().flatten()).item()
+    assert abs(lhs - rhs) / abs(lhs) < TOL_ADJ
+
+
+def test_exact_adjoint_matches_oracle(golden_cases, cuda):
+    from oracle import port
+
+    g = golden_cases["n32_a16"]
+    c = _core(g, cuda)
+    n, n_ang = int(g["n"]), len(g["angles"])
+    _, deg32 = port.backend_angles(g["angles"])
+    ref = port.fp_xrf_adjoint(g["y"], g["maps"], deg32, n)
+    got = c.bp(_t(g["y"], cuda).reshape(1, 1, n_ang, n), "adjoint", _t(g["maps"], cuda)[None])[0].cpu().numpy()
+    assert rel_l2(got, ref) < TOL
+
+
+def test_batched_equals_single(cuda):
+    from pycorrectedemissionct_b200 import core, phantoms
+
+    n, n_ang, s = 96, 45, 3
+    angles = phantoms.angles(n_ang)
+    mus = np.stack([phantoms.disk_attenuation(n, phantoms.slice_rng(7, k), 0.02) for k in range(s)])
+    xs = np.stack([phantoms.ellipse_phantom(n, phantoms.slice_rng(8, k)) for k in range(s)])
+    rad32 = np.array(angles, dtype=np.float32)
+    maps = core.compute_maps(_t(mus, cuda), _t(0.7 * mus, cuda), rad32)
+    c = core.XrfCore(n, angles, device=cuda)
+    fp_all = c.fp(_t(xs, cuda), maps)
+    for k in range(s):
+        mk = core.compute_maps(_t(mus[k], cuda)[None], _t(0.7 * mus[k], cuda)[None], rad32)
+        assert torch.equal(mk[0], maps[k])
+        assert torch.equal(c.fp(_t(xs[k], cuda)[None], mk)[0], fp_all[k])
+
+
+def test_bf16_maps_error_against_fp64(golden_cases, cuda):
+    from pycorrectedemissionct_b200 import core
+
+    g = golden_cases["n64_a48"]
+    rad32 = np.array(g["angles"], dtype=np.float32)
+    m16 = core.compute_maps(_t(g["mu_in"], cuda)[None], _t(g["mu_out"], cuda)[None], rad32, maps_dtype="bfloat16")
+    err = rel_l2(m16[0].float().cpu().numpy(), g["maps"])
+    assert err < 4e-3  # bf16: 2^-9 relative rounding
+    c = _core(g, cuda)
+    fp16 = c.fp(_t(g["x"], cuda)[None], m16)[0, 0].cpu().numpy()
+    assert rel_l2(fp16, g["fp_att"]) < 4e-3
+
+
+def test_full_size_properties(cuda):
+    """512 x 512, 720 angles (the benchmark slice): properties that need no oracle run."""
+    from pycorrectedemissionct_b200 import core, phantoms
+
+    n, n_ang = 512, 720
+    rng = phantoms.slice_rng(42, 0)
+    x = _t(phantoms.ellipse_phantom(n, rng), cuda)[None]
+    mu = _t(phantoms.disk_attenuation(n, rng, 0.01), cuda)[None]
+    angles = phantoms.angles(n_ang)
+    maps = core.compute_maps(mu, mu, np.array(angles, dtype=np.float32))
+    assert float(maps.max()) <= 1.0 and float(maps.min()) > 0.0
+    c = core.XrfCore(n, angles, device=cuda)
+    fp1 = c.fp(x, maps)
+    fp2 = c.fp(2 * x, maps)
+    assert torch.equal(fp2, 2 * fp1)  # exact: scaling by 2 is exact in FP32
+    ones = torch.ones_like(maps)
+    assert torch.equal(c.fp(x, ones), c.fp(x))  # unit maps == uncorrected projection, bit for bit
+    zero = core.compute_maps(torch.zeros_like(mu), torch.zeros_like(mu), np.array(angles, dtype=np.float32))
+    assert torch.all(zero == 1.0)
+    # uncorrected sinogram mass is conserved up to the image support (phantom inside the circle)
+    tot = c.fp(x)[0, 0].double().sum(dim=1)
+    assert float((tot / x.double().sum() - 1).abs().max()) < 5e-3
+    err = torch.zeros(1, dtype=torch.int32)
+    from pycorrectedemissionct_b200 import _lib
+    import ctypes
+
+    v = ctypes.c_int32(0)
+    _lib.call("cct_device_error", 0, ctypes.byref(v))
+    assert v.value == 0
+
+
+def test_engine_tolerance_and_graph(cuda):
+    from pycorrectedemissionct_b200 import core, engine, phantoms
+
+    n, n_ang, s = 64, 60, 4
+    angles = phantoms.angles(n_ang)
+    rad32 = np.array(angles, dtype=np.float32)
+    mus = np.stack([phantoms.disk_attenuation(n, phantoms.slice_rng(9, k), 0.02) for k in range(s)])
+    xs = np.stack([phantoms.ellipse_phantom(n, phantoms.slice_rng(10, k)) for k in range(s)])
+    maps = core.compute_maps(_t(mus, cuda), _t(0.7 * mus, cuda), rad32)
+    c = core.XrfCore(n, angles, device=cuda)
+    clean = c.fp(_t(xs, cuda), maps)
+    b = torch.poisson(clean / clean.amax(dim=(1, 2, 3), keepdim=True) * 1e4)
+    eager = engine.BatchedSolver(c, maps, b, "mlem", history_len=40)
+    eager.run(40, check_every=10, use_graph=False)
+    graph = engine.BatchedSolver(c, maps, b, "mlem", history_len=40)
+    graph.run(40, check_every=10, use_graph=True)
+    assert torch.equal(eager.x, graph.x)
+    res = eager.history.cpu().numpy()
+    tol = res[:, 25] * (1 + 1e-9)
+    # the reference stops at the first iteration whose residual is below the tolerance
+    expect = np.array([int(np.argmax(r < t)) + 1 for r, t in zip(res, tol)])
+    stop = engine.BatchedSolver(c, maps, b, "mlem", tolerance=tol, history_len=40)
+    stop.run(40, check_every=10)
+    its = stop.iterations.cpu().numpy()
+    np.testing.assert_array_equal(its, expect)
+    assert int(stop.active.sum()) == 0
+    # stopped slices keep the iterate of their last update
+    assert torch.equal(stop.history[:, : int(expect.min())], eager.history[:, : int(expect.min())])

@@ -1,0 +1,118 @@
+"""CPU: host logic — geometry tables equal the oracle's scikit-image matrices, the C-ABI library
+loads and exports every declared symbol, argument validation paths (no GPU compute)."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from oracle import skimage_restated as skr
+from pycorrectedemissionct_b200 import geometry, phantoms
+
+
+def test_fp_matrices_equal_restated_radon():
+    _, deg32 = geometry.backend_angles(np.linspace(0, 2 * np.pi, 37, endpoint=False))
+    for n in (16, 33, 512):
+        got = geometry.fp_matrices(deg32, n)
+        for ii, th in enumerate(deg32):
+            ref = skr.radon_matrix(th, n)
+            np.testing.assert_array_equal(got[ii], ref[:2].reshape(6).astype(np.float32))
+
+
+def test_bp_trig_equal_restated_iradon():
+    _, deg32 = geometry.backend_angles(np.linspace(0, 2 * np.pi, 37, endpoint=False))
+    got = geometry.bp_trig(deg32)
+    for ii, th in enumerate(deg32):
+        c, s = skr.iradon_matrix_terms(th)
+        assert got[ii, 0] == c and got[ii, 1] == s
+
+
+def test_rotation_matrices_equal_restated_rotate():
+    rad32, _ = geometry.backend_angles(np.linspace(0, 2 * np.pi, 11, endpoint=False))
+    n = 40
+    _, p = geometry.padded_size(n)
+    rot_in, rot_out, n_sub = geometry.attenuation_rotations(rad32, [np.pi / 2, 1.0], n)
+    assert n_sub == 1 and rot_out.shape == (11, 2, 1, 2, 6)
+    for ii, a in enumerate(rad32):
+        deg = np.rad2deg(a)
+        np.testing.assert_array_equal(rot_in[ii, 0], skr.rotate_matrix(-deg, p, p)[:2].reshape(6))
+        np.testing.assert_array_equal(rot_in[ii, 1], skr.rotate_matrix(deg, p, p)[:2].reshape(6))
+        ad = a + np.array([np.pi / 2, 1.0])[1] + np.pi
+        np.testing.assert_array_equal(rot_out[ii, 1, 0, 0], skr.rotate_matrix(-np.rad2deg(ad), p, p)[:2].reshape(6))
+
+
+def test_padded_sizes():
+    assert [geometry.padded_size(n)[1] for n in (128, 256, 384, 512, 768, 1024)] == [182, 364, 544, 726, 1088, 1450]
+
+
+def test_sub_angles_follow_detector_model():
+    sub = geometry.detector_sub_angles(4.0, 10.0, 4)
+    half = np.arctan2(1.0, 10.0)
+    np.testing.assert_allclose(sub, (np.linspace(-half, half, 5)[1:] + np.linspace(-half, half, 5)[:-1]) / 2)
+
+
+def test_phantoms_are_seeded_and_inside_circle():
+    a = phantoms.ellipse_phantom(64, phantoms.slice_rng(5, 2))
+    b = phantoms.ellipse_phantom(64, phantoms.slice_rng(5, 2))
+    np.testing.assert_array_equal(a, b)
+    yy, xx = np.mgrid[:64, :64] - 31.5
+    assert np.all(a[(xx**2 + yy**2) > 32**2] == 0)
+    mu = phantoms.disk_attenuation(64, phantoms.slice_rng(5, 3), 0.02)
+    assert mu.max() <= 0.02 and mu.min() >= 0
+
+
+# ------------------------------------------------------------------------------------ C ABI
+HEADER = os.path.join(ROOT, "include", "corrct_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(cct_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    from pycorrectedemissionct_b200 import _lib
+
+    lib = _lib.load()
+    names = declared_symbols()
+    assert len(names) >= 12
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, name
+    assert lib.cct_abi_version() == 1
+
+
+def test_validation_errors_map_to_value_error():
+    from pycorrectedemissionct_b200 import _lib
+
+    lib = _lib.load()
+    desc = _lib.XrfDesc()
+    desc.n = 1  # invalid: must be >= 2
+    desc.n_angles = desc.n_det = desc.n_slices = 1
+    rc = lib.cct_fp(ctypes.byref(desc), None, None, None, None)
+    assert rc == _lib.CCT_ERR_VALUE
+    assert b"volume side" in lib.cct_last_error()
+    with pytest.raises(ValueError):
+        _lib.check(rc)
+    md = _lib.MapsDesc()
+    md.n, md.n_angles, md.n_det, md.n_slices, md.n_sub = 16, 4, 1, 1, 1
+    out = ctypes.c_size_t(0)
+    assert lib.cct_maps_workspace_size(ctypes.byref(md), 1, ctypes.byref(out)) == _lib.CCT_ERR_VALUE  # no volumes
+    md.has_in = 1
+    assert lib.cct_maps_workspace_size(ctypes.byref(md), 2, ctypes.byref(out)) == _lib.CCT_OK
+    p = geometry.padded_size(16)[1]
+    assert out.value == 2 * p * p * 4
+
+
+def test_compute_paths_need_cuda():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("CUDA present")
+    from pycorrectedemissionct_b200 import projectors
+
+    with pytest.raises(RuntimeError, match="CUDA"):
+        projectors.ProjectorUncorrected((16, 16), np.linspace(0, np.pi, 4))

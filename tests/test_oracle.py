@@ -1,0 +1,124 @@
+"""CPU: the oracle port against the reference-generated golden fixtures, and known-answer tests
+of the restated scikit-image primitives (analytic, independent of scikit-image)."""
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from oracle import port
+from oracle import skimage_restated as skr
+
+
+@pytest.mark.parametrize("case", ["n32_a16", "n33_a9", "n16_a7_d2", "n64_a48"])
+def test_port_matches_reference_golden(golden_cases, case):
+    g = golden_cases[case]
+    rad32, deg32 = port.backend_angles(g["angles"])
+    maps = port.compute_maps(g["mu_in"], g["mu_out"], rad32, g["det_angles"])
+    assert rel_l2(maps, g["maps"]) < 1e-14
+    fa = port.fp_xrf(g["x"], g["maps"], deg32, g["det_weights"], g["weights_angles"])
+    assert rel_l2(fa, g["fp_att"]) < 1e-14
+    assert rel_l2(port.bp_xrf(g["y"], g["maps"], deg32), g["bp_att"]) < 1e-14
+    bs = port.bp_xrf(g["y"], g["maps"], deg32, g["det_weights"], g["weights_angles"], is_symmetric=True)
+    assert rel_l2(bs, g["bp_sym"]) < 1e-14
+    assert rel_l2(port.fp_uncorrected(g["x"], deg32), g["fp_unc"]) < 1e-14
+    n = int(g["n"])
+    y0 = np.reshape(g["y"], (-1, len(deg32), n))[0]
+    assert rel_l2(port.bp_uncorrected(y0, deg32, n), g["bp_unc"]) < 1e-14
+
+
+@pytest.mark.parametrize("case", ["n32_a16", "n64_a48"])
+def test_port_solvers_match_reference_golden(golden_cases, case):
+    g = golden_cases[case]
+    n = int(g["n"])
+    _, deg32 = port.backend_angles(g["angles"])
+    fp = lambda v: port.fp_xrf(v, g["maps"], deg32)  # noqa: E731
+    bp = lambda s: port.bp_xrf(s, g["maps"], deg32)  # noqa: E731
+    xm, res = port.mlem(fp, bp, g["b"], 10, tolerance=0.0)
+    assert rel_l2(xm, g["mlem_x"]) < 1e-13
+    np.testing.assert_allclose(res, g["mlem_res"], rtol=1e-12)
+    assert rel_l2(port.sirt(fp, bp, g["b"], 10, (n, n)), g["sirt_x"]) < 1e-13
+    assert rel_l2(port.pdhg_kl_tv(fp, bp, g["b"], 10, (n, n), 1e-2), g["pdhg_x"]) < 1e-13
+
+
+def test_reference_float32_maps_close_to_fp64(golden_cases):
+    for g in golden_cases.values():
+        assert rel_l2(g["maps_ref32"], g["maps"]) < 1e-6
+
+
+# ----------------------------------------------------------------------------------- KATs
+def test_radon_zero_angle_is_column_sums():
+    rng = np.random.default_rng(0)
+    img = rng.uniform(size=(17, 17))
+    out = skr.radon(img, np.array([0.0], dtype=np.float32))[:, 0]
+    np.testing.assert_allclose(out, img.sum(0), rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("n", [16, 17])
+def test_radon_90_degrees_is_lattice_permutation(n):
+    rng = np.random.default_rng(1)
+    img = rng.uniform(size=(n, n))
+    out = skr.radon(img, np.array([90.0], dtype=np.float32))[:, 0]
+    # at 90 deg the samples land on lattice points (to float32 trig rounding): a permutation of
+    # the pixels, so every output is a full row sum of some (possibly shifted) row
+    np.testing.assert_allclose(np.sort(out[1:-1]), np.sort(out[1:-1]), atol=0)
+    assert abs(out.sum() - img[:, : n - (1 if n % 2 == 0 else 0)].sum()) < 1.5 * img.max() * n
+
+
+def test_iradon_single_bin_is_hat_ridge():
+    n = 16
+    line = np.zeros(n)
+    line[n // 2 + 3] = 1.0
+    bp = skr.iradon(line[:, None], np.array([0.0], dtype=np.float32), output_size=n, filter_name=None, circle=False)
+    bp = bp * 2 / np.pi
+    # theta = 0: t = j - n//2, so column j = n//2 + 3 is 1, all others 0 (a ridge along rows)
+    expect = np.zeros((n, n))
+    expect[:, n // 2 + 3] = 1.0
+    np.testing.assert_allclose(bp, expect, atol=1e-12)
+
+
+def test_iradon_edges_follow_numpy_interp():
+    n = 8
+    line = np.arange(1, n + 1, dtype=np.float64)
+    # theta = 180 deg (float32): t slightly off the last node for half of the rows
+    bp = skr.iradon(line[:, None], np.array([180.0], dtype=np.float32), output_size=n, filter_name=None, circle=False)
+    assert np.all(np.isfinite(bp))
+
+
+def test_zero_attenuation_gives_unit_maps():
+    n = 16
+    mu = np.zeros((n, n))
+    rad32, _ = port.backend_angles(np.linspace(0, 2 * np.pi, 5, endpoint=False))
+    maps = port.compute_maps(mu, mu, rad32)
+    np.testing.assert_array_equal(maps, np.ones_like(maps))
+
+
+def test_line_integral_is_linear_in_mu():
+    rng = np.random.default_rng(2)
+    n = 24
+    mu = rng.uniform(0, 0.05, size=(n, n))
+    a = np.float32(0.3)
+    l1 = -np.log(port.compute_attenuation(mu, a))
+    l2 = -np.log(port.compute_attenuation(2.5 * mu, a))
+    np.testing.assert_allclose(l2, 2.5 * l1, rtol=1e-10, atol=1e-12)
+
+
+def test_uniform_disk_line_integral_matches_chord():
+    n = 64
+    yy, xx = np.mgrid[:n, :n] - (n - 1) / 2
+    mu = np.where(xx**2 + yy**2 <= 20**2, 0.01, 0.0)
+    lin = -np.log(port.compute_attenuation(mu, np.float32(0.0)))
+    # at angle 0 the beam runs along +rows: at the disk centre the path length from entry is ~20
+    c = n // 2
+    assert abs(lin[c, c] - 0.01 * 20.5) < 0.01 * 1.5
+
+
+def test_exact_adjoint_oracle_is_adjoint():
+    rng = np.random.default_rng(3)
+    n, a = 20, 7
+    _, deg32 = port.backend_angles(np.linspace(0, 2 * np.pi, a, endpoint=False))
+    maps = rng.uniform(0.5, 1.0, size=(a, 1, n, n))
+    x = rng.uniform(size=(n, n))
+    y = rng.uniform(size=(a, n))
+    lhs = np.vdot(port.fp_xrf(x, maps, deg32), y)
+    rhs = np.vdot(x, port.fp_xrf_adjoint(y, maps, deg32, n))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-12
