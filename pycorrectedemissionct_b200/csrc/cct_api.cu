@@ -226,6 +226,7 @@ int cct_pdhg_step(const cct_xrf_desc* desc, const void* maps, int32_t bp_mode, c
   if (rc != CCT_OK) return rc;
   CCT_REQUIRE(st->sigma != nullptr && st->x_relax != nullptr && st->tv_dual != nullptr,
               "PDHG needs sigma, x_relax and tv_dual");
+  CCT_REQUIRE(st->vol_buf != nullptr, "PDHG needs vol_buf");
   CCT_REQUIRE(bp_mode == CCT_BP_REFERENCE || bp_mode == CCT_BP_SYMMETRIC, "PDHG bp_mode must be REFERENCE or SYMMETRIC");
   CCT_REQUIRE(bp_mode != CCT_BP_SYMMETRIC || maps != nullptr, "the symmetric back projection needs maps");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

@@ -36,19 +36,59 @@ __device__ int g_box_overflow = 0;
 constexpr int FP_TC = 64;                          // detector bins per CTA
 constexpr int FP_TR = 64;                          // rows per staged chunk
 constexpr int FP_THREADS = 256;
-constexpr int FP_RGROUPS = FP_THREADS / FP_TC;     // 4 row groups
-constexpr int FP_RPT = FP_TR / FP_RGROUPS;         // 16 rows per thread per chunk
-// Rotated 64x64 chunk: extent <= 64*sqrt(2) = 90.6, +1/+2 tap margins, +3 for float4
+// Lanes of a warp cover an 8 (columns) x 4 (rows) block of samples: 32 points of a rotated
+// lattice patch spread over ~2 wavefronts per shared load at any angle, where a 32 x 1 line
+// of lanes hits 32-way bank conflicts at some angles.  Warp w owns columns 8w..8w+7.
+constexpr int FP_LC = 8;
+constexpr int FP_LR = 4;
+constexpr int FP_RPT = FP_TR / FP_LR;              // 16 samples per thread per chunk
+// Rotated 64x64 chunk: extent <= 63*sqrt(2) = 89.1, +1/+2 tap margins, +3 for float4
 // alignment of the left edge, rounded up to a multiple of 4.
 constexpr int FP_BOX_W = 100;
 constexpr int FP_BOX_H = 96;
-constexpr int FP_STRIDE = FP_BOX_W + 1;            // odd stride: conflict-free steep-angle lanes
+constexpr int FP_STRIDE = FP_BOX_W;                // 16-byte rows: conflict-free float4 fills
+constexpr int FP_FILL_BATCH = 4;                   // float4 items whose loads are issued together
+
+template <bool HAS_MAPS, int MAPS_DTYPE>
+__device__ __forceinline__ float4 fp_load_item(const float* vol, const void* maps, int64_t map_off, int n, int gy,
+                                               int gx, bool vec4) {
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (gy < 0 || gy >= n || gx + 3 < 0 || gx >= n) return v;
+  const int off = gy * n + gx;  // < 2^31 for n <= 8192... n*n <= 2^26
+  if (vec4 && gx >= 0 && gx + 3 < n) {
+    v = __ldg(reinterpret_cast<const float4*>(vol + off));
+    if (HAS_MAPS) {
+      if (MAPS_DTYPE == CCT_DTYPE_BF16) {
+        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(
+            reinterpret_cast<const __nv_bfloat16*>(maps) + map_off + off));
+        const float2 flo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.x));
+        const float2 fhi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.y));
+        v.x *= flo.x; v.y *= flo.y; v.z *= fhi.x; v.w *= fhi.y;
+      } else {
+        const float4 mv = __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const float*>(maps) + map_off + off));
+        v.x *= mv.x; v.y *= mv.y; v.z *= mv.z; v.w *= mv.w;
+      }
+    }
+    return v;
+  }
+  float e[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int xx = gx + k;
+    float val = 0.f;
+    if (xx >= 0 && xx < n) {
+      val = __ldg(vol + off + k);
+      if (HAS_MAPS) val *= load_map(maps, MAPS_DTYPE, map_off + off + k);
+    }
+    e[k] = val;
+  }
+  return make_float4(e[0], e[1], e[2], e[3]);
+}
 
 template <int EPI, bool HAS_MAPS, int MAPS_DTYPE>
 __global__ void __launch_bounds__(FP_THREADS) fp_kernel(FpArgs args) {
-  __shared__ float z[FP_BOX_H * FP_STRIDE];
-  __shared__ float red[FP_THREADS];
-  __shared__ double red_d[FP_TC / 32];
+  __shared__ __align__(16) float z[FP_BOX_H * FP_STRIDE];
+  __shared__ double red_d[FP_TC / FP_LC];
 
   const int n = args.n;
   const int band = blockIdx.x;
@@ -64,15 +104,18 @@ __global__ void __launch_bounds__(FP_THREADS) fp_kernel(FpArgs args) {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  const int cl = tid & (FP_TC - 1);
-  const int rg = tid / FP_TC;
+  const int lc = lane & (FP_LC - 1);
+  const int lr = lane / FP_LC;
   const int c0 = band * FP_TC;
-  const int c = c0 + cl;
+  const int c = c0 + warp * FP_LC + lc;
   const int c_last = min(c0 + FP_TC, n) - 1;
 
   const float* vol = args.vol + (int64_t)s * n * n;
   const int64_t map_off = (((int64_t)s * args.n_angles + a) * args.n_det + d) * (int64_t)n * n;
   const bool vec4 = (n & 3) == 0;
+  const float fc = (float)c;
+  const float pxc = fmaf(m00, fc, m02);
+  const float pyc = fmaf(m10, fc, m12);
 
   float acc = 0.f;
   for (int r0 = 0; r0 < n; r0 += FP_TR) {
@@ -85,11 +128,10 @@ __global__ void __launch_bounds__(FP_THREADS) fp_kernel(FpArgs args) {
     const float yc = sample_x(m10, m11, m12, fc0, fr1), yd = sample_x(m10, m11, m12, fc1, fr1);
     const float xmin = fminf(fminf(xa, xb), fminf(xc, xd)), xmax = fmaxf(fmaxf(xa, xb), fmaxf(xc, xd));
     const float ymin = fminf(fminf(ya, yb), fminf(yc, yd)), ymax = fmaxf(fmaxf(ya, yb), fmaxf(yc, yd));
-    int bx0 = (int)floorf(xmin) - 1;
+    const int bx0 = ((int)floorf(xmin) - 1) & ~3;  // floor to a multiple of 4 (two's complement)
     const int bx1 = (int)floorf(xmax) + 2;
     const int by0 = (int)floorf(ymin) - 1;
     const int by1 = (int)floorf(ymax) + 2;
-    bx0 &= ~3;  // floor to a multiple of 4 (two's complement) for aligned float4 loads
     const int q4 = (bx1 - bx0) / 4 + 1;  // float4 columns
     const int bh = by1 - by0 + 1;
     if (4 * q4 > FP_BOX_W || bh > FP_BOX_H) {  // cannot happen for valid matrices; never trap
@@ -97,97 +139,113 @@ __global__ void __launch_bounds__(FP_THREADS) fp_kernel(FpArgs args) {
       return;
     }
 
-    // Stage z = vol * map over the box (zeros outside the image).
-    for (int rr = warp; rr < bh; rr += FP_THREADS / 32) {
-      const int gy = by0 + rr;
-      const bool row_in = gy >= 0 && gy < n;
-      for (int q = lane; q < q4; q += 32) {
-        const int gx = bx0 + 4 * q;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (row_in) {
-          const int64_t off = (int64_t)gy * n + gx;
-          if (vec4 && gx >= 0 && gx + 3 < n) {
-            v = __ldg(reinterpret_cast<const float4*>(vol + off));
-            if (HAS_MAPS) {
-              if (MAPS_DTYPE == CCT_DTYPE_BF16) {
-                const uint2 raw = __ldg(reinterpret_cast<const uint2*>(
-                    reinterpret_cast<const __nv_bfloat16*>(args.maps) + map_off + off));
-                const __nv_bfloat162 lo = *reinterpret_cast<const __nv_bfloat162*>(&raw.x);
-                const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162*>(&raw.y);
-                const float2 flo = __bfloat1622float2(lo), fhi = __bfloat1622float2(hi);
-                v.x *= flo.x; v.y *= flo.y; v.z *= fhi.x; v.w *= fhi.y;
-              } else {
-                const float4 mv = __ldg(reinterpret_cast<const float4*>(
-                    reinterpret_cast<const float*>(args.maps) + map_off + off));
-                v.x *= mv.x; v.y *= mv.y; v.z *= mv.z; v.w *= mv.w;
-              }
-            }
-          } else if (!vec4 || (gx + 3 >= 0 && gx < n)) {
-            float e[4];
+    // Stage z = vol * map over the box (zeros outside the image); every thread takes items
+    // tid, tid + 256, ... of the q4 x bh grid, issuing FP_FILL_BATCH items' loads at once.
+    const int items = q4 * bh;
+    // it / q4 as a multiply-high: with it < 2^12 and q4 <= 25 the rounding error of
+    // ceil(2^32 / q4) stays below 2^-15 and never reaches the next integer
+    const unsigned magic = (unsigned)((0x100000000ull + (unsigned)q4 - 1) / (unsigned)q4);
+    for (int base = tid; base < items; base += FP_THREADS * FP_FILL_BATCH) {
+      float4 v[FP_FILL_BATCH];
+      int dst[FP_FILL_BATCH];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-              const int xx = gx + k;
-              float val = 0.f;
-              if (xx >= 0 && xx < n) {
-                val = __ldg(vol + off + k);
-                if (HAS_MAPS) val *= load_map(args.maps, MAPS_DTYPE, map_off + off + k);
+      for (int k = 0; k < FP_FILL_BATCH; ++k) {
+        const int it = base + k * FP_THREADS;
+        dst[k] = -1;
+        v[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (it < items) {
+          const int rr = (int)__umulhi((unsigned)it, magic);
+          const int qq = it - rr * q4;
+          const int gy = by0 + rr, gx = bx0 + 4 * qq;
+          dst[k] = rr * FP_STRIDE + 4 * qq;
+          if (vec4) {
+            // n % 4 == 0 and gx % 4 == 0: a float4 is either fully inside or fully outside
+            if ((unsigned)gy < (unsigned)n && (unsigned)gx < (unsigned)n) {
+              const int off = gy * n + gx;
+              v[k] = __ldg(reinterpret_cast<const float4*>(vol + off));
+              if (HAS_MAPS) {
+                if (MAPS_DTYPE == CCT_DTYPE_BF16) {
+                  const uint2 raw = __ldg(reinterpret_cast<const uint2*>(
+                      reinterpret_cast<const __nv_bfloat16*>(args.maps) + map_off + off));
+                  const float2 flo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.x));
+                  const float2 fhi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.y));
+                  v[k].x *= flo.x; v[k].y *= flo.y; v[k].z *= fhi.x; v[k].w *= fhi.y;
+                } else {
+                  const float4 mv = __ldg(reinterpret_cast<const float4*>(
+                      reinterpret_cast<const float*>(args.maps) + map_off + off));
+                  v[k].x *= mv.x; v[k].y *= mv.y; v[k].z *= mv.z; v[k].w *= mv.w;
+                }
               }
-              e[k] = val;
             }
-            v = make_float4(e[0], e[1], e[2], e[3]);
+          } else {
+            v[k] = fp_load_item<HAS_MAPS, MAPS_DTYPE>(vol, args.maps, map_off, n, gy, gx, false);
           }
         }
-        float* dst = z + rr * FP_STRIDE + 4 * q;
-        dst[0] = v.x; dst[1] = v.y; dst[2] = v.z; dst[3] = v.w;
+      }
+#pragma unroll
+      for (int k = 0; k < FP_FILL_BATCH; ++k) {
+        if (dst[k] >= 0) *reinterpret_cast<float4*>(z + dst[k]) = v[k];
       }
     }
     __syncthreads();
 
     if (c <= c_last) {
-      const int rb = r0 + rg * FP_RPT;
-      const int re = min(rb + FP_RPT, r_last + 1);
-      // Sample positions use exactly sample_x()'s expression so that the adjoint
-      // kernel (and the box corners) see bit-identical coordinates.
-      const float fc = (float)c;
-      const float pxc = fmaf(m00, fc, m02);
-      const float pyc = fmaf(m10, fc, m12);
-      const float* zb = z - by0 * FP_STRIDE - bx0;
-      float fr = (float)rb;
+      // Sample positions use exactly sample_x()'s expression so that the adjoint kernel (and
+      // the box corners) see bit-identical coordinates.  Taps index the __shared__ array with
+      // 32-bit offsets (zoff moves the box origin to (by0, bx0)).
+      const int zoff = -by0 * FP_STRIDE - bx0;
+      float fr = (float)(r0 + lr);
+      const int rem = r_last - r0 - lr;                      // rows of this thread left in the chunk
+      const int kmax = rem >= 0 ? rem / FP_LR + 1 : 0;       // samples of this thread in the chunk
+      if (kmax >= FP_RPT) {
 #pragma unroll 4
-      for (int r = rb; r < re; ++r) {
-        const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
-        const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
-        const float* p = zb + fy.i * FP_STRIDE + fx.i;
-        const float t0 = p[0], t1 = p[1], b0 = p[FP_STRIDE], b1 = p[FP_STRIDE + 1];
-        const float top = fmaf(fx.f, t1 - t0, t0);
-        const float bot = fmaf(fx.f, b1 - b0, b0);
-        acc += fmaf(fy.f, bot - top, top);
-        fr += 1.f;
+        for (int k = 0; k < FP_RPT; ++k) {
+          const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
+          const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
+          const int q = fy.i * FP_STRIDE + fx.i + zoff;
+          const float t0 = z[q], t1 = z[q + 1], b0 = z[q + FP_STRIDE], b1 = z[q + FP_STRIDE + 1];
+          const float top = fmaf(fx.f, t1 - t0, t0);
+          const float bot = fmaf(fx.f, b1 - b0, b0);
+          acc += fmaf(fy.f, bot - top, top);
+          fr += (float)FP_LR;
+        }
+      } else {
+        for (int k = 0; k < kmax; ++k) {
+          const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
+          const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
+          const int q = fy.i * FP_STRIDE + fx.i + zoff;
+          const float t0 = z[q], t1 = z[q + 1], b0 = z[q + FP_STRIDE], b1 = z[q + FP_STRIDE + 1];
+          const float top = fmaf(fx.f, t1 - t0, t0);
+          const float bot = fmaf(fx.f, b1 - b0, b0);
+          acc += fmaf(fy.f, bot - top, top);
+          fr += (float)FP_LR;
+        }
       }
     }
     __syncthreads();
   }
 
-  red[tid] = acc;
-  __syncthreads();
-  if (rg == 0) {
-    double part = 0.0;
-    if (c <= c_last) {
-      float total = red[cl] + red[cl + FP_TC] + red[cl + 2 * FP_TC] + red[cl + 3 * FP_TC];
-      if (args.weights != nullptr) total *= args.weights[a * args.n_det + d];
-      const int64_t idx = (((int64_t)s * args.n_det + d) * args.n_angles + a) * n + c;
-      part = fp_epilogue<EPI>(args, idx, total);
-    }
-    if (EPI != FP_EPI_STORE) {
-      part = warp_sum_double(part);
-      if (lane == 0) red_d[warp] = part;
-    }
+  // column sum over the 4 row-lanes of the 8x4 lane block (lanes lc, lc+8, lc+16, lc+24)
+  acc += __shfl_xor_sync(0xffffffffu, acc, 8);
+  acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+  double part = 0.0;
+  if (lr == 0 && c <= c_last) {
+    float total = acc;
+    if (args.weights != nullptr) total *= args.weights[a * args.n_det + d];
+    const int64_t idx = (((int64_t)s * args.n_det + d) * args.n_angles + a) * n + c;
+    part = fp_epilogue<EPI>(args, idx, total);
   }
-  if (EPI != FP_EPI_STORE) {
+  // only the MLEM and SIRT epilogues produce residual partials (PDHG passes none)
+  if (EPI == FP_EPI_MLEM || EPI == FP_EPI_SIRT) {
+    part = warp_sum_double(part);
+    if (lane == 0) red_d[warp] = part;
     __syncthreads();
     if (tid == 0) {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < FP_TC / FP_LC; ++w) t += red_d[w];
       const int64_t per_slice = (int64_t)gridDim.x * gridDim.y;
-      args.partials[(int64_t)s * per_slice + (int64_t)blockIdx.y * gridDim.x + blockIdx.x] = red_d[0] + red_d[1];
+      args.partials[(int64_t)s * per_slice + (int64_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
     }
   }
 }
@@ -195,18 +253,19 @@ __global__ void __launch_bounds__(FP_THREADS) fp_kernel(FpArgs args) {
 // ------------------------------------------------------------------------------------------
 // Back projection (reference iradon discretisation, optional maps x weights)
 // ------------------------------------------------------------------------------------------
-constexpr int BP_TILE = 32;
+constexpr int BP_TJ = 32;                                // tile columns (one per lane)
+constexpr int BP_TI = 64;                                // tile rows
 constexpr int BP_THREADS = 256;
-constexpr int BP_PPT = BP_TILE * BP_TILE / BP_THREADS;  // 4 pixels per thread
+constexpr int BP_PPT = BP_TI / (BP_THREADS / 32);        // 8 pixels (rows warp, warp+8, ...) per thread
 constexpr int BP_LINES = 32;                             // lines staged per chunk
-constexpr int BP_KW = 64;                                // staged pairs per line (>= 48 needed)
+constexpr int BP_KW = 80;                                // staged pairs per line (>= 74 needed)
 constexpr float BP_EDGE_GUARD = 0.01f;
 
 enum : int { LINE_FAST = 0, LINE_CHECKED = 1, LINE_EMPTY = 2 };
 
 template <int EPI, bool SYM, int MAPS_DTYPE>
 __global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
-  __shared__ float2 pairs[BP_LINES][BP_KW];
+  __shared__ __align__(16) float2 pairs[BP_LINES][BP_KW];
   __shared__ float4 linfo[BP_LINES];  // cos, sin, offset (K - kbase), weight
   __shared__ int lkind[BP_LINES];
   __shared__ int lkbase[BP_LINES];
@@ -214,10 +273,10 @@ __global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
   const int n = args.n;
   const int s = blockIdx.y;
   if (args.active != nullptr && args.active[s] == 0) return;
-  const int tiles_j = (n + BP_TILE - 1) / BP_TILE;
+  const int tiles_j = (n + BP_TJ - 1) / BP_TJ;
   const int ti = blockIdx.x / tiles_j;
   const int tj = blockIdx.x - ti * tiles_j;
-  const int i0 = ti * BP_TILE, j0 = tj * BP_TILE;
+  const int i0 = ti * BP_TI, j0 = tj * BP_TJ;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int j = j0 + lane;
   const int R = n / 2;      // iradon output radius (output_size // 2)
@@ -226,11 +285,14 @@ __global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
   const int n_lines = args.n_det * args.n_angles;
   const float* sino = args.sino + (int64_t)s * n_lines * n;
 
-  // tile corners relative to the centre
-  // full tile (also pixels beyond n, which are computed and discarded) so every
-  // thread's lookup stays inside the staged range
-  const float cj0 = (float)(j0 - R), cj1 = (float)(j0 + BP_TILE - 1 - R);
-  const float ci0 = (float)(i0 - R), ci1 = (float)(i0 + BP_TILE - 1 - R);
+  // full tile (also pixels beyond n, which are computed and discarded) so every thread's
+  // lookup stays inside the staged range
+  const float cj0 = (float)(j0 - R), cj1 = (float)(j0 + BP_TJ - 1 - R);
+  const float ci0 = (float)(i0 - R), ci1 = (float)(i0 + BP_TI - 1 - R);
+  const float fjR = (float)(j - R);
+  float nfiR[BP_PPT];
+#pragma unroll
+  for (int k = 0; k < BP_PPT; ++k) nfiR[k] = -(float)(i0 + warp + 8 * k - R);
 
   float acc[BP_PPT];
 #pragma unroll
@@ -259,11 +321,19 @@ __global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
       float w = 1.f;
       if (SYM && args.weights != nullptr) w = args.weights[a * args.n_det + d];
       const float* line = sino + ((int64_t)d * args.n_angles + a) * n;
-      for (int q = lane; q < BP_KW; q += 32) {
-        const int kk = kbase + q;
-        const float v0 = (kk >= 0 && kk < n) ? __ldg(line + kk) : 0.f;
-        const float v1 = (kk + 1 >= 0 && kk + 1 < n) ? __ldg(line + kk + 1) : 0.f;
-        pairs[ll][q] = make_float2(w * v0, w * (v1 - v0));
+      if (kind != LINE_EMPTY) {
+        float v[3], vn[3];
+#pragma unroll
+        for (int q3 = 0; q3 < 3; ++q3) {
+          const int kk = kbase + lane + 32 * q3;
+          v[q3] = (kk >= 0 && kk < n) ? __ldg(line + kk) : 0.f;
+          vn[q3] = (kk + 1 >= 0 && kk + 1 < n) ? __ldg(line + kk + 1) : 0.f;
+        }
+#pragma unroll
+        for (int q3 = 0; q3 < 3; ++q3) {
+          const int q = lane + 32 * q3;
+          if (q < BP_KW) pairs[ll][q] = make_float2(w * v[q3], w * (vn[q3] - v[q3]));
+        }
       }
       if (lane == 0) {
         linfo[ll] = make_float4(cs, sn, (float)(K - kbase), w);
@@ -279,7 +349,7 @@ __global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
       const int kind = lkind[ll];
       if (kind == LINE_EMPTY) continue;
       const float4 inf = linfo[ll];
-      const float base = fmaf((float)(j - R), inf.x, inf.z);
+      const float base = fmaf(fjR, inf.x, inf.z);
       const float2* pr = pairs[ll];
       int a = 0, d = 0;
       if (SYM) {
@@ -287,11 +357,19 @@ __global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
         d = l / args.n_angles;
         a = l - d * args.n_angles;
       }
+      if (kind == LINE_FAST && !SYM) {
+#pragma unroll
+        for (int k = 0; k < BP_PPT; ++k) {
+          const FloorSplit fs = floor_split(fmaf(nfiR[k], inf.y, base));
+          const float2 p = pr[fs.i];
+          acc[k] += fmaf(fs.f, p.y, p.x);
+        }
+        continue;
+      }
 #pragma unroll
       for (int k = 0; k < BP_PPT; ++k) {
         const int i = i0 + warp + 8 * k;
-        const float u = fmaf(-(float)(i - R), inf.y, base);
-        const FloorSplit fs = floor_split(u);
+        const FloorSplit fs = floor_split(fmaf(nfiR[k], inf.y, base));
         const float2 p = pr[fs.i];
         float v = fmaf(fs.f, p.y, p.x);
         if (kind == LINE_CHECKED) {
@@ -406,8 +484,8 @@ void launch_fp(const FpArgs& a, cudaStream_t st) {
 
 template <int EPI>
 static void launch_bp_epi(const BpArgs& a, cudaStream_t st) {
-  const int tiles = (a.n + BP_TILE - 1) / BP_TILE;
-  const dim3 grid(tiles * tiles, a.n_slices);
+  const int tiles = ((a.n + BP_TJ - 1) / BP_TJ) * ((a.n + BP_TI - 1) / BP_TI);
+  const dim3 grid(tiles, a.n_slices);
   const bool sym = a.mode == CCT_BP_SYMMETRIC;
   if (!sym) {
     bp_kernel<EPI, false, CCT_DTYPE_F32><<<grid, BP_THREADS, 0, st>>>(a);

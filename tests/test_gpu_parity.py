@@ -87,7 +87,7 @@ def test_solvers_match_reference(golden_cases, case, cuda):
     assert rel_l2(xp, g["pdhg_x"]) < TOL_RECON
 
 
-@pytest.mark.parametrize("n,n_ang", [(128, 90), (256, 360)])
+@pytest.mark.parametrize("n,n_ang", [(66, 20), (130, 45), (128, 90), (256, 360)])
 def test_against_oracle_port_medium(n, n_ang, cuda):
     from oracle import port
     from pycorrectedemissionct_b200 import core, phantoms
