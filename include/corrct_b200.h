@@ -112,6 +112,16 @@ int cct_maps_workspace_size(const cct_maps_desc* desc, int32_t angles_per_pass, 
 int cct_compute_maps(const cct_maps_desc* desc, const float* mu_in, const float* mu_out, void* maps,
                      void* workspace, size_t workspace_bytes, void* stream);
 
+/* Same maps as cct_compute_maps, computed without any device allocation: the scratch is a
+   32 MiB array in the library's static device memory.  No counterpart in the reference; it is
+   for callers that cannot allocate device memory (a pool allocator owns it all, a plugin host
+   forbids cudaMalloc in its callbacks, or cudaMalloc's implicit synchronisation is not allowed).
+   Calls whose one-angle pass needs more than 32 MiB return CCT_ERR_VALUE.  The first call on a
+   device looks up the array's device address (cudaGetSymbolAddress), so make that first call
+   before any stream capture.  All calls share the array: calls that overlap on the GPU race. */
+int cct_compute_maps_noalloc(const cct_maps_desc* desc, const float* mu_in, const float* mu_out, void* maps,
+                             void* stream);
+
 /* ---------------------------------------------------------------------------------------------
  * Device-resident solver steps for a batch of slices (update equations of corrct's MLEM,
  * SIRT and PDHG: src/corrct/solvers.py:688-805, 867-984, 1060-1206).

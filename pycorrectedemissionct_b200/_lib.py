@@ -104,6 +104,10 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.POINTER(MapsDesc), c_float_p, c_float_p, c_float_p, c_float_p, ctypes.c_size_t, ctypes.c_void_p],
     ),
+    "cct_compute_maps_noalloc": (
+        ctypes.c_int,
+        [ctypes.POINTER(MapsDesc), c_float_p, c_float_p, c_float_p, ctypes.c_void_p],
+    ),
     "cct_solver_partials_count": (ctypes.c_int, [ctypes.POINTER(XrfDesc), ctypes.POINTER(ctypes.c_int64)]),
     "cct_mlem_step": (
         ctypes.c_int,
