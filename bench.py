@@ -219,6 +219,9 @@ def run_ours(a):
     maps = torch.empty((S, a.angles, 1, n, n), dtype=tdt, device=dev)
     ws = torch.empty(core.DEFAULT_MAPS_WORKSPACE, dtype=torch.uint8, device=dev)
     core.compute_maps(mu_in, mu_out, rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
+    from pycorrectedemissionct_b200 import autotune
+
+    variant = autotune.tune(c, x_true, maps)
     clean = c.fp(x_true, maps)
     gen = torch.Generator(device=dev)
     gen.manual_seed(a.seed + rank)
@@ -330,6 +333,7 @@ def run_ours(a):
             "parallelism": f"slices sharded over {world} GPU(s), no collective on the data path",
             "l2": "inputs larger than L2 (maps %.0f MB per slice)" % (a.angles * n * n * map_bytes / 1e6),
             "mean_iterations": float(np.mean(iterations)), "converged_slices_last_step": converged,
+            "fp_variant": "tma" if variant else "ldg",
         },
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

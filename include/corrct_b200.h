@@ -45,6 +45,10 @@ extern "C" {
                               (corrct: src/corrct/projectors.py:533-568, 608-618) */
 #define CCT_BP_ADJOINT 2   /* exact transpose of cct_fp (no reference counterpart) */
 
+/* Kernel variants (results are identical; only the speed differs). */
+#define CCT_VARIANT_FP_TMA 1 /* forward projection stages its boxes with TMA bulk tensor copies
+                                (needs n % 8 == 0; otherwise the load/store staging is used) */
+
 /* Geometry of a batch of slices that share n, the angles and the detectors. */
 typedef struct cct_xrf_desc {
   int32_t n;          /* square volume side and detector width in pixels (>= 2) */
@@ -52,7 +56,7 @@ typedef struct cct_xrf_desc {
   int32_t n_det;      /* D >= 1 fluorescence detectors (maps per angle) */
   int32_t n_slices;   /* S >= 1 */
   int32_t maps_dtype; /* CCT_DTYPE_F32 or CCT_DTYPE_BF16 */
-  int32_t reserved;
+  int32_t variant;    /* kernel variant chosen by the autotuner: CCT_VARIANT_* flags, 0 = default */
   const float* fp_matrix; /* device [A][6]: per-angle inverse map of scikit-image radon,
                              (M00, M01, M02, M10, M11, M12): col_in = M00*c + M01*r + M02,
                              row_in = M10*c + M11*r + M12, entries as radon builds them in float32 */

@@ -25,6 +25,8 @@ CCT_BP_REFERENCE = 0
 CCT_BP_SYMMETRIC = 1
 CCT_BP_ADJOINT = 2
 
+CCT_VARIANT_FP_TMA = 1
+
 c_float_p = ctypes.c_void_p  # device pointers are passed as integers
 
 
@@ -35,7 +37,7 @@ class XrfDesc(ctypes.Structure):
         ("n_det", ctypes.c_int32),
         ("n_slices", ctypes.c_int32),
         ("maps_dtype", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("variant", ctypes.c_int32),
         ("fp_matrix", ctypes.c_void_p),
         ("bp_trig", ctypes.c_void_p),
         ("weights", ctypes.c_void_p),

@@ -67,8 +67,9 @@ class XrfCore:
         ``w_det[d] * w_angle[a, d]`` applied by the attenuated fp and the symmetric bp.
     """
 
-    def __init__(self, n: int, angles_rot_rad, n_det: int = 1, weights=None, device=None):
+    def __init__(self, n: int, angles_rot_rad, n_det: int = 1, weights=None, device=None, variant: int = 0):
         self.device = require_cuda(device)
+        self.variant = int(variant)
         self.n = int(n)
         self.n_det = int(n_det)
         self.angles_rad32, self.angles_deg32 = geometry.backend_angles(angles_rot_rad)
@@ -95,6 +96,7 @@ class XrfCore:
         d.n_det = self.n_det
         d.n_slices = int(n_slices)
         d.maps_dtype = maps_dtype
+        d.variant = self.variant
         if angles is None:
             d.n_angles = self.n_angles
             d.fp_matrix = self.fp_mat.data_ptr()

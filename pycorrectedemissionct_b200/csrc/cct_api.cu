@@ -47,7 +47,7 @@ static cct::FpArgs make_fp_args(const cct_xrf_desc* d, const float* vol, const v
   cct::FpArgs a;
   std::memset(&a, 0, sizeof(a));
   a.n = d->n; a.n_angles = d->n_angles; a.n_det = d->n_det; a.n_slices = d->n_slices;
-  a.maps_dtype = d->maps_dtype; a.epi = cct::FP_EPI_STORE;
+  a.maps_dtype = d->maps_dtype; a.epi = cct::FP_EPI_STORE; a.variant = d->variant;
   a.fp_matrix = d->fp_matrix; a.weights = d->weights; a.vol = vol; a.maps = maps; a.out = out;
   return a;
 }

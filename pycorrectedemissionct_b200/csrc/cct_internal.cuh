@@ -17,7 +17,7 @@ enum FpEpilogue : int { FP_EPI_STORE = 0, FP_EPI_MLEM = 1, FP_EPI_SIRT = 2, FP_E
 enum BpEpilogue : int { BP_EPI_STORE = 0, BP_EPI_MLEM = 1, BP_EPI_SIRT = 2, BP_EPI_PDHG = 3 };
 
 struct FpArgs {
-  int n, n_angles, n_det, n_slices, maps_dtype, epi;
+  int n, n_angles, n_det, n_slices, maps_dtype, epi, variant;
   const float* fp_matrix;
   const float* weights;
   const float* vol;

@@ -21,6 +21,11 @@
 // 0.01 bin of an edge take a checked path that decides edge cases in double
 // precision exactly as numpy does.
 
+#include <cstring>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "cct_common.cuh"
 #include "cct_internal.cuh"
 
@@ -251,6 +256,216 @@ __global__ void __launch_bounds__(FP_THREADS) fp_kernel(FpArgs args) {
 }
 
 // ------------------------------------------------------------------------------------------
+// Forward projection, TMA-staged variant (n % 8 == 0)
+//
+// The chunk's x box and map box (fixed 96 x 104 boxes, zero-filled outside the image) arrive
+// through two cp.async.bulk.tensor loads on one mbarrier; one vectorised pass multiplies them
+// in place (z = x * map), then the same 8x4-lane sampling as fp_kernel runs on row stride 104.
+// No load instruction per element, and the copy overlaps the other resident CTA's sampling.
+// The left box edge is a multiple of 8 elements (16 bytes for BF16 maps too), as TMA needs.
+// ------------------------------------------------------------------------------------------
+constexpr int FPT_BOX_W = 104;
+constexpr int FPT_BOX_H = 96;
+constexpr int FPT_Q4 = FPT_BOX_W / 4;              // float4 per box row
+constexpr uint32_t FPT_WAIT_LIMIT = 1u << 22;      // bounded mbarrier polling (never spins forever)
+
+__device__ int g_tma_timeout = 0;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
+  for (uint32_t it = 0; it < FPT_WAIT_LIMIT; ++it) {
+    if (mbar_try_wait(bar, phase)) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <int EPI, bool HAS_MAPS, int MAPS_DTYPE>
+__global__ void __launch_bounds__(FP_THREADS, 2)
+    fp_tma_kernel(FpArgs args, const __grid_constant__ CUtensorMap tm_vol, const __grid_constant__ CUtensorMap tm_maps) {
+  extern __shared__ __align__(128) unsigned char fpt_smem[];
+  float* zb = reinterpret_cast<float*>(fpt_smem);                                  // [96][104] x, then z
+  unsigned char* mraw = fpt_smem + FPT_BOX_H * FPT_BOX_W * sizeof(float);         // [96][104] map
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ double red_d[FP_TC / FP_LC];
+  __shared__ int timed_out;
+
+  const int n = args.n;
+  const int band = blockIdx.x;
+  const int ad = blockIdx.y;
+  const int s = blockIdx.z;
+  if (args.active != nullptr && args.active[s] == 0) return;
+  const int a = ad / args.n_det;
+  const int d = ad - a * args.n_det;
+
+  const float* M = args.fp_matrix + 6 * a;
+  const float m00 = M[0], m01 = M[1], m02 = M[2], m10 = M[3], m11 = M[4], m12 = M[5];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int lc = lane & (FP_LC - 1);
+  const int lr = lane / FP_LC;
+  const int c0 = band * FP_TC;
+  const int c = c0 + warp * FP_LC + lc;
+  const int c_last = min(c0 + FP_TC, n) - 1;
+  const int map_img = (s * args.n_angles + a) * args.n_det + d;
+  const uint32_t box_bytes = FPT_BOX_H * FPT_BOX_W * sizeof(float) +
+                             (HAS_MAPS ? FPT_BOX_H * FPT_BOX_W * (MAPS_DTYPE == CCT_DTYPE_BF16 ? 2 : 4) : 0);
+  const float fc = (float)c;
+  const float pxc = fmaf(m00, fc, m02);
+  const float pyc = fmaf(m10, fc, m12);
+
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    timed_out = 0;
+  }
+  __syncthreads();
+
+  uint32_t phase = 0;
+  float acc = 0.f;
+  for (int r0 = 0; r0 < n; r0 += FP_TR) {
+    const int r_last = min(r0 + FP_TR, n) - 1;
+    const float fc0 = (float)c0, fc1 = (float)c_last, fr0 = (float)r0, fr1 = (float)r_last;
+    const float xa = sample_x(m00, m01, m02, fc0, fr0), xb = sample_x(m00, m01, m02, fc1, fr0);
+    const float xc = sample_x(m00, m01, m02, fc0, fr1), xd = sample_x(m00, m01, m02, fc1, fr1);
+    const float ya = sample_x(m10, m11, m12, fc0, fr0), yb = sample_x(m10, m11, m12, fc1, fr0);
+    const float yc = sample_x(m10, m11, m12, fc0, fr1), yd = sample_x(m10, m11, m12, fc1, fr1);
+    const float xmin = fminf(fminf(xa, xb), fminf(xc, xd)), xmax = fmaxf(fmaxf(xa, xb), fmaxf(xc, xd));
+    const float ymin = fminf(fminf(ya, yb), fminf(yc, yd)), ymax = fmaxf(fmaxf(ya, yb), fmaxf(yc, yd));
+    const int bx0 = ((int)floorf(xmin) - 1) & ~7;  // 16-byte aligned TMA x coordinate (BF16 too)
+    const int bx1 = (int)floorf(xmax) + 2;
+    const int by0 = (int)floorf(ymin) - 1;
+    const int by1 = (int)floorf(ymax) + 2;
+    const int wq = (bx1 - bx0) / 4 + 1;  // float4 columns used
+    const int bh = by1 - by0 + 1;
+    if (4 * wq > FPT_BOX_W || bh > FPT_BOX_H) {  // cannot happen for valid matrices; never trap
+      if (tid == 0) atomicExch(&g_box_overflow, 1);
+      return;
+    }
+
+    if (tid == 0) {
+      mbar_expect_tx(&bar, box_bytes);
+      tma_load_3d(zb, &tm_vol, bx0, by0, s, &bar);
+      if (HAS_MAPS) tma_load_3d(mraw, &tm_maps, bx0, by0, map_img, &bar);
+    }
+    // every thread observes the phase flip itself (acquire of the bulk-copy writes)
+    if (!mbar_wait_bounded(&bar, phase)) timed_out = 1;
+    __syncthreads();
+    if (timed_out) {
+      // give the copies in flight one more bounded wait, then leave without touching smem
+      if (tid == 0) {
+        atomicExch(&g_tma_timeout, 1);
+        mbar_wait_bounded(&bar, phase);
+      }
+      return;
+    }
+    phase ^= 1u;
+
+    if (HAS_MAPS) {
+      float4* z4 = reinterpret_cast<float4*>(zb);
+      for (int it = tid; it < bh * FPT_Q4; it += FP_THREADS) {
+        const int rr = it / FPT_Q4;
+        const int qq = it - rr * FPT_Q4;
+        if (qq < wq) {
+          float4 v = z4[it];
+          if (MAPS_DTYPE == CCT_DTYPE_BF16) {
+            const uint2 raw = reinterpret_cast<const uint2*>(mraw)[it];
+            const float2 flo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.x));
+            const float2 fhi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.y));
+            v.x *= flo.x; v.y *= flo.y; v.z *= fhi.x; v.w *= fhi.y;
+          } else {
+            const float4 mv = reinterpret_cast<const float4*>(mraw)[it];
+            v.x *= mv.x; v.y *= mv.y; v.z *= mv.z; v.w *= mv.w;
+          }
+          z4[it] = v;
+        }
+      }
+      __syncthreads();
+    }
+
+    if (c <= c_last) {
+      const int zoff = -by0 * FPT_BOX_W - bx0;
+      float fr = (float)(r0 + lr);
+      const int rem = r_last - r0 - lr;
+      const int kmax = rem >= 0 ? rem / FP_LR + 1 : 0;
+      if (kmax >= FP_RPT) {
+#pragma unroll 4
+        for (int k = 0; k < FP_RPT; ++k) {
+          const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
+          const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
+          const int q = fy.i * FPT_BOX_W + fx.i + zoff;
+          const float t0 = zb[q], t1 = zb[q + 1], b0 = zb[q + FPT_BOX_W], b1 = zb[q + FPT_BOX_W + 1];
+          const float top = fmaf(fx.f, t1 - t0, t0);
+          const float bot = fmaf(fx.f, b1 - b0, b0);
+          acc += fmaf(fy.f, bot - top, top);
+          fr += (float)FP_LR;
+        }
+      } else {
+        for (int k = 0; k < kmax; ++k) {
+          const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
+          const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
+          const int q = fy.i * FPT_BOX_W + fx.i + zoff;
+          const float t0 = zb[q], t1 = zb[q + 1], b0 = zb[q + FPT_BOX_W], b1 = zb[q + FPT_BOX_W + 1];
+          const float top = fmaf(fx.f, t1 - t0, t0);
+          const float bot = fmaf(fx.f, b1 - b0, b0);
+          acc += fmaf(fy.f, bot - top, top);
+          fr += (float)FP_LR;
+        }
+      }
+    }
+    __syncthreads();
+    // generic-proxy writes/reads of the boxes are done; order them before the next bulk copy
+    if (tid == 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+
+  acc += __shfl_xor_sync(0xffffffffu, acc, 8);
+  acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+  double part = 0.0;
+  if (lr == 0 && c <= c_last) {
+    float total = acc;
+    if (args.weights != nullptr) total *= args.weights[a * args.n_det + d];
+    const int64_t idx = (((int64_t)s * args.n_det + d) * args.n_angles + a) * n + c;
+    part = fp_epilogue<EPI>(args, idx, total);
+  }
+  if (EPI == FP_EPI_MLEM || EPI == FP_EPI_SIRT) {
+    part = warp_sum_double(part);
+    if (lane == 0) red_d[warp] = part;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < FP_TC / FP_LC; ++w) t += red_d[w];
+      const int64_t per_slice = (int64_t)gridDim.x * gridDim.y;
+      args.partials[(int64_t)s * per_slice + (int64_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
 // Back projection (reference iradon discretisation, optional maps x weights)
 // ------------------------------------------------------------------------------------------
 constexpr int BP_TJ = 32;                                // tile columns (one per lane)
@@ -461,9 +676,78 @@ __global__ void __launch_bounds__(256) bp_adjoint_kernel(BpArgs args) {
 // ------------------------------------------------------------------------------------------
 // Launchers
 // ------------------------------------------------------------------------------------------
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link needed)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess) {
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+  }
+  return fn;
+}
+
+// 3-D tiled map over `images` row-major n x n images with a 96 x 104 box.
+static bool make_box_map(CUtensorMap* map, const void* base, int n, int64_t images, bool bf16) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (enc == nullptr) return false;
+  const uint64_t esz = bf16 ? 2 : 4;
+  const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)images};
+  const cuuint64_t strides[2] = {(cuuint64_t)(n * esz), (cuuint64_t)((uint64_t)n * n * esz)};
+  const cuuint32_t box[3] = {(cuuint32_t)FPT_BOX_W, (cuuint32_t)FPT_BOX_H, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                         const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <int EPI, bool HAS_MAPS, int MAPS_DTYPE>
+static bool launch_fp_tma_inst(const FpArgs& a, const dim3& grid, cudaStream_t st) {
+  CUtensorMap tv, tm;
+  std::memset(&tm, 0, sizeof(tm));
+  if (!make_box_map(&tv, a.vol, a.n, a.n_slices, false)) return false;
+  if (HAS_MAPS &&
+      !make_box_map(&tm, a.maps, a.n, (int64_t)a.n_slices * a.n_angles * a.n_det, MAPS_DTYPE == CCT_DTYPE_BF16)) {
+    return false;
+  }
+  const size_t smem = FPT_BOX_H * FPT_BOX_W * sizeof(float) +
+                      (HAS_MAPS ? FPT_BOX_H * FPT_BOX_W * (MAPS_DTYPE == CCT_DTYPE_BF16 ? 2 : 4) : 0);
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(fp_tma_kernel<EPI, HAS_MAPS, MAPS_DTYPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess) {
+      return false;
+    }
+    attr_set = true;
+  }
+  fp_tma_kernel<EPI, HAS_MAPS, MAPS_DTYPE><<<grid, FP_THREADS, smem, st>>>(a, tv, tm);
+  return true;
+}
+
 template <int EPI>
 static void launch_fp_epi(const FpArgs& a, cudaStream_t st) {
   const dim3 grid((a.n + FP_TC - 1) / FP_TC, a.n_angles * a.n_det, a.n_slices);
+  // TMA path: rows and images must be 16-byte multiples for both FP32 and BF16 boxes
+  const bool aligned = (a.n % 8) == 0 && (reinterpret_cast<uintptr_t>(a.vol) % 16) == 0 &&
+                       (a.maps == nullptr || (reinterpret_cast<uintptr_t>(a.maps) % 16) == 0);
+  if (aligned && (a.variant & CCT_VARIANT_FP_TMA)) {
+    bool ok;
+    if (a.maps == nullptr) {
+      ok = launch_fp_tma_inst<EPI, false, CCT_DTYPE_F32>(a, grid, st);
+    } else if (a.maps_dtype == CCT_DTYPE_BF16) {
+      ok = launch_fp_tma_inst<EPI, true, CCT_DTYPE_BF16>(a, grid, st);
+    } else {
+      ok = launch_fp_tma_inst<EPI, true, CCT_DTYPE_F32>(a, grid, st);
+    }
+    if (ok) return;
+  }
   if (a.maps == nullptr) {
     fp_kernel<EPI, false, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(a);
   } else if (a.maps_dtype == CCT_DTYPE_BF16) {
@@ -523,12 +807,17 @@ int read_device_error(int clear, int* value) {
   int v = 0;
   cudaError_t e = cudaMemcpyFromSymbol(&v, g_box_overflow, sizeof(int));
   if (e != cudaSuccess) return (int)e;
-  if (clear && v != 0) {
+  int t = 0;
+  e = cudaMemcpyFromSymbol(&t, g_tma_timeout, sizeof(int));
+  if (e != cudaSuccess) return (int)e;
+  if (clear) {
     const int zero = 0;
     e = cudaMemcpyToSymbol(g_box_overflow, &zero, sizeof(int));
     if (e != cudaSuccess) return (int)e;
+    e = cudaMemcpyToSymbol(g_tma_timeout, &zero, sizeof(int));
+    if (e != cudaSuccess) return (int)e;
   }
-  *value = v;
+  *value = v | (t << 1);
   return 0;
 }
 }  // namespace cct

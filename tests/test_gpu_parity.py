@@ -229,3 +229,20 @@ def test_engine_tolerance_and_graph(cuda):
     assert int(stop.active.sum()) == 0
     # stopped slices keep the iterate of their last update
     assert torch.equal(stop.history[:, : int(expect.min())], eager.history[:, : int(expect.min())])
+
+
+@pytest.mark.parametrize("n,n_ang,dtype", [(64, 48, torch.float32), (512, 90, torch.float32), (512, 90, torch.bfloat16)])
+def test_fp_variants_bit_identical(n, n_ang, dtype, cuda, tmp_path, monkeypatch):
+    from pycorrectedemissionct_b200 import _lib, autotune, core, phantoms
+
+    rng = phantoms.slice_rng(77, n)
+    x = _t(np.stack([phantoms.ellipse_phantom(n, rng) for _ in range(2)]), cuda)
+    maps = _t(rng.uniform(0.3, 1.0, size=(2, n_ang, 1, n, n)), cuda, dtype)
+    c = core.XrfCore(n, phantoms.angles(n_ang), device=cuda)
+    ref = c.fp(x, maps)
+    c.variant = _lib.CCT_VARIANT_FP_TMA
+    assert torch.equal(c.fp(x, maps), ref)
+    monkeypatch.setenv("CCT_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    v = autotune.tune(c, x, maps)
+    assert v in autotune.VARIANTS and (tmp_path / "tune.json").exists()
+    assert torch.equal(c.fp(x, maps), ref)
