@@ -217,7 +217,9 @@ def run_ours(a):
     x_true = torch.from_numpy(xs_h).to(dev)
     tdt = torch.float32 if a.maps_dtype == "float32" else torch.bfloat16
     maps = torch.empty((S, a.angles, 1, n, n), dtype=tdt, device=dev)
-    ws = torch.empty(core.DEFAULT_MAPS_WORKSPACE, dtype=torch.uint8, device=dev)
+    # maps workspace: ~16 angles of the whole batch per pass (2 x 2.1 MB per angle and slice)
+    ws = torch.empty(max(core.DEFAULT_MAPS_WORKSPACE, 16 * 2 * (a.n + 2 * ((int(np.ceil(np.sqrt(2) * a.n)) - a.n + 1) // 2)) ** 2 * 4 * S),
+                     dtype=torch.uint8, device=dev)
     core.compute_maps(mu_in, mu_out, rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
     from pycorrectedemissionct_b200 import autotune
 
@@ -337,7 +339,10 @@ def run_ours(a):
         },
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "kernel": "fp_kernel<MLEM> (attenuated fp + ratio + KL residual)",
+            # DRAM bytes per launch from one ncu capture of this kernel on 2 slices (1.4366 GB), scaled
+            # by the slices per launch; only for the capture's own configuration
+            "traffic": (1.4366e9 / 2 * S) if (n == 512 and a.angles == 720 and a.maps_dtype == "float32") else None,
+            "kernel": "fp_kernel<MLEM> (attenuated fp + ratio + KL residual)",
             "peak_source": peak_src, "fp_launch_us": fp_avg_s * 1e6, "bp_launch_us": bp_avg_s * 1e6,
             "algorithmic_bytes_per_launch": fp_bytes,
         },

@@ -221,7 +221,8 @@ def compute_maps(
     need = ctypes.c_size_t(0)
     _lib.call("cct_maps_workspace_size", ctypes.byref(desc), 1, ctypes.byref(need))
     if workspace is None:
-        nbytes = max(int(need.value), min(int(workspace_bytes), int(need.value) * n_ang))
+        # at least 8 angles (of the whole batch) per pass, at most all of them
+        nbytes = min(max(int(workspace_bytes), 8 * int(need.value)), int(need.value) * n_ang)
         workspace = torch.empty(nbytes, dtype=torch.uint8, device=device)
     if out is None:
         maps = torch.empty((s, n_ang, n_det, n, n), dtype=tdt, device=device)
