@@ -186,6 +186,81 @@ int cct_pdhg_step(const cct_xrf_desc* desc, const void* maps, int32_t bp_mode, c
 int cct_reduce_norm(const float* v, int64_t count, int32_t n_slices, int32_t ord, double* out,
                     double* partials, void* stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * Learned warm start (no reference counterpart): a small convolutional encoder-decoder whose
+ * 3x3 convolutions run as implicit GEMMs on tcgen05 tensor cores (BF16 in, FP32 accumulate in
+ * TMEM).  Activations are NHWC bfloat16 with channel counts that are multiples of 16; weights are
+ * [cout][3][3][cin] bfloat16; padding is 1 (same size), stride 1.  Its output is only an initial
+ * guess x0 for the reference's MLEM (corrct: src/corrct/solvers.py:747-752 accepts x0).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct cct_conv_desc {
+  int32_t batch;
+  int32_t height;
+  int32_t width;
+  int32_t cin;  /* power of two in [16, 512] */
+  int32_t cout; /* multiple of 16 in [16, 512] */
+} cct_conv_desc;
+
+/* y = act(conv3x3(x, w) + bias); act = ReLU when relu != 0; bias may be NULL.  With x = dy and
+   w = the flipped weights of cct_net_flip_weights this is the data gradient of a convolution. */
+int cct_conv3x3_fwd(const cct_conv_desc* desc, const void* x, const void* w, const float* bias, int32_t relu,
+                    void* y, void* stream);
+
+/* dw[co][tap][ci] += sum over pixels of dy[p][co] * x[p + tap][ci] (FP32, caller zeroes dw). */
+int cct_conv3x3_wgrad(const cct_conv_desc* desc, const void* x, const void* dy, float* dw, void* stream);
+
+/* [cout][3][3][cin] -> [cin][3][3][cout] with the 3x3 taps reversed (data-gradient weights). */
+int cct_net_flip_weights(const void* w, void* w_flipped, int32_t cin, int32_t cout, void* stream);
+
+/* dx = dy where y > 0 else 0 (bf16, `count` elements). */
+int cct_net_relu_bwd(const void* y, const void* dy, void* dx, int64_t count, void* stream);
+
+/* 2x2 average pooling of NHWC x (height, width even); backward != 0: adjoint from the pooled
+   gradient x to the full-resolution gradient y. */
+int cct_net_avgpool2(const void* x, void* y, int32_t batch, int32_t height, int32_t width, int32_t channels,
+                     int32_t backward, void* stream);
+
+/* nearest 2x upsampling of NHWC x (height, width = the small size); backward != 0: adjoint
+   (sum of the 4 children) from the large gradient x to the small gradient y. */
+int cct_net_upsample2(const void* x, void* y, int32_t batch, int32_t height, int32_t width, int32_t channels,
+                      int32_t backward, void* stream);
+
+/* out = a + b (bf16, `count` elements). */
+int cct_net_add(const void* a, const void* b, void* out, int64_t count, void* stream);
+
+/* db[c] += sum over pixels of dy[p][c] (FP32, caller zeroes db). */
+int cct_net_bias_grad(const void* dy, float* db, int64_t pixels, int32_t channels, void* stream);
+
+/* Mean squared error of channel 0 of pred (NHWC) against target [pixels] (FP32):
+   *loss += mean (pred - target)^2 (FP64), grad (NHWC bf16) = d loss / d pred. */
+int cct_net_mse(const void* pred, const float* target, void* grad, double* loss, int64_t pixels, int32_t channels,
+                void* stream);
+
+/* One Adam step on FP32 master parameters p with gradient g and moments m, v (step >= 1, bias
+   corrected); p_bf16 (may be NULL) receives the bfloat16 copy used by the convolutions. */
+int cct_net_adam(float* p, const float* g, float* m, float* v, void* p_bf16, int64_t count, float lr, float beta1,
+                 float beta2, float eps, int32_t step, void* stream);
+
+/* NHWC bf16 network input from n_src FP32 planar images of `pixels` values each (device array of
+   device pointers); every value is divided by its slice's slice_scale[p / slice_pixels]
+   (slice_scale may be NULL); channels beyond n_src are zero. */
+int cct_net_pack_nhwc(const float* const* src, int32_t n_src, void* dst, int64_t pixels, int32_t channels,
+                      const float* slice_scale, int64_t slice_pixels, void* stream);
+
+/* Warm start from the head output v = src[p][0] with s = slice_scale[p / slice_pixels] (1 if NULL):
+   mode 0 (additive):       out[p] = max(base[p] + s * v, floor_value)
+   mode 1 (multiplicative): out[p] = max((base[p] + s * floor_value) * exp(v) - s * floor_value, floor_value)
+   (base may be NULL). */
+int cct_net_unpack_c0(const void* src, int32_t channels, const float* base, const float* slice_scale,
+                      int64_t slice_pixels, int32_t mode, float floor_value, float* out, int64_t pixels, void* stream);
+
+/* out[i] = a[i] / b[i % b_count] (FP32; b broadcast over slices), e.g. A^T b / A^T 1. */
+int cct_net_ratio(const float* a, const float* b, float* out, int64_t count, int64_t b_count, void* stream);
+
+/* Network kernels never trap: a tensor-core wait that exceeds its bound raises a flag instead.
+   *value = the flag; clear != 0 resets it.  Synchronous. */
+int cct_net_timeout(int32_t clear, int32_t* value);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,16 @@ class MapsDesc(ctypes.Structure):
     ]
 
 
+class ConvDesc(ctypes.Structure):
+    _fields_ = [
+        ("batch", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("width", ctypes.c_int32),
+        ("cin", ctypes.c_int32),
+        ("cout", ctypes.c_int32),
+    ]
+
+
 class SolverState(ctypes.Structure):
     _fields_ = [
         ("x", ctypes.c_void_p),
@@ -132,6 +142,43 @@ SIGNATURES = {
         ctypes.c_int,
         [c_float_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, c_float_p, c_float_p, ctypes.c_void_p],
     ),
+    "cct_conv3x3_fwd": (
+        ctypes.c_int,
+        [ctypes.POINTER(ConvDesc), c_float_p, c_float_p, c_float_p, ctypes.c_int32, c_float_p, ctypes.c_void_p],
+    ),
+    "cct_conv3x3_wgrad": (ctypes.c_int, [ctypes.POINTER(ConvDesc), c_float_p, c_float_p, c_float_p, ctypes.c_void_p]),
+    "cct_net_flip_weights": (ctypes.c_int, [c_float_p, c_float_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
+    "cct_net_relu_bwd": (ctypes.c_int, [c_float_p, c_float_p, c_float_p, ctypes.c_int64, ctypes.c_void_p]),
+    "cct_net_avgpool2": (
+        ctypes.c_int,
+        [c_float_p, c_float_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p],
+    ),
+    "cct_net_upsample2": (
+        ctypes.c_int,
+        [c_float_p, c_float_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p],
+    ),
+    "cct_net_add": (ctypes.c_int, [c_float_p, c_float_p, c_float_p, ctypes.c_int64, ctypes.c_void_p]),
+    "cct_net_bias_grad": (ctypes.c_int, [c_float_p, c_float_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p]),
+    "cct_net_mse": (
+        ctypes.c_int,
+        [c_float_p, c_float_p, c_float_p, c_float_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p],
+    ),
+    "cct_net_adam": (
+        ctypes.c_int,
+        [c_float_p, c_float_p, c_float_p, c_float_p, c_float_p, ctypes.c_int64, ctypes.c_float, ctypes.c_float,
+         ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_void_p],
+    ),
+    "cct_net_pack_nhwc": (
+        ctypes.c_int,
+        [c_float_p, ctypes.c_int32, c_float_p, ctypes.c_int64, ctypes.c_int32, c_float_p, ctypes.c_int64, ctypes.c_void_p],
+    ),
+    "cct_net_unpack_c0": (
+        ctypes.c_int,
+        [c_float_p, ctypes.c_int32, c_float_p, c_float_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_float, c_float_p,
+         ctypes.c_int64, ctypes.c_void_p],
+    ),
+    "cct_net_ratio": (ctypes.c_int, [c_float_p, c_float_p, c_float_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p]),
+    "cct_net_timeout": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
 }
 
 _lib = None
