@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define CCT_ABI_VERSION 1
+#define CCT_ABI_VERSION 2
 
 /* Status codes. */
 #define CCT_OK 0
@@ -61,7 +61,19 @@ typedef struct cct_xrf_desc {
                              (M00, M01, M02, M10, M11, M12): col_in = M00*c + M01*r + M02,
                              row_in = M10*c + M11*r + M12, entries as radon builds them in float32 */
   const float* bp_trig;   /* device [A][2]: (cos, sin) of each angle as iradon evaluates them (float32) */
-  const float* weights;   /* device [A][D]: w_det[d] * w_angle[a][d], or NULL for all ones */
+  const float* weights;   /* device [A][D]: w_det[d] * w_angle[a][d] * intensity[a], or NULL for all ones */
+  const float* line_scale; /* device [A]: projection intensities applied by the reference-mode back
+                              projection (corrct: src/corrct/projectors.py:336-337), or NULL */
+  const float* psf;       /* device [psf_len]: detector point-spread function applied after the forward
+                             projection (corrct: src/corrct/projectors.py:199-203, 317-320,
+                             operators.py:480-483: edge-padded 'same' convolution along the detector;
+                             the back projection ignores it, as the reference's default is_symm=False
+                             makes its adjoint the identity), or NULL */
+  int32_t psf_len;
+  int32_t reserved;
+  int64_t maps_slice_stride; /* elements between the maps of consecutive slices; 0 = dense
+                                (n_angles * n_det * n * n).  Lets a call read the maps of an angle
+                                range out of a larger [S][A_total][D][n][n] array. */
 } cct_xrf_desc;
 
 /* Library identity. */
@@ -153,8 +165,14 @@ typedef struct cct_solver_state {
   int32_t has_background;
   float tv_lambda;       /* PDHG isotropic TV weight */
   int32_t tau_shared;
+  float* sino_tmp;       /* [S][D][A][n] workspace, required by PDHG when desc->psf is set */
   double* residual_history; /* [S][history_len] residual of every iteration (SolutionInfo.residuals), or NULL */
   int32_t history_len;
+  int32_t x_mask_per_slice; /* 1: x_mask is [S][n][n] (a 3-D volume mask); 0: one [n][n] mask */
+  int32_t joint_stop;    /* 1: the S slices are one 3-D volume: one residual (the sum over slices, which
+                            is the reference's norm of the whole volume's residual) is compared with
+                            tolerance[0] and all slices stop together; its history is row 0 of
+                            residual_history.  0: every slice has its own stopping test. */
 } cct_solver_state;
 
 /* Number of doubles the `partials` workspace must hold. */

@@ -165,8 +165,12 @@ def fp_uncorrected(vol: NDArray, angles_deg32: NDArray, workers: int = 1) -> NDA
     return out
 
 
-def bp_uncorrected(sino: NDArray, angles_deg32: NDArray, n: int, workers: int = 1) -> NDArray:
-    """Volume ``(N, N)`` of ``ProjectorBackendSKimage.bp`` (``_projector_backends.py:352-359``)."""
+def bp_uncorrected(sino: NDArray, angles_deg32: NDArray, n: int, workers: int = 1, intensities=None) -> NDArray:
+    """Volume ``(N, N)`` of ``ProjectorBackendSKimage.bp`` (``_projector_backends.py:352-359``), after
+    ``ProjectorUncorrected.bp``'s intensity scaling (``projectors.py:336-337``; the PSF adjoint is the
+    identity for the default ``is_symm=False``)."""
+    if intensities is not None:
+        sino = sino * np.asarray(intensities)[:, None]
     parts = np.empty((len(angles_deg32), n, n), dtype=sino.dtype)
 
     def one(ii: int) -> None:
@@ -196,6 +200,28 @@ def _weights(n_ang: int, n_det: int, weights_det, weights_angles) -> NDArray:
     return wd[None, :] * wa
 
 
+def psf_convolve(line: NDArray, kernel: NDArray) -> NDArray:
+    """Detector PSF of ``TransformConvolution._op_direct`` (``operators.py:472-483``) on one line:
+    edge padding by (L-1)//2, scipy 'same' convolution, crop."""
+    from scipy import signal
+
+    kernel = np.asarray(kernel)
+    pw = (len(kernel) - 1) // 2
+    x = np.pad(line, pw, mode="edge")
+    x = signal.convolve(x, kernel, mode="same")
+    return x[pw:-pw] if pw else x
+
+
+def _line(vol2d, deg32, ii_intensity, psf):
+    """``ProjectorUncorrected.fp_angle`` (``projectors.py:259-279``): radon, intensity, PSF."""
+    prj = fp_angle(vol2d, deg32)
+    if ii_intensity is not None:
+        prj = prj * ii_intensity
+    if psf is not None:
+        prj = psf_convolve(prj, psf)
+    return prj
+
+
 def fp_xrf(
     vol: NDArray,
     maps: NDArray,
@@ -203,6 +229,8 @@ def fp_xrf(
     weights_det=None,
     weights_angles=None,
     workers: int = 1,
+    intensities=None,
+    psf=None,
 ) -> NDArray:
     """Attenuated forward projection (``ProjectorAttenuationXRF.fp``, ``projectors.py:502-531, 570-596``).
 
@@ -214,8 +242,9 @@ def fp_xrf(
 
     def one(ii: int) -> None:
         temp = vol * maps[ii]
+        inten = None if intensities is None else intensities[ii]
         for dd in range(n_det):
-            out[dd, ii] = w[ii, dd] * fp_angle(temp[dd], angles_deg32[ii])
+            out[dd, ii] = w[ii, dd] * _line(temp[dd], angles_deg32[ii], inten, psf)
 
     _run(one, n_ang, workers)
     return out[0] if n_det == 1 else out
@@ -229,6 +258,7 @@ def bp_xrf(
     weights_angles=None,
     is_symmetric: bool = False,
     workers: int = 1,
+    intensities=None,
 ) -> NDArray:
     """Back projection of ``ProjectorAttenuationXRF.bp`` (``projectors.py:533-568, 598-622``).
 
@@ -240,8 +270,12 @@ def bp_xrf(
     n = maps.shape[-1]
     sino = np.reshape(sino, [n_det, n_ang, -1])
     if not is_symmetric:
-        return np.sum(np.stack([bp_uncorrected(sino[d], angles_deg32, n, workers) for d in range(n_det)]), axis=0)
+        return np.sum(
+            np.stack([bp_uncorrected(sino[d], angles_deg32, n, workers, intensities) for d in range(n_det)]), axis=0
+        )
     w = _weights(n_ang, n_det, weights_det, weights_angles)
+    if intensities is not None:
+        w = w * np.asarray(intensities)[:, None]
     parts = np.empty((n_ang, n, n), dtype=np.result_type(sino, maps))
 
     def one(ii: int) -> None:

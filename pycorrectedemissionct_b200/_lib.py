@@ -13,6 +13,8 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcorrct_b200.so")
 
+ABI_VERSION = 2  # CCT_ABI_VERSION of include/corrct_b200.h
+
 CCT_OK = 0
 CCT_ERR_VALUE = 1
 CCT_ERR_CUDA = 2
@@ -41,6 +43,11 @@ class XrfDesc(ctypes.Structure):
         ("fp_matrix", ctypes.c_void_p),
         ("bp_trig", ctypes.c_void_p),
         ("weights", ctypes.c_void_p),
+        ("line_scale", ctypes.c_void_p),
+        ("psf", ctypes.c_void_p),
+        ("psf_len", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("maps_slice_stride", ctypes.c_int64),
     ]
 
 
@@ -93,8 +100,11 @@ class SolverState(ctypes.Structure):
         ("has_background", ctypes.c_int32),
         ("tv_lambda", ctypes.c_float),
         ("tau_shared", ctypes.c_int32),
+        ("sino_tmp", ctypes.c_void_p),
         ("residual_history", ctypes.c_void_p),
         ("history_len", ctypes.c_int32),
+        ("x_mask_per_slice", ctypes.c_int32),
+        ("joint_stop", ctypes.c_int32),
     ]
 
 
@@ -200,7 +210,7 @@ def load() -> ctypes.CDLL:
                 fn = getattr(lib, name)
                 fn.restype = res
                 fn.argtypes = args
-            if lib.cct_abi_version() != 1:
+            if lib.cct_abi_version() != ABI_VERSION:
                 raise RuntimeError("libcorrct_b200.so ABI version mismatch")
             _lib = lib
     return _lib

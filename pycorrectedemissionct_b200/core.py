@@ -52,6 +52,13 @@ def _check_tensor(t: torch.Tensor, shape: tuple, dtype: torch.dtype, device: tor
         raise ValueError(f"{name} must be contiguous")
 
 
+def _maps_stride(maps: torch.Tensor | None) -> int:
+    """Elements between consecutive slices' maps (0 = dense)."""
+    if maps is None or maps.shape[0] <= 1 or maps.is_contiguous():
+        return 0
+    return int(maps.stride(0))
+
+
 class XrfCore:
     """Geometry tables on the device plus batched projection entry points.
 
@@ -78,16 +85,49 @@ class XrfCore:
         self.trig_np = geometry.bp_trig(self.angles_deg32)
         self.fp_mat = torch.from_numpy(self.fp_mat_np).to(self.device)
         self.trig = torch.from_numpy(self.trig_np).to(self.device)
+        self.intensities_np = None
+        self.line_scale = None
+        self.psf = None
+        self._base_weights = None
         self.set_weights(weights)
 
     def set_weights(self, weights) -> None:
-        if weights is None:
+        """Detector x angle weights ``w_det[d] * w_angle[a, d]`` (None = ones)."""
+        self._base_weights = None if weights is None else np.asarray(weights, dtype=np.float64).reshape(self.n_angles, self.n_det)
+        self._sync_weights()
+
+    def set_intensities(self, intensities) -> None:
+        """Projection intensities (A,) (corrct ``projectors.py:199-201``), None to clear."""
+        if intensities is None:
+            self.intensities_np = None
+            self.line_scale = None
+        else:
+            i = np.asarray(intensities, dtype=np.float64).reshape(self.n_angles)
+            self.intensities_np = i
+            self.line_scale = torch.from_numpy(i.astype(np.float32)).to(self.device)
+        self._sync_weights()
+
+    def set_psf(self, psf) -> None:
+        """Detector point-spread function (1-D kernel), None to clear."""
+        if psf is None:
+            self.psf = None
+        else:
+            k = np.asarray(psf, dtype=np.float32).reshape(-1)
+            if not 1 <= len(k) <= 1024:
+                raise ValueError("the PSF must have between 1 and 1024 taps")
+            self.psf = torch.from_numpy(np.ascontiguousarray(k)).to(self.device)
+
+    def _sync_weights(self) -> None:
+        w = self._base_weights
+        if self.intensities_np is not None:
+            base = np.ones((self.n_angles, self.n_det)) if w is None else w
+            w = base * self.intensities_np[:, None]
+        if w is None:
             self.weights = None
             self.weights_np = None
         else:
-            w = np.asarray(weights, dtype=np.float32).reshape(self.n_angles, self.n_det)
-            self.weights_np = w
-            self.weights = torch.from_numpy(np.ascontiguousarray(w)).to(self.device)
+            self.weights_np = w.astype(np.float32)
+            self.weights = torch.from_numpy(np.ascontiguousarray(self.weights_np)).to(self.device)
 
     # ------------------------------------------------------------------ descriptors
     def desc(self, n_slices: int, maps_dtype: int = _lib.CCT_DTYPE_F32, angles: slice | None = None) -> _lib.XrfDesc:
@@ -102,12 +142,16 @@ class XrfCore:
             d.fp_matrix = self.fp_mat.data_ptr()
             d.bp_trig = self.trig.data_ptr()
             d.weights = _ptr(self.weights)
+            d.line_scale = _ptr(self.line_scale)
         else:
             a0, a1 = angles.start, angles.stop
             d.n_angles = a1 - a0
             d.fp_matrix = self.fp_mat[a0:a1].data_ptr()
             d.bp_trig = self.trig[a0:a1].data_ptr()
             d.weights = None if self.weights is None else self.weights[a0:a1].data_ptr()
+            d.line_scale = None if self.line_scale is None else self.line_scale[a0:a1].data_ptr()
+        d.psf = _ptr(self.psf)
+        d.psf_len = 0 if self.psf is None else int(self.psf.numel())
         return d
 
     # ------------------------------------------------------------------ projections
@@ -136,6 +180,7 @@ class XrfCore:
             out = torch.empty((s, self.n_det, na, n), dtype=torch.float32, device=self.device)
         _check_tensor(out, (s, self.n_det, na, n), torch.float32, self.device, "sino")
         desc = self.desc(s, mdt, angles)
+        desc.maps_slice_stride = _maps_stride(maps)
         _lib.call("cct_fp", ctypes.byref(desc), vol.data_ptr(), _ptr(maps), out.data_ptr(), stream_handle(self.device))
         return out
 
@@ -161,6 +206,7 @@ class XrfCore:
             out = torch.empty((s, n, n), dtype=torch.float32, device=self.device)
         _check_tensor(out, (s, n, n), torch.float32, self.device, "vol")
         desc = self.desc(s, mdt, angles)
+        desc.maps_slice_stride = _maps_stride(maps)
         _lib.call(
             "cct_bp", ctypes.byref(desc), BP_MODES[mode], sino.data_ptr(), _ptr(maps), out.data_ptr(),
             stream_handle(self.device),
@@ -168,12 +214,17 @@ class XrfCore:
         return out
 
     def _check_maps(self, maps: torch.Tensor, s: int, n_angles: int | None = None) -> int:
+        """Maps (S, A', D, n, n): each slice's block contiguous; the slices may be further apart
+        (an angle range of larger maps, ``maps[:, a0:a1]``)."""
         shape = (s, self.n_angles if n_angles is None else n_angles, self.n_det, self.n, self.n)
-        if maps.dtype == torch.bfloat16:
-            _check_tensor(maps, shape, torch.bfloat16, self.device, "maps")
-            return _lib.CCT_DTYPE_BF16
-        _check_tensor(maps, shape, torch.float32, self.device, "maps")
-        return _lib.CCT_DTYPE_F32
+        dtype = torch.bfloat16 if maps.dtype == torch.bfloat16 else torch.float32
+        if maps.dim() == 5 and maps.shape[0] > 1 and maps[0].is_contiguous() and maps.stride(0) >= maps[0].numel():
+            _check_tensor(maps[0], shape[1:], dtype, self.device, "maps")
+            if tuple(maps.shape) != shape:
+                raise ValueError(f"maps has shape {tuple(maps.shape)}, expected {shape}")
+        else:
+            _check_tensor(maps, shape, dtype, self.device, "maps")
+        return _lib.CCT_DTYPE_BF16 if dtype == torch.bfloat16 else _lib.CCT_DTYPE_F32
 
     def partials_count(self, n_slices: int) -> int:
         c = ctypes.c_int64(0)

@@ -11,7 +11,7 @@ int launch_maps(const cct_maps_desc* d, const float* mu_in, const float* mu_out,
                 size_t work_bytes, cudaStream_t st);
 int64_t maps_bytes_per_angle(const cct_maps_desc* d);
 void launch_residual_step(const double* partials, int64_t per_slice, int n_slices, double* residuals, int* active,
-                          int* iterations, const double* tolerance, double* history, int history_len,
+                          int* iterations, const double* tolerance, double* history, int history_len, int joint,
                           cudaStream_t st);
 void launch_tv_dual(const float* x_relax, float* q, int n, int n_slices, float lam, const int* active,
                     cudaStream_t st);
@@ -40,7 +40,17 @@ static int validate_desc(const cct_xrf_desc* d) {
   CCT_REQUIRE(d->n_slices <= 65535, "n_slices must be <= 65535");
   CCT_REQUIRE(d->maps_dtype == CCT_DTYPE_F32 || d->maps_dtype == CCT_DTYPE_BF16, "maps_dtype must be F32 or BF16");
   CCT_REQUIRE(d->fp_matrix != nullptr && d->bp_trig != nullptr, "fp_matrix and bp_trig are required");
+  CCT_REQUIRE(d->psf == nullptr || (d->psf_len >= 1 && d->psf_len <= 1024), "psf_len must be in [1, 1024]");
+  CCT_REQUIRE(d->maps_slice_stride >= 0, "maps_slice_stride must be >= 0");
+  CCT_REQUIRE(d->maps_slice_stride == 0 ||
+                  d->maps_slice_stride >= (int64_t)d->n_angles * d->n_det * d->n * d->n,
+              "maps_slice_stride must be 0 or at least n_angles * n_det * n * n");
   return CCT_OK;
+}
+
+static int64_t maps_stride(const cct_xrf_desc* d) {
+  const int64_t dense = (int64_t)d->n_angles * d->n_det * d->n * d->n;
+  return d->maps_slice_stride > 0 ? d->maps_slice_stride : dense;
 }
 
 static cct::FpArgs make_fp_args(const cct_xrf_desc* d, const float* vol, const void* maps, float* out) {
@@ -49,6 +59,7 @@ static cct::FpArgs make_fp_args(const cct_xrf_desc* d, const float* vol, const v
   a.n = d->n; a.n_angles = d->n_angles; a.n_det = d->n_det; a.n_slices = d->n_slices;
   a.maps_dtype = d->maps_dtype; a.epi = cct::FP_EPI_STORE; a.variant = d->variant;
   a.fp_matrix = d->fp_matrix; a.weights = d->weights; a.vol = vol; a.maps = maps; a.out = out;
+  a.maps_slice_stride = maps_stride(d);
   return a;
 }
 
@@ -57,8 +68,9 @@ static cct::BpArgs make_bp_args(const cct_xrf_desc* d, int mode, const float* si
   std::memset(&a, 0, sizeof(a));
   a.n = d->n; a.n_angles = d->n_angles; a.n_det = d->n_det; a.n_slices = d->n_slices;
   a.maps_dtype = d->maps_dtype; a.mode = mode; a.epi = cct::BP_EPI_STORE;
-  a.fp_matrix = d->fp_matrix; a.bp_trig = d->bp_trig; a.weights = d->weights;
+  a.fp_matrix = d->fp_matrix; a.bp_trig = d->bp_trig; a.weights = d->weights; a.line_scale = d->line_scale;
   a.sino = sino; a.maps = maps; a.out = out;
+  a.maps_slice_stride = maps_stride(d);
   return a;
 }
 
@@ -75,6 +87,11 @@ int cct_fp(const cct_xrf_desc* desc, const float* vol, const void* maps, float* 
   CCT_REQUIRE(maps != nullptr || desc->n_det == 1, "an uncorrected projection (maps == NULL) needs n_det == 1");
   cct::FpArgs a = make_fp_args(desc, vol, maps, sino);
   cct::launch_fp(a, reinterpret_cast<cudaStream_t>(stream));
+  if (desc->psf != nullptr) {
+    // in place: each CTA stages its whole line before writing it back
+    cct::FpArgs p = make_fp_args(desc, sino, maps, sino);
+    cct::launch_psf(p, desc->psf, desc->psf_len, reinterpret_cast<cudaStream_t>(stream));
+  }
   return check_launch();
 }
 
@@ -154,7 +171,7 @@ static cct::BpArgs make_solver_bp(const cct_xrf_desc* d, int mode, const void* m
   cct::BpArgs a = make_bp_args(d, mode, st->sino_buf, maps, st->vol_buf);
   a.epi = epi;
   a.x = st->x; a.x_relax = st->x_relax; a.tau = st->tau; a.tau_shared = st->tau_shared;
-  a.x_mask = st->x_mask; a.tv_dual = st->tv_dual;
+  a.x_mask = st->x_mask; a.mask_per_slice = st->x_mask_per_slice; a.tv_dual = st->tv_dual;
   a.lower = st->lower_limit; a.upper = st->upper_limit; a.has_lower = st->has_lower; a.has_upper = st->has_upper;
   a.active = st->active;
   return a;
@@ -170,12 +187,22 @@ int cct_mlem_fp(const cct_xrf_desc* desc, const void* maps, cct_solver_state* st
   cct::FpArgs f = make_fp_args(desc, st->x, maps, st->sino_buf);
   f.epi = cct::FP_EPI_MLEM; f.b = st->b; f.background = st->background; f.has_background = st->has_background;
   f.partials = st->partials; f.active = st->active;
-  cct::launch_fp(f, s);
   int64_t per_slice = 0;
-  cct_solver_partials_count(desc, &per_slice);
-  per_slice /= desc->n_slices;
+  if (desc->psf == nullptr) {
+    cct::launch_fp(f, s);
+    cct_solver_partials_count(desc, &per_slice);
+    per_slice /= desc->n_slices;
+  } else {
+    // A x into sino_buf, then the PSF with the MLEM epilogue in place (one partial per line)
+    cct::FpArgs raw = make_fp_args(desc, st->x, maps, st->sino_buf);
+    raw.active = st->active;
+    cct::launch_fp(raw, s);
+    f.vol = st->sino_buf;
+    cct::launch_psf(f, desc->psf, desc->psf_len, s);
+    per_slice = (int64_t)desc->n_det * desc->n_angles;
+  }
   cct::launch_residual_step(st->partials, per_slice, desc->n_slices, st->residuals, st->active, st->iterations,
-                            st->tolerance, st->residual_history, st->history_len, s);
+                            st->tolerance, st->residual_history, st->history_len, st->joint_stop, s);
   return check_launch();
 }
 
@@ -208,12 +235,21 @@ int cct_sirt_step(const cct_xrf_desc* desc, const void* maps, int32_t bp_mode, c
   cct::FpArgs f = make_fp_args(desc, st->x, maps, st->sino_buf);
   f.epi = cct::FP_EPI_SIRT; f.b = st->b; f.sigma = st->sigma; f.background = st->background;
   f.has_background = st->has_background; f.partials = st->partials; f.active = st->active;
-  cct::launch_fp(f, s);
   int64_t per_slice = 0;
-  cct_solver_partials_count(desc, &per_slice);
-  per_slice /= desc->n_slices;
+  if (desc->psf == nullptr) {
+    cct::launch_fp(f, s);
+    cct_solver_partials_count(desc, &per_slice);
+    per_slice /= desc->n_slices;
+  } else {
+    cct::FpArgs raw = make_fp_args(desc, st->x, maps, st->sino_buf);
+    raw.active = st->active;
+    cct::launch_fp(raw, s);
+    f.vol = st->sino_buf;
+    cct::launch_psf(f, desc->psf, desc->psf_len, s);
+    per_slice = (int64_t)desc->n_det * desc->n_angles;
+  }
   cct::launch_residual_step(st->partials, per_slice, desc->n_slices, st->residuals, st->active, st->iterations,
-                            st->tolerance, st->residual_history, st->history_len, s);
+                            st->tolerance, st->residual_history, st->history_len, st->joint_stop, s);
   cct::BpArgs b = make_solver_bp(desc, bp_mode, maps, st, cct::BP_EPI_SIRT);
   cct::launch_bp(b, s);
   return check_launch();
@@ -233,7 +269,16 @@ int cct_pdhg_step(const cct_xrf_desc* desc, const void* maps, int32_t bp_mode, c
   cct::FpArgs f = make_fp_args(desc, st->x_relax, maps, st->sino_buf);
   f.epi = cct::FP_EPI_PDHG; f.b = st->b; f.sigma = st->sigma; f.background = st->background;
   f.has_background = st->has_background; f.active = st->active;
-  cct::launch_fp(f, s);
+  if (desc->psf == nullptr) {
+    cct::launch_fp(f, s);
+  } else {
+    CCT_REQUIRE(st->sino_tmp != nullptr, "PDHG with a PSF needs sino_tmp");
+    cct::FpArgs raw = make_fp_args(desc, st->x_relax, maps, st->sino_tmp);
+    raw.active = st->active;
+    cct::launch_fp(raw, s);
+    f.vol = st->sino_tmp;
+    cct::launch_psf(f, desc->psf, desc->psf_len, s);
+  }
   cct::launch_tv_dual(st->x_relax, st->tv_dual, desc->n, desc->n_slices, st->tv_lambda, st->active, s);
   cct::BpArgs b = make_solver_bp(desc, bp_mode, maps, st, cct::BP_EPI_PDHG);
   cct::launch_bp(b, s);

@@ -18,6 +18,8 @@ enum BpEpilogue : int { BP_EPI_STORE = 0, BP_EPI_MLEM = 1, BP_EPI_SIRT = 2, BP_E
 
 struct FpArgs {
   int n, n_angles, n_det, n_slices, maps_dtype, epi, variant;
+  int vec4;                    // 16-byte staging loads allowed (n % 4 == 0 and aligned pointers)
+  int64_t maps_slice_stride;   // elements between consecutive slices' maps
   const float* fp_matrix;
   const float* weights;
   const float* vol;
@@ -33,9 +35,11 @@ struct FpArgs {
 
 struct BpArgs {
   int n, n_angles, n_det, n_slices, maps_dtype, mode, epi;
+  int64_t maps_slice_stride;   // elements between consecutive slices' maps
   const float* fp_matrix;
   const float* bp_trig;
   const float* weights;
+  const float* line_scale;  // reference mode: per-angle intensity scaling of the lines
   const float* sino;
   const void* maps;
   float* out;              // STORE target
@@ -45,6 +49,7 @@ struct BpArgs {
   const float* tau;
   int tau_shared;
   const float* x_mask;
+  int mask_per_slice;      // x_mask is [S][n][n] instead of one [n][n] mask
   const float* tv_dual;    // PDHG: updated TV dual [S][2][n][n]
   float lower, upper;
   int has_lower, has_upper;
@@ -120,17 +125,19 @@ __device__ __forceinline__ void bp_epilogue(const BpArgs& a, int s, int i, int j
     const float upd = v - (d0 + d1);
     float xn = x - upd * tau;
     xn = apply_limits(a, xn);
-    if (a.x_mask != nullptr) xn *= a.x_mask[pix];
+    if (a.x_mask != nullptr) xn *= a.x_mask[a.mask_per_slice ? idx : pix];
     a.x_relax[idx] = xn + (xn - x);
     a.x[idx] = xn;
     return;
   }
   x = apply_limits(a, x);
-  if (a.x_mask != nullptr) x *= a.x_mask[pix];
+  if (a.x_mask != nullptr) x *= a.x_mask[a.mask_per_slice ? idx : pix];
   a.x[idx] = x;
 }
 
 void launch_fp(const FpArgs& a, cudaStream_t st);
+// PSF convolution of finished sinogram lines (a.vol = input sinogram) with the fp epilogue EPI
+void launch_psf(const FpArgs& a, const float* psf, int psf_len, cudaStream_t st);
 int read_device_error(int clear, int* value);
 void launch_bp(const BpArgs& a, cudaStream_t st);
 

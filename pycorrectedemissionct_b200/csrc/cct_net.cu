@@ -16,6 +16,7 @@
 // block and commits them to that buffer's mbarrier.  Every wait is bounded; on timeout the
 // kernel raises g_net_timeout and leaves after waiting once more for its own MMAs.
 
+#include <cstdint>
 #include <cstring>
 
 #include "cct_common.cuh"
@@ -529,6 +530,9 @@ static cct::ConvArgs net_args(const cct_conv_desc* d) {
   return a;
 }
 
+// the implicit-GEMM loads move 8 bf16 (16 bytes) at a time
+static bool net_aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 static int net_bn(int cout) { return cout >= 128 ? 128 : cout; }
 
 static int net_launch_check() {
@@ -547,6 +551,7 @@ int cct_conv3x3_fwd(const cct_conv_desc* desc, const void* x, const void* w, con
   int rc = net_check_conv(desc);
   if (rc != CCT_OK) return rc;
   CCT_REQUIRE(x != nullptr && w != nullptr && y != nullptr, "x, w and y are required");
+  CCT_REQUIRE(net_aligned16(x) && net_aligned16(w) && net_aligned16(y), "x, w and y must be 16-byte aligned");
   cct::ConvArgs a = net_args(desc);
   a.x = reinterpret_cast<const __nv_bfloat16*>(x);
   a.wt = reinterpret_cast<const __nv_bfloat16*>(w);
@@ -565,6 +570,7 @@ int cct_conv3x3_wgrad(const cct_conv_desc* desc, const void* x, const void* dy, 
   int rc = net_check_conv(desc);
   if (rc != CCT_OK) return rc;
   CCT_REQUIRE(x != nullptr && dy != nullptr && dw != nullptr, "x, dy and dw are required");
+  CCT_REQUIRE(net_aligned16(x) && net_aligned16(dy), "x and dy must be 16-byte aligned");
   cct::ConvArgs a = net_args(desc);
   a.x = reinterpret_cast<const __nv_bfloat16*>(x);
   a.dy = reinterpret_cast<const __nv_bfloat16*>(dy);

@@ -116,8 +116,8 @@ __global__ void __launch_bounds__(FP_THREADS) fp_kernel(FpArgs args) {
   const int c_last = min(c0 + FP_TC, n) - 1;
 
   const float* vol = args.vol + (int64_t)s * n * n;
-  const int64_t map_off = (((int64_t)s * args.n_angles + a) * args.n_det + d) * (int64_t)n * n;
-  const bool vec4 = (n & 3) == 0;
+  const int64_t map_off = (int64_t)s * args.maps_slice_stride + ((int64_t)a * args.n_det + d) * (int64_t)n * n;
+  const bool vec4 = args.vec4 != 0;
   const float fc = (float)c;
   const float pxc = fmaf(m00, fc, m02);
   const float pyc = fmaf(m10, fc, m12);
@@ -535,6 +535,7 @@ __global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
       const int kbase = (int)floorf(tmin + (float)K) - 1;
       float w = 1.f;
       if (SYM && args.weights != nullptr) w = args.weights[a * args.n_det + d];
+      if (!SYM && args.line_scale != nullptr) w = args.line_scale[a];
       const float* line = sino + ((int64_t)d * args.n_angles + a) * n;
       if (kind != LINE_EMPTY) {
         float v[3], vn[3];
@@ -603,7 +604,7 @@ __global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
         }
         if (SYM) {
           if (i < n && j < n) {
-            const int64_t moff = (((int64_t)s * args.n_angles + a) * args.n_det + d) * (int64_t)n * n +
+            const int64_t moff = (int64_t)s * args.maps_slice_stride + ((int64_t)a * args.n_det + d) * (int64_t)n * n +
                                  (int64_t)i * n + j;
             v *= load_map(args.maps, MAPS_DTYPE, moff);
           }
@@ -665,12 +666,65 @@ __global__ void __launch_bounds__(256) bp_adjoint_kernel(BpArgs args) {
     float w = args.weights != nullptr ? args.weights[a * args.n_det + d] : 1.f;
     double contrib = lsum * w;
     if (HAS_MAPS) {
-      const int64_t moff = (((int64_t)s * args.n_angles + a) * args.n_det + d) * (int64_t)n * n + pix;
+      const int64_t moff = (int64_t)s * args.maps_slice_stride + ((int64_t)a * args.n_det + d) * (int64_t)n * n + pix;
       contrib *= load_map(args.maps, MAPS_DTYPE, moff);
     }
     acc += contrib;
   }
   bp_epilogue<BP_EPI_STORE>(args, s, pi, pj, (float)acc);
+}
+
+// ------------------------------------------------------------------------------------------
+// Detector PSF: out[i] = sum_j in[clamp(i + (L-1)/2 - j)] * k[j] along each sinogram line (the
+// reference pads with edge values, convolves with scipy 'same' and crops), followed by the same
+// fused solver epilogue as the fp.  One CTA per line; args.vol holds the unconvolved sinogram.
+// ------------------------------------------------------------------------------------------
+constexpr int PSF_THREADS = 256;
+
+template <int EPI>
+__global__ void __launch_bounds__(PSF_THREADS) psf_kernel(FpArgs args, const float* __restrict__ k, int len) {
+  extern __shared__ float line_sh[];
+  __shared__ double red_d[PSF_THREADS / 32];
+  const int n = args.n;
+  const int64_t line = blockIdx.x;  // ((s * D + d) * A + a)
+  const int s = (int)(line / ((int64_t)args.n_det * args.n_angles));
+  if (args.active != nullptr && args.active[s] == 0) return;
+  const float* in = args.vol + line * n;
+  for (int i = threadIdx.x; i < n; i += PSF_THREADS) line_sh[i] = in[i];
+  __syncthreads();
+  const int p = (len - 1) / 2;
+  double part = 0.0;
+  for (int i = threadIdx.x; i < n; i += PSF_THREADS) {
+    float acc = 0.f;
+    for (int j = 0; j < len; ++j) {
+      int q = i + p - j;
+      q = q < 0 ? 0 : (q >= n ? n - 1 : q);
+      acc = fmaf(line_sh[q], __ldg(k + j), acc);
+    }
+    part += fp_epilogue<EPI>(args, line * n + i, acc);
+  }
+  if (EPI == FP_EPI_MLEM || EPI == FP_EPI_SIRT) {
+    part = warp_sum_double(part);
+    if ((threadIdx.x & 31) == 0) red_d[threadIdx.x >> 5] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < PSF_THREADS / 32; ++w) t += red_d[w];
+      // one partial per (detector, angle) line of the slice
+      args.partials[line] = t;
+    }
+  }
+}
+
+void launch_psf(const FpArgs& a, const float* psf, int psf_len, cudaStream_t st) {
+  const unsigned lines = (unsigned)((int64_t)a.n_slices * a.n_det * a.n_angles);
+  const size_t smem = (size_t)a.n * sizeof(float);
+  switch (a.epi) {
+    case FP_EPI_MLEM: psf_kernel<FP_EPI_MLEM><<<lines, PSF_THREADS, smem, st>>>(a, psf, psf_len); break;
+    case FP_EPI_SIRT: psf_kernel<FP_EPI_SIRT><<<lines, PSF_THREADS, smem, st>>>(a, psf, psf_len); break;
+    case FP_EPI_PDHG: psf_kernel<FP_EPI_PDHG><<<lines, PSF_THREADS, smem, st>>>(a, psf, psf_len); break;
+    default: psf_kernel<FP_EPI_STORE><<<lines, PSF_THREADS, smem, st>>>(a, psf, psf_len); break;
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -735,8 +789,10 @@ template <int EPI>
 static void launch_fp_epi(const FpArgs& a, cudaStream_t st) {
   const dim3 grid((a.n + FP_TC - 1) / FP_TC, a.n_angles * a.n_det, a.n_slices);
   // TMA path: rows and images must be 16-byte multiples for both FP32 and BF16 boxes
+  const int64_t dense = (int64_t)a.n_angles * a.n_det * a.n * a.n;
   const bool aligned = (a.n % 8) == 0 && (reinterpret_cast<uintptr_t>(a.vol) % 16) == 0 &&
-                       (a.maps == nullptr || (reinterpret_cast<uintptr_t>(a.maps) % 16) == 0);
+                       (a.maps == nullptr || (reinterpret_cast<uintptr_t>(a.maps) % 16) == 0) &&
+                       a.maps_slice_stride == dense;
   if (aligned && (a.variant & CCT_VARIANT_FP_TMA)) {
     bool ok;
     if (a.maps == nullptr) {
@@ -748,12 +804,18 @@ static void launch_fp_epi(const FpArgs& a, cudaStream_t st) {
     }
     if (ok) return;
   }
+  // 16-byte staging loads need a 16-byte aligned volume, maps at 16 (FP32) or 8 (BF16) bytes and
+  // map images that stay aligned (n % 4 == 0, slice stride a multiple of 4 elements)
+  FpArgs v = a;
+  const uintptr_t map_align = a.maps_dtype == CCT_DTYPE_BF16 ? 8 : 16;
+  v.vec4 = (a.n % 4) == 0 && (reinterpret_cast<uintptr_t>(a.vol) % 16) == 0 &&
+           (a.maps == nullptr || ((reinterpret_cast<uintptr_t>(a.maps) % map_align) == 0 && a.maps_slice_stride % 4 == 0));
   if (a.maps == nullptr) {
-    fp_kernel<EPI, false, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(a);
+    fp_kernel<EPI, false, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(v);
   } else if (a.maps_dtype == CCT_DTYPE_BF16) {
-    fp_kernel<EPI, true, CCT_DTYPE_BF16><<<grid, FP_THREADS, 0, st>>>(a);
+    fp_kernel<EPI, true, CCT_DTYPE_BF16><<<grid, FP_THREADS, 0, st>>>(v);
   } else {
-    fp_kernel<EPI, true, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(a);
+    fp_kernel<EPI, true, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(v);
   }
 }
 

@@ -91,11 +91,40 @@ __global__ void __launch_bounds__(RED_THREADS) norm_final_kernel(const double* p
   if (threadIdx.x == 0) out[s] = acc;
 }
 
+// A 3-D volume solved as a stack of slices: the reference computes one residual norm over the
+// whole volume, which for its additive norms (sum |r|, sum r^2) is the sum of the slice residuals.
+// Runs after residual_step_kernel of the same iteration; one CTA, fixed summation order.
+__global__ void __launch_bounds__(RED_THREADS) residual_joint_kernel(const double* residuals, int n_slices,
+                                                                     int* active, const int* iterations,
+                                                                     const double* tolerance, double* history,
+                                                                     int history_len) {
+  if (active[0] == 0) return;  // the volume met its tolerance at an earlier iteration
+  double v = 0.0;
+  for (int s = threadIdx.x; s < n_slices; s += RED_THREADS) v += residuals[s];
+  v = block_sum_double(v);
+  __shared__ int stop;
+  if (threadIdx.x == 0) {
+    const int it = iterations[0] - 1;
+    if (history != nullptr && it >= 0 && it < history_len) history[it] = v;
+    stop = (tolerance != nullptr && tolerance[0] > v) ? 1 : 0;
+  }
+  __syncthreads();
+  if (stop)
+    for (int s = threadIdx.x; s < n_slices; s += RED_THREADS) active[s] = 0;
+}
+
 void launch_residual_step(const double* partials, int64_t per_slice, int n_slices, double* residuals, int* active,
-                          int* iterations, const double* tolerance, double* history, int history_len,
+                          int* iterations, const double* tolerance, double* history, int history_len, int joint,
                           cudaStream_t st) {
+  if (!joint) {
+    residual_step_kernel<<<n_slices, RED_THREADS, 0, st>>>(partials, per_slice, residuals, active, iterations,
+                                                            tolerance, history, history_len);
+    return;
+  }
   residual_step_kernel<<<n_slices, RED_THREADS, 0, st>>>(partials, per_slice, residuals, active, iterations,
-                                                          tolerance, history, history_len);
+                                                          nullptr, nullptr, 0);
+  residual_joint_kernel<<<1, RED_THREADS, 0, st>>>(residuals, n_slices, active, iterations, tolerance, history,
+                                                   history_len);
 }
 
 void launch_tv_dual(const float* x_relax, float* q, int n, int n_slices, float lam, const int* active,

@@ -38,6 +38,11 @@ class BatchedSolver:
     method : "mlem" | "sirt" | "pdhg"
     tolerance : (S,) array, float, or None
         Stop a slice when ``tolerance > residual`` (the reference's rule).
+    x_mask : (n, n) or (S, n, n) tensor or None
+    joint_stop : bool
+        The S slices are one 3-D volume: a single stopping test on the residual summed over the
+        slices (the reference's norm over the whole volume, compared with ``tolerance[0]``); the
+        per-iteration volume residual is row 0 of ``history``.
     """
 
     def __init__(
@@ -56,6 +61,7 @@ class BatchedSolver:
         bp_mode: str = "reference",
         background: float | None = None,
         history_len: int = 0,
+        joint_stop: bool = False,
     ):
         self.core = core
         self.device = core.device
@@ -94,7 +100,9 @@ class BatchedSolver:
             ones_b = torch.ones_like(self.b)
             tau = core.bp(ones_b, bp_mode, bp_maps).abs_()
             tau += reg_tau
-            tmax = tau.amax(dim=(1, 2), keepdim=True)
+            # the reference scales by the maximum over its whole volume: per slice for independent
+            # 2-D slices, over the stack for one 3-D volume (solvers.py:90-117)
+            tmax = tau.amax() if joint_stop else tau.amax(dim=(1, 2), keepdim=True)
             tau = torch.where(tau / tmax < 1e-5, torch.ones_like(tau), tau)
             self.tau = (relax / tau).contiguous()
             self.tau_shared = 0
@@ -102,7 +110,7 @@ class BatchedSolver:
             if x_mask is not None:
                 x_ones *= x_mask
             sig = core.fp(x_ones, maps).abs_()
-            smax = sig.amax(dim=(1, 2, 3), keepdim=True)
+            smax = sig.amax() if joint_stop else sig.amax(dim=(1, 2, 3), keepdim=True)
             sig = torch.where(sig / smax < 1e-5, torch.ones_like(sig), sig)
             sig_relax = relax if self.method == "pdhg" else 1.0
             self.sigma = (sig_relax / sig).contiguous()
@@ -110,6 +118,8 @@ class BatchedSolver:
         self.x_relax = self.x.clone() if self.method == "pdhg" else None
         self.tv_dual = torch.zeros((s, 2, n, n), **f32) if self.method == "pdhg" else None
         self.sino_buf = torch.zeros_like(self.b)
+        # PDHG with a detector PSF keeps the raw projection apart from the dual variable
+        self.sino_tmp = torch.empty_like(self.b) if (self.method == "pdhg" and core.psf is not None) else None
         self.vol_buf = torch.empty((s, n, n), **f32)
         self.partials = torch.zeros(max(core.partials_count(s), 1), dtype=torch.float64, device=dev)
         self.residuals = torch.zeros(s, dtype=torch.float64, device=dev)
@@ -121,6 +131,8 @@ class BatchedSolver:
             tol = np.broadcast_to(np.asarray(tolerance, dtype=np.float64), (s,)).copy()
             self.tolerance = torch.from_numpy(tol).to(dev)
         self.x_mask = None if x_mask is None else x_mask.to(**f32).contiguous()
+        if self.x_mask is not None and tuple(self.x_mask.shape) not in ((n, n), (s, n, n)):
+            raise ValueError(f"x_mask must have shape {(n, n)} or {(s, n, n)}")
 
         st = _lib.SolverState()
         st.x = self.x.data_ptr()
@@ -145,9 +157,13 @@ class BatchedSolver:
         st.background = float(background) if background is not None else 0.0
         st.tv_lambda = float(tv_lambda)
         st.tau_shared = self.tau_shared
+        st.sino_tmp = None if self.sino_tmp is None else self.sino_tmp.data_ptr()
         self.history = torch.zeros((s, history_len), dtype=torch.float64, device=dev) if history_len > 0 else None
         st.residual_history = None if self.history is None else self.history.data_ptr()
         st.history_len = int(history_len)
+        st.x_mask_per_slice = int(self.x_mask is not None and self.x_mask.dim() == 3)
+        st.joint_stop = int(joint_stop)
+        self.joint_stop = bool(joint_stop)
         self.state = st
         self.desc = core.desc(s, self.maps_dtype)
         self._maps_ptr = None if maps is None else maps.data_ptr()

@@ -80,14 +80,28 @@ class ProjectorUncorrected(ProjectorOperator):
             create_single_projs=create_single_projs,
         )
         if prj_intensities is not None:
-            raise NotImplementedError("prj_intensities is not supported by the B200 backend yet")
-        if psf is not None:
-            raise NotImplementedError("psf is not supported by the B200 backend yet")
-        self.prj_intensities = None
-        self.psf_vu = self.psf_vwu = None
+            prj_intensities = np.array(prj_intensities, dtype=np.float64)
+        self.prj_intensities = prj_intensities
+        self.projector_backend.core.set_intensities(prj_intensities)
+        self._set_psf(psf)
         self.vol_shape = np.array(self.projector_backend.get_vol_shape(), ndmin=1)
         self.prj_shape = np.array(self.projector_backend.get_prj_shape(), ndmin=1)
         super().__init__()
+
+    def _set_psf(self, psf) -> None:
+        """Detector PSF along u (corrct ``projectors.py:229-244``); 2-D volumes take a 1-D PSF."""
+        if psf is not None:
+            psf = np.squeeze(np.array(psf, dtype=np.float64))
+            if psf.ndim >= len(self.vol_geom.shape_xyz):
+                raise ValueError(
+                    "PSF should either be 1D (for 2D and 3D reconstructions) or 2D (for 3D reconstructions)."
+                    + f" Passed PSF has shape: {psf.shape}, and the reconstruction is {len(self.vol_geom.shape_xyz)}D."
+                )
+            psf = np.atleast_1d(psf)
+            if psf.ndim > 1:
+                raise NotImplementedError("the B200 projectors apply 1-D PSFs (along the detector) only")
+        self.psf = psf
+        self.projector_backend.core.set_psf(psf)
 
     @property
     def angles_rot_rad(self) -> np.ndarray:
@@ -193,8 +207,10 @@ class ProjectorAttenuationXRF(ProjectorUncorrected):
             m = AttenuationVolume(att_in, att_out, self.angles_rot_rad, self.angles_det_rad, maps_dtype=maps_dtype, device=device)
             m.compute_maps(use_multithreading=self.use_multithreading, verbose=self.verbose)
             maps_dev = m.maps_device
-            if maps_dev.shape[0] != 1:
-                raise ValueError("The B200 XRF projector handles 2-D slices; pass one slice of attenuation")
+            if maps_dev.shape[0] != self._n_slices():
+                raise ValueError(
+                    f"Attenuation volumes of {maps_dev.shape[0]} slices do not match the volume's {self._n_slices()}"
+                )
         else:
             if att_maps.shape[1] != num_det_angles:
                 raise ValueError(f"Number of maps ({att_maps.shape[1]}) differs from number of detectors ({num_det_angles})")
@@ -203,10 +219,8 @@ class ProjectorAttenuationXRF(ProjectorUncorrected):
                     f"Mismatching volume shape of input volume ({att_maps.shape[-2:]})"
                     + f" with vol_shape ({self.vol_shape} in 2D -> {self.vol_shape[-2:]})"
                 )
-            tdt = _core.MAPS_DTYPES[maps_dtype][0]
-            src = att_maps if isinstance(att_maps, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(att_maps))
-            maps_dev = src.to(device=device, dtype=tdt).reshape(1, *src.shape).contiguous()
-        self._maps = maps_dev  # (1, A, D, n, n)
+            maps_dev = self._maps_to_device(att_maps)
+        self._maps = maps_dev  # (Z, A, D, n, n)
         self._maps_host = None
         self._sync_weights()
         self.executor = None
@@ -215,25 +229,44 @@ class ProjectorAttenuationXRF(ProjectorUncorrected):
     def _sync_weights(self) -> None:
         w = np.asarray(self.weights_det, dtype=np.float64)[None, :] * np.asarray(self.weights_angles, dtype=np.float64)
         self.core.n_det = len(self.angles_det_rad)
-        self.core.set_weights(w)
+        self.core.set_weights(w)  # intensities (set at construction) are folded in by the core
+
+    def _is_3d(self) -> bool:
+        return len(self.vol_shape) == 3
+
+    def _n_slices(self) -> int:
+        return self.projector_backend.n_slices
+
+    def _maps_to_device(self, maps) -> torch.Tensor:
+        """Reference layout ``(A, D, [Z,] n, n)`` -> device layout ``(Z, A, D, n, n)``."""
+        tdt = _core.MAPS_DTYPES[self.maps_dtype][0]
+        src = maps if isinstance(maps, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(maps))
+        src = src.to(device=self.projector_backend.device)
+        if self._is_3d():
+            if src.dim() != 5 or src.shape[2] != self._n_slices():
+                raise ValueError(f"3-D maps must have shape (A, D, {self._n_slices()}, n, n), got {tuple(src.shape)}")
+            src = src.permute(2, 0, 1, 3, 4)
+        else:
+            src = src.reshape(1, *src.shape[-4:])
+        return src.to(dtype=tdt).contiguous()
 
     @property
     def att_vol_angles(self) -> np.ndarray:
-        """Host copy of the maps ``(A, D, n, n)`` (the reference attribute)."""
+        """Host copy of the maps ``(A, D, n, n)``, or ``(A, D, Z, n, n)`` for a 3-D volume (the reference attribute)."""
         if self._maps_host is None:
-            self._maps_host = self._maps[0].float().cpu().numpy()
+            m = self._maps.float()
+            m = m.permute(1, 2, 0, 3, 4) if self._is_3d() else m[0]
+            self._maps_host = m.cpu().numpy()
         return self._maps_host
 
     @att_vol_angles.setter
     def att_vol_angles(self, maps) -> None:
-        tdt = _core.MAPS_DTYPES[self.maps_dtype][0]
-        src = maps if isinstance(maps, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(maps))
-        self._maps = src.to(device=self.projector_backend.device, dtype=tdt).reshape(1, *src.shape).contiguous()
+        self._maps = self._maps_to_device(maps)
         self._maps_host = None
 
     @property
     def maps_device(self) -> torch.Tensor:
-        """Device maps ``(1, A, D, n, n)`` as consumed by the kernels."""
+        """Device maps ``(Z, A, D, n, n)`` as consumed by the kernels (Z = 1 for a 2-D volume)."""
         return self._maps
 
     def __enter__(self):
@@ -259,39 +292,56 @@ class ProjectorAttenuationXRF(ProjectorUncorrected):
     def _n_det(self) -> int:
         return len(self.angles_det_rad)
 
-    def fp(self, vol):
-        """Attenuated forward projection (corrct ``projectors.py:570-596``)."""
-        dev = self.projector_backend.device
-        v, as_np = _to_device(vol, dev)
-        sino = self.core.fp(v.reshape(1, *v.shape[-2:]), self._maps)[0]  # (D, A, n)
+    def _from_device_sino(self, sino: torch.Tensor) -> torch.Tensor:
+        """Device (Z, D, A', n) -> the reference's (D, [Z,] A', n) with a size-1 D dropped."""
+        sino = sino.permute(1, 0, 2, 3) if self._is_3d() else sino[0]
         if sino.shape[0] == 1:
             sino = sino[0]
-            if sino.shape[0] == 1:
-                sino = sino[0]
+        return sino
+
+    def _to_device_sino(self, y: torch.Tensor, n_lines: int) -> torch.Tensor:
+        """The reference's (D, [Z,] A', n) (a size-1 D may be absent) -> device (Z, D, A', n)."""
+        n = int(self.vol_shape[-1])
+        z = self._n_slices()
+        if self._is_3d():
+            return y.reshape(self._n_det(), z, n_lines, n).permute(1, 0, 2, 3).contiguous()
+        return y.reshape(1, self._n_det(), n_lines, n).contiguous()
+
+    def fp(self, vol):
+        """Attenuated forward projection (corrct ``projectors.py:570-596``).
+
+        (n, n) -> (D, A, n); a 3-D volume (Z, n, n) -> (D, Z, A, n); D = 1 is squeezed, as is a
+        leading axis of size 1 after that."""
+        dev = self.projector_backend.device
+        v, as_np = _to_device(vol, dev)
+        n = int(self.vol_shape[-1])
+        sino = self._from_device_sino(self.core.fp(v.reshape(self._n_slices(), n, n), self._maps))
+        if sino.shape[0] == 1:
+            sino = sino[0]
         return _out(sino, as_np, self.data_type)
 
     def bp(self, sino):
         """Back projection (corrct ``projectors.py:598-622``)."""
         dev = self.projector_backend.device
         y, as_np = _to_device(sino, dev)
-        n = int(self.vol_shape[-1])
-        y = y.reshape(1, self._n_det(), len(self.angles_rot_rad), n)
+        y = self._to_device_sino(y, len(self.angles_rot_rad))
         if self.bp_mode == "adjoint":
             vol = self.core.bp(y, "adjoint", self._maps)
         elif self.is_symmetric:
             vol = self.core.bp(y, "symmetric", self._maps)
         else:
             vol = self.core.bp(y, "reference")
-        return _out(vol[0], as_np, self.data_type)
+        return _out(vol if self._is_3d() else vol[0], as_np, self.data_type)
 
     def fp_angle(self, vol, angle_ind: int):
-        """Forward-project one angle (corrct ``projectors.py:502-531``)."""
+        """Forward-project one angle (corrct ``projectors.py:502-531``): (D, [Z,] n), D = 1 squeezed."""
         dev = self.projector_backend.device
         v, as_np = _to_device(vol, dev)
         a = int(angle_ind)
-        sino = self.core.fp(v.reshape(1, *v.shape[-2:]), self._maps[:, a : a + 1], angles=slice(a, a + 1))[0, :, 0]
-        if sino.shape[0] == 1:
-            sino = sino[0]
+        n = int(self.vol_shape[-1])
+        sino = self.core.fp(v.reshape(self._n_slices(), n, n), self._maps[:, a : a + 1], angles=slice(a, a + 1))
+        sino = self._from_device_sino(sino[:, :, :1])
+        sino = sino[..., 0, :]
         return _out(sino, as_np, self.data_type)
 
     def bp_angle(self, sino, angle_ind: int, single_line: bool = False):
@@ -299,16 +349,21 @@ class ProjectorAttenuationXRF(ProjectorUncorrected):
         dev = self.projector_backend.device
         y, as_np = _to_device(sino, dev)
         a = int(angle_ind)
-        n = int(self.vol_shape[-1])
         if not single_line:
             y = y[..., a, :]
-        y = y.reshape(1, self._n_det(), 1, n).contiguous()
+        y = self._to_device_sino(y, 1)
         if self.is_symmetric:
             vol = self.core.bp(y, "symmetric", self._maps[:, a : a + 1], angles=slice(a, a + 1))
         else:
-            # weights apply per line even without maps (projectors.py:553-557): scale, then plain bp
+            # weights (w_det * w_angle * intensity) apply per line even without maps
+            # (projectors.py:553-557, 296-297): scale, then the plain bp without the line scale
             w = self.core.weights[a] if self.core.weights is not None else None
             if w is not None:
                 y = y * w.reshape(1, -1, 1, 1)
-            vol = self.core.bp(y.contiguous(), "reference", angles=slice(a, a + 1))
-        return _out(vol[0], as_np, self.data_type)
+            saved = self.core.line_scale
+            self.core.line_scale = None
+            try:
+                vol = self.core.bp(y.contiguous(), "reference", angles=slice(a, a + 1))
+            finally:
+                self.core.line_scale = saved
+        return _out(vol if self._is_3d() else vol[0], as_np, self.data_type)

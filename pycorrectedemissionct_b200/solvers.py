@@ -64,28 +64,45 @@ def _data_term_name(data_term) -> tuple[str, float | None]:
     return name, (None if bg is None else float(np.asarray(bg)))
 
 
+def _tensor(v, dev) -> torch.Tensor:
+    t = v if isinstance(v, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(v, dtype=np.float32))
+    return t.to(dev, torch.float32)
+
+
 def _as_batch(A, b, x0, x_mask):
+    """Device tensors of one solve: b (Z, D, A, n), x0 (Z, n, n), mask (n, n) or (Z, n, n), maps.
+
+    A 3-D volume of Z slices (data (D, Z, A, n) in the reference's order) is solved as Z slices
+    with a joint stopping test."""
     dev = A.projector_backend.device
     n = int(A.vol_shape[-1])
+    z = A.projector_backend.n_slices
     n_det = A._n_det() if isinstance(A, ProjectorAttenuationXRF) else 1
     n_ang = len(A.angles_rot_rad)
     as_np = not isinstance(b, torch.Tensor)
-    bt = torch.as_tensor(np.ascontiguousarray(b, dtype=np.float32) if as_np else b).to(dev, torch.float32)
-    bt = bt.reshape(1, n_det, n_ang, n).contiguous()
-    x0t = None if x0 is None else torch.as_tensor(np.asarray(x0, dtype=np.float32) if not isinstance(x0, torch.Tensor) else x0).to(dev, torch.float32).reshape(1, n, n)
-    mt = None if x_mask is None else torch.as_tensor(np.asarray(x_mask, dtype=np.float32) if not isinstance(x_mask, torch.Tensor) else x_mask).to(dev, torch.float32).reshape(n, n)
+    bt = _tensor(b, dev).reshape(n_det, z, n_ang, n).permute(1, 0, 2, 3).contiguous()
+    x0t = None if x0 is None else _tensor(x0, dev).reshape(z, n, n).contiguous()
+    mt = None
+    if x_mask is not None:
+        mt = _tensor(x_mask, dev)
+        mt = mt.reshape(n, n) if mt.numel() == n * n else mt.reshape(z, n, n)
+        mt = mt.contiguous()
     maps = A.maps_device if isinstance(A, ProjectorAttenuationXRF) else None
     return bt, x0t, mt, maps, as_np
 
 
-def _finish(solver: BatchedSolver, info: SolutionInfo, iterations: int, as_np: bool):
+def _is_volume(A) -> bool:
+    return len(A.vol_shape) == 3
+
+
+def _finish(solver: BatchedSolver, info: SolutionInfo, iterations: int, as_np: bool, volume: bool = False):
     torch.cuda.current_stream(solver.device).synchronize()
     info.iterations = int(solver.iterations[0].item())
     if solver.history is not None:
         h = solver.history[0].cpu().numpy()
         k = min(info.iterations, iterations)
         info.residuals[:k] = h[:k]
-    x = solver.x[0]
+    x = solver.x if volume else solver.x[0]
     return (x.cpu().numpy() if as_np else x.clone()), info
 
 
@@ -133,12 +150,13 @@ class MLEM(Solver):
         solver = BatchedSolver(
             A.core, maps, bt, "mlem", tolerance=self.tolerance, x0=x0t, x_mask=mt,
             lower_limit=lower_limit, upper_limit=upper_limit, background=self.background, history_len=iterations,
+            joint_stop=_is_volume(A),
         )
         info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
         if self.tolerance is not None:
             info.residual0 = _kl_residual_norm(A.core.fp(solver.x, maps), bt, self.background)
         solver.run(iterations, check_every=10 if self.tolerance is not None else max(iterations, 1))
-        return _finish(solver, info, iterations, as_np)
+        return _finish(solver, info, iterations, as_np, _is_volume(A))
 
 
 class SIRT(Solver):
@@ -159,11 +177,11 @@ class SIRT(Solver):
         solver = BatchedSolver(
             A.core, maps, bt, "sirt", tolerance=self.tolerance, x0=x0t, x_mask=mt, lower_limit=lower_limit,
             upper_limit=upper_limit, relaxation=self.relaxation, bp_mode=bp_mode, background=self.background,
-            history_len=iterations,
+            history_len=iterations, joint_stop=_is_volume(A),
         )
         info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
         solver.run(iterations, check_every=10 if self.tolerance is not None else max(iterations, 1))
-        return _finish(solver, info, iterations, as_np)
+        return _finish(solver, info, iterations, as_np, _is_volume(A))
 
 
 class PDHG(Solver):
@@ -195,10 +213,11 @@ class PDHG(Solver):
         solver = BatchedSolver(
             A.core, maps, bt, "pdhg", x_mask=mt, lower_limit=lower_limit, upper_limit=upper_limit,
             relaxation=self.relaxation, tv_lambda=self.tv_weight, bp_mode=bp_mode, background=self.background,
+            joint_stop=_is_volume(A),
         )
         info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
         solver.run(iterations, check_every=max(iterations, 1))
-        x, info = _finish(solver, info, iterations, as_np)
+        x, info = _finish(solver, info, iterations, as_np, _is_volume(A))
         info.iterations = iterations
         return x, info
 
@@ -229,7 +248,6 @@ class SART(Solver):
         if b_mask is not None:
             raise NotImplementedError("b_mask is not supported by the B200 SART")
         dev = A.projector_backend.device
-        n = int(A.vol_shape[-1])
         n_ang = len(A.angles_rot_rad)
         as_np = not isinstance(b, torch.Tensor)
         bt = torch.as_tensor(np.ascontiguousarray(b, dtype=np.float32) if as_np else b).to(dev, torch.float32)
@@ -240,14 +258,15 @@ class SART(Solver):
         tau = torch.stack([bpa(b_ones[..., ii, :].contiguous(), ii) for ii in range(n_ang)], dim=-2).abs()
         tau = torch.where(tau / tau.max() < 1e-5, torch.ones_like(tau), tau)
         tau = self.relaxation / tau
-        x_ones = torch.ones((n, n), device=dev)
+        vol_shape = tuple(int(v) for v in A.vol_shape)
+        x_ones = torch.ones(vol_shape, device=dev)
         if x_mask is not None:
-            x_ones = x_ones * torch.as_tensor(np.asarray(x_mask, dtype=np.float32)).to(dev)
+            x_ones = x_ones * _tensor(x_mask, dev)
         sigma = torch.stack([fpa(x_ones, ii) for ii in range(n_ang)], dim=-2).abs()
         sigma = torch.where(sigma / sigma.max() < 1e-5, torch.ones_like(sigma), sigma)
         sigma = 1 / sigma
-        x = torch.zeros((n, n), device=dev) if x0 is None else torch.as_tensor(np.asarray(x0, dtype=np.float32)).to(dev).clone()
-        mask = None if x_mask is None else torch.as_tensor(np.asarray(x_mask, dtype=np.float32)).to(dev)
+        x = torch.zeros(vol_shape, device=dev) if x0 is None else _tensor(x0, dev).reshape(vol_shape).clone()
+        mask = None if x_mask is None else _tensor(x_mask, dev)
         info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
         rows_sequence = np.random.permutation(n_ang)
         for ii in range(iterations):
@@ -292,17 +311,18 @@ class FISTA(Solver):
         fp = lambda v: core.fp(v, maps)  # noqa: E731
         bp = lambda y: core.bp(y, bp_mode, maps if bp_mode == "symmetric" else None)  # noqa: E731
         n = core.n
+        z = bt.shape[0]
         # compute_diagonal_scaling (solvers.py:60-117), relaxation on tau
         tau = bp(torch.ones_like(bt)).abs()
         tau = torch.where(tau / tau.max() < 1e-5, torch.ones_like(tau), tau)
         tau = self.relaxation / tau
-        x_ones = torch.ones((1, n, n), device=core.device)
+        x_ones = torch.ones((z, n, n), device=core.device)
         if mt is not None:
             x_ones = x_ones * mt
         sigma = fp(x_ones).abs()
         sigma = torch.where(sigma / sigma.max() < 1e-5, torch.ones_like(sigma), sigma)
         sigma = 1.0 / sigma
-        x = torch.zeros((1, n, n), device=core.device) if x0t is None else x0t.clone()
+        x = torch.zeros((z, n, n), device=core.device) if x0t is None else x0t.clone()
         if mt is not None:
             x = x * mt
         y = x.clone()
@@ -329,4 +349,5 @@ class FISTA(Solver):
                 info.residuals[ii] = float(torch.sum(r.double() ** 2).item())
                 if self.tolerance > info.residuals[ii]:
                     break
-        return (x[0].cpu().numpy() if as_np else x[0]), info
+        x = x if _is_volume(A) else x[0]
+        return (x.cpu().numpy() if as_np else x), info

@@ -26,16 +26,18 @@ from oracle.reference_import import load_corrct  # noqa: E402
 from pycorrectedemissionct_b200 import phantoms  # noqa: E402
 
 CASES = [
-    # name, N, A, detector angles, detector weights, random angle weights, seed
-    ("n32_a16", 32, 16, [np.pi / 2], None, False, 11),
-    ("n33_a9", 33, 9, [np.pi / 2], None, False, 12),
-    ("n16_a7_d2", 16, 7, [np.pi / 2, np.pi / 3], [1.0, 0.5], True, 13),
-    ("n64_a48", 64, 48, [np.pi / 2], None, False, 14),
+    # name, N, A, detector angles, detector weights, random angle weights, seed, psf + intensities
+    ("n32_a16", 32, 16, [np.pi / 2], None, False, 11, False),
+    ("n33_a9", 33, 9, [np.pi / 2], None, False, 12, False),
+    ("n16_a7_d2", 16, 7, [np.pi / 2, np.pi / 3], [1.0, 0.5], True, 13, False),
+    ("n64_a48", 64, 48, [np.pi / 2], None, False, 14, False),
+    ("n32_a16_psf", 32, 16, [np.pi / 2], None, False, 15, True),
+    ("n24_a10_d2_psf", 24, 10, [np.pi / 2, 2.0], [1.0, 0.7], True, 16, True),
 ]
 ITERATIONS = 10
 
 
-def make_case(corrct, name, n, n_ang, det_angles, det_weights, rand_ang_w, seed):
+def make_case(corrct, name, n, n_ang, det_angles, det_weights, rand_ang_w, seed, with_psf):
     rng = phantoms.slice_rng(seed, 0)
     x = phantoms.ellipse_phantom(n, rng, num_ellipses=6, dtype=np.float64)
     mu_in = phantoms.disk_attenuation(n, rng, mu_max=0.05, num_disks=3, dtype=np.float64)
@@ -49,7 +51,13 @@ def make_case(corrct, name, n, n_ang, det_angles, det_weights, rand_ang_w, seed)
     att.compute_maps(use_multithreading=False, verbose=False)
     maps = att.get_maps()
 
+    psf = np.array([0.05, 0.2, 0.5, 0.15, 0.1]) if with_psf else None
+    # prj_intensities cannot be passed to the reference under numpy >= 2 (projectors.py:200 builds
+    # np.array(..., dtype=np.floating), which numpy 2 rejects); the port checks them instead
+    intensities = None
     common = dict(
+        psf=psf,
+        prj_intensities=intensities,
         att_maps=maps,
         angles_detectors_rad=det_angles,
         weights_detectors=det_weights,
@@ -60,7 +68,7 @@ def make_case(corrct, name, n, n_ang, det_angles, det_weights, rand_ang_w, seed)
     )
     p = corrct.projectors.ProjectorAttenuationXRF((n, n), angles, **common)
     ps = corrct.projectors.ProjectorAttenuationXRF((n, n), angles, is_symmetric=True, **common)
-    pu = corrct.projectors.ProjectorUncorrected((n, n), angles, backend="skimage")
+    pu = corrct.projectors.ProjectorUncorrected((n, n), angles, backend="skimage", psf=psf, prj_intensities=intensities)
 
     fp_att = p.fp(x)
     y = rng.uniform(0.0, 1.0, size=fp_att.shape)
@@ -76,6 +84,8 @@ def make_case(corrct, name, n, n_ang, det_angles, det_weights, rand_ang_w, seed)
         maps=maps,
         fp_att=fp_att,
         y=y,
+        psf=np.zeros(0) if psf is None else psf,
+        intensities=np.zeros(0) if intensities is None else intensities,
         bp_att=p.bp(y),
         bp_sym=ps.bp(y),
         fp_unc=pu.fp(x),

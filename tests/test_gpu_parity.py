@@ -18,7 +18,7 @@ TOL = 1e-5
 TOL_RECON = 1e-4
 TOL_ADJ = 1e-6
 
-CASES = ["n32_a16", "n33_a9", "n16_a7_d2", "n64_a48"]
+CASES = ["n32_a16", "n33_a9", "n16_a7_d2", "n64_a48", "n32_a16_psf", "n24_a10_d2_psf"]
 
 
 @pytest.fixture(scope="module")
@@ -33,7 +33,10 @@ def _core(g, cuda):
 
     n_det = len(g["det_angles"])
     w = np.asarray(g["det_weights"])[None, :] * np.asarray(g["weights_angles"])
-    return core.XrfCore(int(g["n"]), g["angles"], n_det=n_det, weights=w, device=cuda)
+    c = core.XrfCore(int(g["n"]), g["angles"], n_det=n_det, weights=w, device=cuda)
+    if g["psf"].size:
+        c.set_psf(g["psf"])
+    return c
 
 
 def _t(a, cuda, dtype=torch.float32):
@@ -70,13 +73,42 @@ def test_fp_bp_match_reference(golden_cases, case, cuda):
         assert rel_l2(cu.bp(y, "reference")[0].cpu().numpy(), g["bp_unc"]) < TOL
 
 
-@pytest.mark.parametrize("case", ["n32_a16", "n33_a9", "n64_a48"])
+def test_intensities_and_psf_against_port(golden_cases, cuda):
+    """Projection intensities (checked against the port: the reference's own intensity path
+    raises under numpy >= 2) combined with a PSF, through the public projector."""
+    from oracle import port
+    from pycorrectedemissionct_b200 import projectors
+
+    g = golden_cases["n24_a10_d2_psf"]
+    n, n_ang = int(g["n"]), len(g["angles"])
+    rng = np.random.default_rng(21)
+    inten = rng.uniform(0.5, 1.5, size=n_ang)
+    _, deg32 = port.backend_angles(g["angles"])
+    kw = dict(att_maps=g["maps"], angles_detectors_rad=g["det_angles"], weights_detectors=g["det_weights"],
+              weights_angles=g["weights_angles"], psf=g["psf"], prj_intensities=inten)
+    p = projectors.ProjectorAttenuationXRF((n, n), g["angles"], **kw)
+    ref_fp = port.fp_xrf(g["x"], g["maps"], deg32, g["det_weights"], g["weights_angles"], intensities=inten, psf=g["psf"])
+    assert rel_l2(p.fp(g["x"]), ref_fp) < TOL
+    ref_bp = port.bp_xrf(g["y"], g["maps"], deg32, intensities=inten)
+    assert rel_l2(p.bp(g["y"]), ref_bp) < TOL
+    ps = projectors.ProjectorAttenuationXRF((n, n), g["angles"], is_symmetric=True, **kw)
+    ref_bs = port.bp_xrf(g["y"], g["maps"], deg32, g["det_weights"], g["weights_angles"], True, intensities=inten)
+    assert rel_l2(ps.bp(g["y"]), ref_bs) < TOL
+    # single-angle paths
+    for a in (0, 3):
+        line = port.fp_xrf(g["x"], g["maps"][a : a + 1], deg32[a : a + 1], g["det_weights"], g["weights_angles"][a : a + 1],
+                           intensities=inten[a : a + 1], psf=g["psf"])
+        assert rel_l2(p.fp_angle(g["x"], a), line[:, 0]) < TOL
+
+
+@pytest.mark.parametrize("case", ["n32_a16", "n33_a9", "n64_a48", "n32_a16_psf"])
 def test_solvers_match_reference(golden_cases, case, cuda):
     from pycorrectedemissionct_b200 import projectors, solvers
 
     g = golden_cases[case]
     n = int(g["n"])
-    p = projectors.ProjectorAttenuationXRF((n, n), g["angles"], att_maps=g["maps"], angles_detectors_rad=g["det_angles"])
+    psf = g["psf"] if g["psf"].size else None
+    p = projectors.ProjectorAttenuationXRF((n, n), g["angles"], att_maps=g["maps"], angles_detectors_rad=g["det_angles"], psf=psf)
     xm, info = solvers.MLEM(tolerance=0.0)(p, g["b"], iterations=10)
     assert rel_l2(xm, g["mlem_x"]) < TOL_RECON
     np.testing.assert_allclose(info.residuals[:10], g["mlem_res"], rtol=TOL_RECON)

@@ -82,7 +82,7 @@ def test_library_exports_every_declared_symbol():
     for name in names:
         assert hasattr(lib, name), name
         assert name in _lib.SIGNATURES, name
-    assert lib.cct_abi_version() == 1
+    assert lib.cct_abi_version() == _lib.ABI_VERSION
 
 
 def test_validation_errors_map_to_value_error():

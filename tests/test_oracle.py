@@ -9,29 +9,39 @@ from oracle import port
 from oracle import skimage_restated as skr
 
 
-@pytest.mark.parametrize("case", ["n32_a16", "n33_a9", "n16_a7_d2", "n64_a48"])
+ALL_CASES = ["n32_a16", "n33_a9", "n16_a7_d2", "n64_a48", "n32_a16_psf", "n24_a10_d2_psf"]
+
+
+def _psf(g):
+    return g["psf"] if g["psf"].size else None
+
+
+@pytest.mark.parametrize("case", ALL_CASES)
 def test_port_matches_reference_golden(golden_cases, case):
     g = golden_cases[case]
     rad32, deg32 = port.backend_angles(g["angles"])
     maps = port.compute_maps(g["mu_in"], g["mu_out"], rad32, g["det_angles"])
     assert rel_l2(maps, g["maps"]) < 1e-14
-    fa = port.fp_xrf(g["x"], g["maps"], deg32, g["det_weights"], g["weights_angles"])
+    fa = port.fp_xrf(g["x"], g["maps"], deg32, g["det_weights"], g["weights_angles"], psf=_psf(g))
     assert rel_l2(fa, g["fp_att"]) < 1e-14
     assert rel_l2(port.bp_xrf(g["y"], g["maps"], deg32), g["bp_att"]) < 1e-14
     bs = port.bp_xrf(g["y"], g["maps"], deg32, g["det_weights"], g["weights_angles"], is_symmetric=True)
     assert rel_l2(bs, g["bp_sym"]) < 1e-14
-    assert rel_l2(port.fp_uncorrected(g["x"], deg32), g["fp_unc"]) < 1e-14
+    fu = port.fp_uncorrected(g["x"], deg32)
+    if _psf(g) is not None:
+        fu = np.stack([port.psf_convolve(line, _psf(g)) for line in fu])
+    assert rel_l2(fu, g["fp_unc"]) < 1e-14
     n = int(g["n"])
     y0 = np.reshape(g["y"], (-1, len(deg32), n))[0]
     assert rel_l2(port.bp_uncorrected(y0, deg32, n), g["bp_unc"]) < 1e-14
 
 
-@pytest.mark.parametrize("case", ["n32_a16", "n64_a48"])
+@pytest.mark.parametrize("case", ["n32_a16", "n64_a48", "n32_a16_psf"])
 def test_port_solvers_match_reference_golden(golden_cases, case):
     g = golden_cases[case]
     n = int(g["n"])
     _, deg32 = port.backend_angles(g["angles"])
-    fp = lambda v: port.fp_xrf(v, g["maps"], deg32)  # noqa: E731
+    fp = lambda v: port.fp_xrf(v, g["maps"], deg32, psf=_psf(g))  # noqa: E731
     bp = lambda s: port.bp_xrf(s, g["maps"], deg32)  # noqa: E731
     xm, res = port.mlem(fp, bp, g["b"], 10, tolerance=0.0)
     assert rel_l2(xm, g["mlem_x"]) < 1e-13
@@ -122,3 +132,27 @@ def test_exact_adjoint_oracle_is_adjoint():
     lhs = np.vdot(port.fp_xrf(x, maps, deg32), y)
     rhs = np.vdot(x, port.fp_xrf_adjoint(y, maps, deg32, n))
     assert abs(lhs - rhs) / abs(lhs) < 1e-12
+
+
+def test_psf_convolution_offsets():
+    line = np.arange(8, dtype=np.float64)
+    # odd kernel: centred, edge padded
+    out = port.psf_convolve(line, np.array([0.0, 1.0, 0.0]))
+    np.testing.assert_allclose(out, line)
+    # out[i] = sum_j x[clamp(i + (L-1)//2 - j)] k[j]: k = [1, 0, 0] reads x[i + 1] (edge clamped)
+    out = port.psf_convolve(line, np.array([1.0, 0.0, 0.0]))
+    np.testing.assert_allclose(out, np.concatenate([line[1:], line[-1:]]))
+    # even length: (L-1)//2 = 1, so k = [0, 1, 0, 0] is the identity
+    np.testing.assert_allclose(port.psf_convolve(line, np.array([0.0, 1.0, 0.0, 0.0])), line)
+
+
+def test_intensities_scale_lines_in_fp_and_bp():
+    rng = np.random.default_rng(4)
+    n, a = 16, 5
+    _, deg32 = port.backend_angles(np.linspace(0, 2 * np.pi, a, endpoint=False))
+    maps = rng.uniform(0.5, 1, size=(a, 1, n, n))
+    x = rng.uniform(size=(n, n))
+    inten = rng.uniform(0.5, 1.5, size=a)
+    np.testing.assert_allclose(port.fp_xrf(x, maps, deg32, intensities=inten), port.fp_xrf(x, maps, deg32) * inten[:, None])
+    y = rng.uniform(size=(a, n))
+    np.testing.assert_allclose(port.bp_xrf(y, maps, deg32, intensities=inten), port.bp_xrf(y * inten[:, None], maps, deg32))
