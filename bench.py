@@ -1,15 +1,20 @@
-"""Benchmark: converged slices/s of attenuated XRF MLEM on 512x512-pixel, 720-angle slices.
+"""Benchmark: converged slices/s of attenuated XRF MLEM on 512x512-pixel, 720-angle slices,
+plain (cold start) vs learned warm start.
 
 One step = the hot path over one batch of synthetic slices already resident in HBM:
 ``compute_maps`` (incident + emitted attenuation maps) followed by MLEM with the reference's
 KL-residual stopping rule, run until every slice reaches the residual that the plain solver
-reaches after 200 iterations (calibrated once, untimed).  ``value`` = slices converged per
-second over the timed steps (max over ranks; weak scaling, each rank owns its own slices).
+reaches after 200 iterations (calibrated once, untimed).  The warm-started step runs the first
+10 MLEM iterations, the encoder-decoder on them (tensor-core kernels) and MLEM from its
+prediction to the same residual.  ``value`` = slices converged per second over the timed steps
+of the warm-started path when trained weights are present (else of the plain path); the plain
+path is timed the same way and reported under ``plain``.  Max over ranks; weak scaling (each
+rank owns its own slices, no collective on the data path).
 
-``e2e`` repeats the step through the public API from pinned host buffers (mu_in, mu_out and the
+``e2e`` repeats the headline step through the public API from pinned host buffers (mu and the
 data copied in, the reconstruction copied out inside the timed region).  ``--impl reference``
-times the reference algorithm's CPU implementation (the oracle port in ``oracle/``) on the host
-cores on a bounded sample of the same workload.
+times the reference algorithm's CPU implementation (the oracle port in ``oracle/``) on the
+host cores on a bounded sample of the same workload.
 """
 
 from __future__ import annotations
@@ -28,6 +33,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "converged slices/s, XRF MLEM 512²x720 to fixed residual: plain vs warm start"
 UNIT = "slices/s"
+WEIGHTS = os.path.join(ROOT, "pycorrectedemissionct_b200", "weights", "warmstart.pt")
 
 
 def parse():
@@ -43,6 +49,7 @@ def parse():
     ap.add_argument("--maps-dtype", default="float32", choices=["float32", "bfloat16"])
     ap.add_argument("--peak", type=float, default=1e5)
     ap.add_argument("--seed", type=int, default=20240)
+    ap.add_argument("--method", default="auto", choices=["auto", "plain", "warm"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-angles", type=int, default=144)
     return ap.parse_args()
@@ -73,9 +80,10 @@ class ClockSampler:
     )
 
     def __init__(self, index: int):
+        out = os.path.join(ROOT, "gpurun_out")
+        self.path = os.path.join(out, f"clocks_rank{index}.csv") if os.path.isdir(out) else f"/tmp/cct_clocks_{os.getpid()}.csv"
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv") if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/cct_clocks_{os.getpid()}.csv"
 
     def start(self):
         try:
@@ -84,7 +92,7 @@ class ClockSampler:
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=self.fh, stderr=subprocess.DEVNULL,
             )
-        except (OSError, FileNotFoundError):
+        except OSError:
             self.proc = None
 
     def stop(self) -> dict | None:
@@ -128,7 +136,7 @@ def cpu_baseline(a, iterations_per_slice: float) -> dict:
     mu = phantoms.disk_attenuation(a.n, rng, 0.01)
     angles = phantoms.angles(a.angles)
     sample = max(1, min(a.cpu_sample_angles, a.angles))
-    rad32, deg32 = port.backend_angles(angles[:: a.angles // sample][:sample])
+    rad32, deg32 = port.backend_angles(angles[:: max(1, a.angles // sample)][:sample])
     t0 = time.perf_counter()
     maps = port.compute_maps(mu, mu, rad32, dtype=np.float32, workers=workers)
     t1 = time.perf_counter()
@@ -146,7 +154,7 @@ def cpu_baseline(a, iterations_per_slice: float) -> dict:
         "sample": (
             f"numpy/float32 oracle port of the reference's scikit-image path on {workers} threads: compute_maps, "
             f"one attenuated fp and one bp over {len(rad32)} of {a.angles} angles of one {a.n}x{a.n} slice "
-            f"({t3 - t0:.1f} s), scaled to {a.angles} angles and {iterations_per_slice:.1f} MLEM iterations per slice"
+            f"({t3 - t0:.1f} s), scaled to {a.angles} angles and {iterations_per_slice:.1f} plain MLEM iterations per slice"
         ),
         "seconds_per_slice": t_slice,
     }
@@ -157,11 +165,9 @@ def run_reference(a):
     if rank != 0:
         return
     iters = float(a.iters)
-    samples = []
-    for _ in range(max(1, a.warmup)):
+    for _ in range(max(0, a.warmup)):
         cpu_baseline(a, iters)
-    for _ in range(max(1, a.steps)):
-        samples.append(cpu_baseline(a, iters))
+    samples = [cpu_baseline(a, iters) for _ in range(max(1, a.steps))]
     v = float(np.median([s["value"] for s in samples]))
     cb = dict(samples[-1])
     cb["value"] = v
@@ -169,7 +175,8 @@ def run_reference(a):
         "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded ellipse phantoms, disk attenuation)",
-        "config": {"workload": workload_name(a), "n": a.n, "angles": a.angles, "mlem_iterations": a.iters},
+        "config": {"workload": workload_name(a), "n": a.n, "angles": a.angles, "mlem_iterations": a.iters,
+                   "solver": "plain MLEM (the reference has no warm start)"},
         "impl": "reference", "cpu_baseline": cb,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -180,32 +187,14 @@ def run_reference(a):
 def run_ours(a):
     import torch
 
-    from pycorrectedemissionct_b200 import core, engine
+    from pycorrectedemissionct_b200 import autotune, core, distributed, engine
+    from pycorrectedemissionct_b200 import train_warmstart as tw
+    from pycorrectedemissionct_b200.warmstart import N_ITERATES, WarmStartNet
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = distributed.env_ranks()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
-
-    def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    distributed.init("nccl", dev)
 
     xs_h, mus_h = make_inputs(a, rank)
     angles = np.linspace(0, 2 * np.pi, a.angles, endpoint=False)
@@ -217,12 +206,10 @@ def run_ours(a):
     x_true = torch.from_numpy(xs_h).to(dev)
     tdt = torch.float32 if a.maps_dtype == "float32" else torch.bfloat16
     maps = torch.empty((S, a.angles, 1, n, n), dtype=tdt, device=dev)
-    # maps workspace: ~16 angles of the whole batch per pass (2 x 2.1 MB per angle and slice)
-    ws = torch.empty(max(core.DEFAULT_MAPS_WORKSPACE, 16 * 2 * (a.n + 2 * ((int(np.ceil(np.sqrt(2) * a.n)) - a.n + 1) // 2)) ** 2 * 4 * S),
-                     dtype=torch.uint8, device=dev)
+    _, P = core.geometry.padded_size(n)
+    # maps workspace: ~16 angles of the whole batch per pass (incident + emitted W of P^2 floats)
+    ws = torch.empty(max(core.DEFAULT_MAPS_WORKSPACE, 16 * 2 * P * P * 4 * S), dtype=torch.uint8, device=dev)
     core.compute_maps(mu_in, mu_out, rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
-    from pycorrectedemissionct_b200 import autotune
-
     variant = autotune.tune(c, x_true, maps)
     clean = c.fp(x_true, maps)
     gen = torch.Generator(device=dev)
@@ -231,23 +218,32 @@ def run_ours(a):
     del clean
 
     # calibration (untimed): the plain solver's residual after `iters` iterations defines the target
-    solver = engine.BatchedSolver(c, maps, b, "mlem", history_len=a.iters + 1)
-    solver.run(a.iters, check_every=a.iters, use_graph=False)
+    calib = engine.BatchedSolver(c, maps, b, "mlem")
+    calib.run(a.iters, check_every=a.iters, use_graph=False)
     torch.cuda.synchronize(dev)
-    tol = solver.residuals.clone()
-    tol_np = tol.cpu().numpy()
-    solver = engine.BatchedSolver(c, maps, b, "mlem", tolerance=tol_np * (1 + 1e-9), history_len=2 * a.iters + 2)
+    tol_np = calib.residuals.cpu().numpy() * (1 + 1e-9)
+    del calib
     max_iters = 2 * a.iters
+    plain = engine.BatchedSolver(c, maps, b, "mlem", tolerance=tol_np)
+    net = None
+    method = a.method
+    if method in ("auto", "warm") and os.path.exists(WEIGHTS):
+        net = WarmStartNet(device=dev)
+        net.load(WEIGHTS)
+        method = "warm"
+    elif method == "warm":
+        raise FileNotFoundError(f"no trained warm-start weights at {WEIGHTS}")
+    else:
+        method = "plain"
+    warm = engine.BatchedSolver(c, maps, b, "mlem", tolerance=tol_np) if net is not None else None
+    first = engine.BatchedSolver(c, maps, b, "mlem") if net is not None else None
 
-    passes = int(getattr(core.compute_maps, "last_passes", 1))
+    passes = -(-a.angles // max(1, ws.numel() // (2 * P * P * 4 * S)))
     fp_ms, bp_ms, launches = [], [], [0]
 
-    def one_step(timed: bool):
-        core.compute_maps(mu_in, mu_out, rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
-        launches[0] += 2 * passes
-        solver.reset()
+    def solve_to_tol(solver, timed: bool, budget: int) -> int:
         its, active = 0, S
-        while its < max_iters and active > 0:
+        while its < budget and active > 0:
             evs = []
             for _ in range(10):
                 e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
@@ -264,79 +260,110 @@ def run_ours(a):
                     bp_ms.append(e[1].elapsed_time(e[2]))
         return its
 
+    def step_plain(timed: bool) -> float:
+        core.compute_maps(mu_in, mu_out, rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
+        launches[0] += 2 * passes
+        plain.reset()
+        solve_to_tol(plain, timed, max_iters)
+        return float(plain.iterations.float().mean().item())
+
+    def step_warm(timed: bool) -> float:
+        core.compute_maps(mu_in, mu_out, rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
+        launches[0] += 2 * passes
+        first.reset()
+        its = tw.first_iterates(first)
+        bpn = tw.normalized_backprojection(c, b, first.tau)
+        scale = tw.slice_means(its[-1])
+        x0 = net.predict(its + [bpn], base=its[-1], slice_scale=scale)
+        launches[0] += 3 * N_ITERATES + 2 + 90  # 10 iterations, bp + ratio, network (~90 kernels)
+        warm.reset(x0)
+        solve_to_tol(warm, False, max_iters)
+        return float((warm.iterations.float() + N_ITERATES).mean().item())
+
+    def timed_steps(fn, k: int) -> tuple[float, float]:
+        distributed.barrier(dev)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        its = [fn(True) for _ in range(k)]
+        t1.record()
+        distributed.barrier(dev)
+        return t0.elapsed_time(t1) / 1e3, float(np.mean(its))
+
+    headline = step_warm if method == "warm" else step_plain
     for _ in range(a.warmup):
-        one_step(False)
-    barrier()
-    fp_ms.clear(); bp_ms.clear(); launches[0] = 0
+        headline(False)
+        if method == "warm":
+            step_plain(False)
+    # plain path (always timed; also feeds the fp/bp kernel timings)
+    fp_ms.clear(); bp_ms.clear()
+    plain_s, plain_its = timed_steps(step_plain, a.steps)
+    plain_s = distributed.max_over_ranks(plain_s, dev)
+    fp_keep, bp_keep = list(fp_ms), list(bp_ms)
+    # headline path
     clocks = ClockSampler(local)
     clocks.start()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    barrier()
-    t0.record()
-    its_total = 0
-    for _ in range(a.steps):
-        its_total += one_step(True)
-    t1.record()
-    barrier()
+    launches[0] = 0
+    if method == "warm":
+        head_s, head_its = timed_steps(step_warm, a.steps)
+        head_s = distributed.max_over_ranks(head_s, dev)
+        converged = int((warm.residuals.cpu().numpy() <= tol_np).sum())
+    else:
+        head_s, head_its = plain_s, plain_its
+        converged = int((plain.residuals.cpu().numpy() <= tol_np).sum())
     clk = clocks.stop()
-    elapsed_s = t0.elapsed_time(t1) / 1e3
-    iterations = solver.iterations.cpu().numpy()
-    converged = int((solver.residuals.cpu().numpy() <= tol_np * (1 + 1e-9)).sum())
-    elapsed_max = max_over_ranks(elapsed_s)
+    head_launches = launches[0] // max(1, a.steps) * a.steps
     total_slices = S * a.steps * world
-    value = total_slices / elapsed_max
+    value = total_slices / head_s
 
-    # ---- e2e: the same step from pinned host buffers, copies inside the timed region
+    # ---- e2e: the headline step from pinned host buffers, copies inside the timed region
     mu_h = torch.from_numpy(mus_h).pin_memory()
     b_h = b.cpu().pin_memory()
     x_h = torch.empty((S, n, n), dtype=torch.float32).pin_memory()
-    def e2e_step():
+    result = warm if method == "warm" else plain
+
+    def e2e_step(_timed):
         mu_in.copy_(mu_h, non_blocking=True)
         mu_out.copy_(mu_h, non_blocking=True)
-        solver.b.copy_(b_h, non_blocking=True)
-        one_step(False)
-        x_h.copy_(solver.x, non_blocking=True)
-    e2e_step()
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(a.steps):
-        e2e_step()
-    e1.record()
-    barrier()
-    e2e_s = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        b.copy_(b_h, non_blocking=True)
+        its = headline(False)
+        x_h.copy_(result.x, non_blocking=True)
+        return its
+
+    e2e_step(False)
+    e2e_s, _ = timed_steps(e2e_step, a.steps)
+    e2e_s = distributed.max_over_ranks(e2e_s, dev)
     h2d = S * (2 * n * n + a.angles * n) * 4
     d2h = S * n * n * 4
 
     # ---- roofline of the dominant kernel (attenuated fp with the fused MLEM epilogue)
-    import json as _json
-
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
-        peak = float(_json.load(open(peaks_path))["hbm_gbs"])
+        peak = float(json.load(open(peaks_path))["hbm_gbs"])
         peak_src = "measured"
     else:
         peak = 6650.0
         peak_src = "fallback"
     map_bytes = 4 if a.maps_dtype == "float32" else 2
     fp_bytes = S * (a.angles * n * n * map_bytes + n * n * 4 + 2 * a.angles * n * 4)
-    fp_avg_s = float(np.mean(fp_ms)) / 1e3 if fp_ms else float("nan")
-    bp_avg_s = float(np.mean(bp_ms)) / 1e3 if bp_ms else float("nan")
+    fp_avg_s = float(np.mean(fp_keep)) / 1e3 if fp_keep else float("nan")
+    bp_avg_s = float(np.mean(bp_keep)) / 1e3 if bp_keep else float("nan")
     achieved = fp_bytes / fp_avg_s / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": elapsed_max / a.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": head_s / a.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded ellipse phantoms, disk attenuation, Poisson 1e5 peak counts)",
         "config": {
             "workload": workload_name(a), "n": n, "angles": a.angles, "slices_per_gpu": S, "maps_dtype": a.maps_dtype,
-            "target": f"KL residual of plain MLEM after {a.iters} iterations (per slice)", "solver": "plain MLEM (cold start)",
+            "target": f"KL residual of plain MLEM after {a.iters} iterations (per slice)",
+            "solver": "MLEM warm-started by the learned encoder-decoder" if method == "warm" else "plain MLEM (cold start)",
             "parallelism": f"slices sharded over {world} GPU(s), no collective on the data path",
             "l2": "inputs larger than L2 (maps %.0f MB per slice)" % (a.angles * n * n * map_bytes / 1e6),
-            "mean_iterations": float(np.mean(iterations)), "converged_slices_last_step": converged,
+            "mean_iterations": head_its, "converged_slices_last_step": converged,
             "fp_variant": "tma" if variant else "ldg",
         },
+        "plain": {"value": total_slices / plain_s, "unit": UNIT, "mean_iterations": plain_its,
+                  "ms_per_step": plain_s / a.steps * 1e3},
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             # DRAM bytes per launch from one ncu capture of this kernel on 2 slices (1.4366 GB), scaled
@@ -347,16 +374,14 @@ def run_ours(a):
             "algorithmic_bytes_per_launch": fp_bytes,
         },
         "e2e": {"value": total_slices / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches[0],
+        "gpu_launches": head_launches,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(a, float(np.mean(iterations)))
+        line["cpu_baseline"] = cpu_baseline(a, plain_its)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    distributed.finalize()
 
 
 def main():

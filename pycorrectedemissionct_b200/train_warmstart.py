@@ -154,11 +154,15 @@ def main():
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--target-iterations", type=int, default=500)
+    ap.add_argument("--additive", action="store_true", help="additive instead of log-ratio (multiplicative) targets")
+    ap.add_argument("--log-floor", type=float, default=1e-3, help="floor of the log-ratio target, in slice means")
     ap.add_argument("--out", default="warmstart.pt")
     a = ap.parse_args()
     dev = core.require_cuda()
     t0 = time.time()
     net = WarmStartNet(seed=0, device=dev)
+    net.multiplicative = not a.additive
+    net.log_floor = a.log_floor
     inputs, targets = generate_pairs(a.slices, a.n, a.angles, target_iterations=a.target_iterations, device=dev, net=net)
     torch.cuda.synchronize()
     t1 = time.time()
