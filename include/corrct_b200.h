@@ -279,6 +279,37 @@ int cct_net_ratio(const float* a, const float* b, float* out, int64_t count, int
    *value = the flag; clear != 0 resets it.  Synchronous. */
 int cct_net_timeout(int32_t clear, int32_t* value);
 
+/* ---------------------------------------------------------------------------------------------
+ * Synthetic data: the noise model of corrct's testing.add_noise (corrct: src/corrct/testing.py:
+ * 266-320) on device arrays.  Random numbers are counter based (Philox-4x32-10 keyed by `seed`):
+ * every element's draws depend only on the seed and the element index, so results are
+ * reproducible for any launch, and agree with the reference in distribution (numpy's generator
+ * is a different stream).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct cct_noise_desc {
+  double num_photons;          /* photons for an image value of 1.0 */
+  double detection_efficiency; /* scales the photons (the reference passes the detector solid angle) */
+  double background_avg;       /* used when has_background: noisy += photons * eff * |N(avg, std)| */
+  double background_std;
+  double readout_std;          /* used when has_readout: noisy += N(0, readout_std) after the counts */
+  uint64_t seed;
+  int32_t add_poisson;         /* noisy = Poisson(noisy) (after the background) */
+  int32_t has_background;
+  int32_t has_readout;
+  int32_t reserved;
+} cct_noise_desc;
+
+/* Doubles the `partials` workspace of cct_add_noise must hold. */
+int cct_noise_partials_count(int64_t* count);
+
+/* clean_scaled[i] = (float)(photons * eff) * clean[i] (may be NULL), noisy as described above,
+   *background = mean(noisy - clean_scaled) before the Poisson draw (FP64, device).  flags: two
+   int32 that the caller zeroes; flags[0] != 0 when a Poisson mean was negative, NaN or too large
+   (those elements become NaN; numpy raises ValueError), flags[1] != 0 when a draw hit its
+   iteration bound (returns the rounded mean; not reachable in practice). */
+int cct_add_noise(const cct_noise_desc* desc, const float* clean, int64_t count, float* noisy, float* clean_scaled,
+                  double* partials, double* background, int32_t* flags, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

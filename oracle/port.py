@@ -460,3 +460,35 @@ def pdhg_kl_tv(fp, bp, b: NDArray, iterations: int, x_shape, lam: float, relaxat
         x_relax = x_new + (x_new - x)
         x = x_new
     return x
+
+
+# --------------------------------------------------------------------------------------
+# Synthetic data
+# --------------------------------------------------------------------------------------
+def add_noise(
+    img_clean: NDArray,
+    num_photons: float,
+    add_poisson: bool = False,
+    readout_noise_std: float | None = None,
+    background_avg: float | None = None,
+    background_std: float | None = None,
+    detection_efficiency: float = 1.0,
+    dtype=np.float32,
+) -> tuple[NDArray, NDArray, float]:
+    """Noise model of ``testing.add_noise`` (``testing.py:266-320``) on numpy's global generator.
+
+    Draw order and arithmetic follow the reference (a float32 image scaled by a Python float,
+    float64 background and read-out terms added in place, the background mean taken before the
+    Poisson draw), so after ``np.random.seed(s)`` it returns the reference's values.
+    """
+    scaled = num_photons * detection_efficiency * img_clean.copy().astype(dtype)
+    noisy = scaled.copy()
+    if background_avg is not None:
+        std = background_avg * 5e-2 if background_std is None else background_std
+        noisy += num_photons * detection_efficiency * np.abs(np.random.normal(background_avg, std, scaled.shape))
+    background = float(np.mean((noisy - scaled).flatten()))
+    if add_poisson:
+        noisy = np.random.poisson(noisy).astype(dtype)
+    if readout_noise_std is not None:
+        noisy += np.random.normal(0, readout_noise_std, scaled.shape)
+    return noisy, scaled, background

@@ -21,6 +21,6 @@ def __getattr__(name):
     # heavy submodules (torch, the CUDA library) load on first use
     import importlib
 
-    if name in ("projectors", "attenuation", "solvers", "operators", "backend", "core", "engine", "geometry"):
+    if name in ("projectors", "attenuation", "solvers", "operators", "backend", "core", "engine", "geometry", "testing"):
         return importlib.import_module(f".{name}", __name__)
     raise AttributeError(name)

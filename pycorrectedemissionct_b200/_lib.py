@@ -66,6 +66,21 @@ class MapsDesc(ctypes.Structure):
     ]
 
 
+class NoiseDesc(ctypes.Structure):
+    _fields_ = [
+        ("num_photons", ctypes.c_double),
+        ("detection_efficiency", ctypes.c_double),
+        ("background_avg", ctypes.c_double),
+        ("background_std", ctypes.c_double),
+        ("readout_std", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
+        ("add_poisson", ctypes.c_int32),
+        ("has_background", ctypes.c_int32),
+        ("has_readout", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
 class ConvDesc(ctypes.Structure):
     _fields_ = [
         ("batch", ctypes.c_int32),
@@ -189,6 +204,12 @@ SIGNATURES = {
     ),
     "cct_net_ratio": (ctypes.c_int, [c_float_p, c_float_p, c_float_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p]),
     "cct_net_timeout": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+    "cct_noise_partials_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int64)]),
+    "cct_add_noise": (
+        ctypes.c_int,
+        [ctypes.POINTER(NoiseDesc), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
 }
 
 _lib = None

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_NAME = "libcorrct_b200.so"
 LIB_PATH = os.path.join(HERE, LIB_NAME)
 
-SOURCES = ["cct_api.cu", "cct_project.cu", "cct_maps.cu", "cct_solver.cu", "cct_noalloc.cu", "cct_net.cu"]
+SOURCES = ["cct_api.cu", "cct_project.cu", "cct_maps.cu", "cct_solver.cu", "cct_noalloc.cu", "cct_net.cu", "cct_noise.cu"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

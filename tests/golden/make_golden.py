@@ -114,12 +114,37 @@ def make_case(corrct, name, n, n_ang, det_angles, det_weights, rand_ang_w, seed,
     print(f"{name}: maps {maps.shape} fp {fp_att.shape}")
 
 
+NOISE_CASES = [
+    # name, photons, efficiency, poisson, readout std, background avg, background std, seed
+    ("poisson", 1e3, 0.5, True, None, None, None, 101),
+    ("background_poisson_readout", 2e3, 0.25, True, 2.0, 0.01, None, 102),
+    ("background_only", 5e2, 1.0, False, None, 0.02, 0.003, 103),
+]
+
+
+def make_noise_golden(corrct):
+    """testing.add_noise (testing.py:266-320) on a small seeded sinogram after np.random.seed."""
+    rng = np.random.default_rng(7)
+    clean = rng.uniform(0.0, 3.0, size=(12, 20)).astype(np.float32)
+    out = {"clean": clean}
+    for name, photons, eff, poisson, readout, bg_avg, bg_std, seed in NOISE_CASES:
+        np.random.seed(seed)
+        noisy, scaled, background = corrct.testing.add_noise(
+            clean, photons, add_poisson=poisson, readout_noise_std=readout, background_avg=bg_avg,
+            background_std=bg_std, detection_efficiency=eff,
+        )
+        out[f"{name}_noisy"], out[f"{name}_scaled"], out[f"{name}_background"] = noisy, scaled, background
+    np.savez_compressed(os.path.join(HERE, "noise_cases.npz"), **out)
+    print(f"noise: {len(NOISE_CASES)} cases")
+
+
 def main():
     corrct = load_corrct()
     with contextlib.redirect_stdout(io.StringIO()) as log:
         for case in CASES:
             make_case(corrct, *case)
-    print("\n".join(line for line in log.getvalue().splitlines() if ":" in line and "maps" in line))
+        make_noise_golden(corrct)
+    print("\n".join(line for line in log.getvalue().splitlines() if ":" in line and ("maps" in line or "noise" in line)))
 
 
 if __name__ == "__main__":

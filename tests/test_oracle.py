@@ -156,3 +156,30 @@ def test_intensities_scale_lines_in_fp_and_bp():
     np.testing.assert_allclose(port.fp_xrf(x, maps, deg32, intensities=inten), port.fp_xrf(x, maps, deg32) * inten[:, None])
     y = rng.uniform(size=(a, n))
     np.testing.assert_allclose(port.bp_xrf(y, maps, deg32, intensities=inten), port.bp_xrf(y * inten[:, None], maps, deg32))
+
+
+NOISE_CASES = [
+    # name, photons, efficiency, poisson, readout std, background avg, background std, seed
+    ("poisson", 1e3, 0.5, True, None, None, None, 101),
+    ("background_poisson_readout", 2e3, 0.25, True, 2.0, 0.01, None, 102),
+    ("background_only", 5e2, 1.0, False, None, 0.02, 0.003, 103),
+]
+
+
+@pytest.mark.parametrize("case", NOISE_CASES, ids=[c[0] for c in NOISE_CASES])
+def test_port_add_noise_matches_reference_golden(case):
+    """After np.random.seed the port draws exactly what the reference's add_noise drew."""
+    import os
+
+    from conftest import GOLDEN
+
+    g = dict(np.load(os.path.join(GOLDEN, "noise_cases.npz")))
+    name, photons, eff, poisson, readout, bg_avg, bg_std, seed = case
+    np.random.seed(seed)
+    noisy, scaled, background = port.add_noise(
+        g["clean"], photons, add_poisson=poisson, readout_noise_std=readout, background_avg=bg_avg,
+        background_std=bg_std, detection_efficiency=eff,
+    )
+    np.testing.assert_array_equal(scaled, g[f"{name}_scaled"])
+    np.testing.assert_array_equal(noisy, g[f"{name}_noisy"])
+    assert background == float(g[f"{name}_background"])
