@@ -1,15 +1,20 @@
 """Benchmark: converged slices/s of attenuated XRF MLEM on 512x512-pixel, 720-angle slices,
-plain (cold start) vs learned warm start.
+plain (cold start) vs warm start.
 
 One step = the hot path over one batch of synthetic slices already resident in HBM:
 ``compute_maps`` (incident + emitted attenuation maps) followed by MLEM with the reference's
 KL-residual stopping rule, run until every slice reaches the residual that the plain solver
-reaches after 200 iterations (calibrated once, untimed).  The warm-started step runs the first
-10 MLEM iterations, the encoder-decoder on them (tensor-core kernels) and MLEM from its
-prediction to the same residual.  ``value`` = slices converged per second over the timed steps
-of the warm-started path when trained weights are present (else of the plain path); the plain
-path is timed the same way and reported under ``plain``.  Max over ranks; weak scaling (each
-rank owns its own slices, no collective on the data path).
+reaches after 200 iterations (calibrated once, untimed).  Three paths are timed:
+
+* plain: MLEM from the default start;
+* learned: 10 MLEM iterations, the encoder-decoder on them (tensor-core kernels), MLEM to the
+  residual (when trained weights are present);
+* subsets: ordered-subsets EM passes (30 subsets x 10 passes, then 10 x 10; each pass costs one
+  MLEM iteration), then MLEM to the residual, which judges every slice.
+
+``value`` = slices converged per second over the timed steps of the headline path (``--method``,
+default the ordered-subsets warm start); the other paths are reported beside it.  Max over ranks;
+weak scaling (each rank owns its own slices, no collective on the data path).
 
 ``e2e`` repeats the headline step through the public API from pinned host buffers (mu and the
 data copied in, the reconstruction copied out inside the timed region).  ``--impl reference``
@@ -49,7 +54,9 @@ def parse():
     ap.add_argument("--maps-dtype", default="float32", choices=["float32", "bfloat16"])
     ap.add_argument("--peak", type=float, default=1e5)
     ap.add_argument("--seed", type=int, default=20240)
-    ap.add_argument("--method", default="auto", choices=["auto", "plain", "warm"])
+    ap.add_argument("--method", default="auto", choices=["auto", "plain", "learned", "subsets"],
+                    help="headline path (auto: ordered subsets); the others are timed beside it")
+    ap.add_argument("--subsets", default="30:10,10:10", help="ordered-subsets schedule subsets:passes,...")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-angles", type=int, default=144)
     return ap.parse_args()
@@ -198,24 +205,37 @@ def run_ours(a):
 
     xs_h, mus_h = make_inputs(a, rank)
     angles = np.linspace(0, 2 * np.pi, a.angles, endpoint=False)
-    rad32 = np.array(angles, dtype=np.float32)
     S, n = a.slices, a.n
-    c = core.XrfCore(n, angles, device=dev)
+    schedule = parse_schedule(a.subsets)
+    perm = engine.subset_permutation(a.angles, [k for k, _ in schedule])
+    perm_t = torch.from_numpy(perm).to(dev)
+    c = core.XrfCore(n, angles, device=dev)                 # natural angle order (plain, learned)
+    c_os = core.XrfCore(n, angles[perm], device=dev)        # subset-major order (ordered subsets)
     mu_in = torch.from_numpy(mus_h).to(dev)
     mu_out = mu_in.clone()  # mu_out = mu_in for this workload
     x_true = torch.from_numpy(xs_h).to(dev)
     tdt = torch.float32 if a.maps_dtype == "float32" else torch.bfloat16
-    maps = torch.empty((S, a.angles, 1, n, n), dtype=tdt, device=dev)
+    maps = torch.empty((S, a.angles, 1, n, n), dtype=tdt, device=dev)  # recomputed by every step, in its order
     _, P = core.geometry.padded_size(n)
     # maps workspace: ~16 angles of the whole batch per pass (incident + emitted W of P^2 floats)
     ws = torch.empty(max(core.DEFAULT_MAPS_WORKSPACE, 16 * 2 * P * P * 4 * S), dtype=torch.uint8, device=dev)
-    core.compute_maps(mu_in, mu_out, rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
+    passes = -(-a.angles // max(1, ws.numel() // (2 * P * P * 4 * S)))
+
+    def maps_natural():
+        core.compute_maps(mu_in, mu_out, c.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
+
+    def maps_subsets():
+        core.compute_maps(mu_in, mu_out, c_os.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
+
+    maps_natural()
     variant = autotune.tune(c, x_true, maps)
+    c_os.variant = variant
     clean = c.fp(x_true, maps)
     gen = torch.Generator(device=dev)
     gen.manual_seed(a.seed + rank)
     b = torch.poisson(clean / clean.amax(dim=(1, 2, 3), keepdim=True) * a.peak, generator=gen)
     del clean
+    b_os = b[:, :, perm_t].contiguous()
 
     # calibration (untimed): the plain solver's residual after `iters` iterations defines the target
     calib = engine.BatchedSolver(c, maps, b, "mlem")
@@ -224,33 +244,32 @@ def run_ours(a):
     tol_np = calib.residuals.cpu().numpy() * (1 + 1e-9)
     del calib
     max_iters = 2 * a.iters
+
     plain = engine.BatchedSolver(c, maps, b, "mlem", tolerance=tol_np)
     net = None
-    method = a.method
-    if method in ("auto", "warm") and os.path.exists(WEIGHTS):
+    if os.path.exists(WEIGHTS):
         net = WarmStartNet(device=dev)
         net.load(WEIGHTS)
-        method = "warm"
-    elif method == "warm":
+    elif a.method == "learned":
         raise FileNotFoundError(f"no trained warm-start weights at {WEIGHTS}")
-    else:
-        method = "plain"
-    warm = engine.BatchedSolver(c, maps, b, "mlem", tolerance=tol_np) if net is not None else None
+    learned = engine.BatchedSolver(c, maps, b, "mlem", tolerance=tol_np) if net is not None else None
     first = engine.BatchedSolver(c, maps, b, "mlem") if net is not None else None
+    subsets = engine.OrderedSubsets(c_os, maps, b_os, schedule)
+    judge = engine.BatchedSolver(c_os, maps, b_os, "mlem", tolerance=tol_np, x_shared=subsets.x)
+    launches_os_pass = sum(k * 3 * p for k, p in schedule)
 
-    passes = -(-a.angles // max(1, ws.numel() // (2 * P * P * 4 * S)))
     fp_ms, bp_ms, launches = [], [], [0]
 
-    def solve_to_tol(solver, timed: bool, budget: int) -> int:
+    def solve_to_tol(solver, timed: bool, budget: int, block: int = 10) -> int:
         its, active = 0, S
         while its < budget and active > 0:
             evs = []
-            for _ in range(10):
+            for _ in range(block):
                 e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
                 solver.step_timed(*e)
                 evs.append(e)
-            its += 10
-            launches[0] += 30
+            its += block
+            launches[0] += 3 * block
             block_full = active == S
             active = int(solver.active.sum().item())  # synchronises the stream
             if timed and block_full:
@@ -261,14 +280,14 @@ def run_ours(a):
         return its
 
     def step_plain(timed: bool) -> float:
-        core.compute_maps(mu_in, mu_out, rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
+        maps_natural()
         launches[0] += 2 * passes
         plain.reset()
         solve_to_tol(plain, timed, max_iters)
         return float(plain.iterations.float().mean().item())
 
-    def step_warm(timed: bool) -> float:
-        core.compute_maps(mu_in, mu_out, rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
+    def step_learned(timed: bool) -> float:
+        maps_natural()
         launches[0] += 2 * passes
         first.reset()
         its = tw.first_iterates(first)
@@ -276,9 +295,18 @@ def run_ours(a):
         scale = tw.slice_means(its[-1])
         x0 = net.predict(its + [bpn], base=its[-1], slice_scale=scale)
         launches[0] += 3 * N_ITERATES + 2 + 90  # 10 iterations, bp + ratio, network (~90 kernels)
-        warm.reset(x0)
-        solve_to_tol(warm, False, max_iters)
-        return float((warm.iterations.float() + N_ITERATES).mean().item())
+        learned.reset(x0)
+        solve_to_tol(learned, False, max_iters)
+        return float((learned.iterations.float() + N_ITERATES).mean().item())
+
+    def step_subsets(timed: bool) -> float:
+        maps_subsets()
+        launches[0] += 2 * passes + launches_os_pass
+        subsets.reset()
+        subsets.run()
+        judge.reset(subsets.x)
+        solve_to_tol(judge, False, max_iters, block=2)
+        return float((judge.iterations.float() + subsets.passes).mean().item())
 
     def timed_steps(fn, k: int) -> tuple[float, float]:
         distributed.barrier(dev)
@@ -290,43 +318,57 @@ def run_ours(a):
         distributed.barrier(dev)
         return t0.elapsed_time(t1) / 1e3, float(np.mean(its))
 
-    headline = step_warm if method == "warm" else step_plain
+    paths = {"plain": step_plain, "subsets": step_subsets}
+    if net is not None:
+        paths["learned"] = step_learned
+    headline = {"auto": "subsets", "plain": "plain", "learned": "learned", "subsets": "subsets"}[a.method]
+    if headline not in paths:
+        raise RuntimeError(f"path {headline!r} is unavailable")
     for _ in range(a.warmup):
-        headline(False)
-        if method == "warm":
-            step_plain(False)
-    # plain path (always timed; also feeds the fp/bp kernel timings)
-    fp_ms.clear(); bp_ms.clear()
-    plain_s, plain_its = timed_steps(step_plain, a.steps)
-    plain_s = distributed.max_over_ranks(plain_s, dev)
-    fp_keep, bp_keep = list(fp_ms), list(bp_ms)
-    # headline path
+        for fn in paths.values():
+            fn(False)
+
+    results = {}
+    fp_keep, bp_keep = [], []
+    for name, fn in paths.items():
+        if name == headline:
+            continue
+        fp_ms.clear(); bp_ms.clear()
+        secs, its = timed_steps(fn, a.steps)
+        secs = distributed.max_over_ranks(secs, dev)
+        results[name] = {"value": S * a.steps * world / secs, "unit": UNIT, "mean_iterations": its,
+                         "ms_per_step": secs / a.steps * 1e3}
+        if name == "plain":
+            fp_keep, bp_keep = list(fp_ms), list(bp_ms)
+    # the headline path, with the clock sampler running
     clocks = ClockSampler(local)
     clocks.start()
     launches[0] = 0
-    if method == "warm":
-        head_s, head_its = timed_steps(step_warm, a.steps)
-        head_s = distributed.max_over_ranks(head_s, dev)
-        converged = int((warm.residuals.cpu().numpy() <= tol_np).sum())
-    else:
-        head_s, head_its = plain_s, plain_its
-        converged = int((plain.residuals.cpu().numpy() <= tol_np).sum())
+    fp_ms.clear(); bp_ms.clear()
+    head_s, head_its = timed_steps(paths[headline], a.steps)
+    head_s = distributed.max_over_ranks(head_s, dev)
     clk = clocks.stop()
-    head_launches = launches[0] // max(1, a.steps) * a.steps
+    head_launches = launches[0]
+    result = {"plain": plain, "learned": learned, "subsets": judge}[headline]
+    converged = int((result.residuals.cpu().numpy() <= tol_np).sum())
     total_slices = S * a.steps * world
     value = total_slices / head_s
+    if headline == "plain":
+        fp_keep, bp_keep = list(fp_ms), list(bp_ms)
 
     # ---- e2e: the headline step from pinned host buffers, copies inside the timed region
     mu_h = torch.from_numpy(mus_h).pin_memory()
     b_h = b.cpu().pin_memory()
     x_h = torch.empty((S, n, n), dtype=torch.float32).pin_memory()
-    result = warm if method == "warm" else plain
 
     def e2e_step(_timed):
         mu_in.copy_(mu_h, non_blocking=True)
         mu_out.copy_(mu_h, non_blocking=True)
         b.copy_(b_h, non_blocking=True)
-        its = headline(False)
+        if headline == "subsets":
+            torch.index_select(b, 2, perm_t, out=b_os)
+            subsets.set_data(b_os)
+        its = paths[headline](False)
         x_h.copy_(result.x, non_blocking=True)
         return its
 
@@ -336,7 +378,7 @@ def run_ours(a):
     h2d = S * (2 * n * n + a.angles * n) * 4
     d2h = S * n * n * 4
 
-    # ---- roofline of the dominant kernel (attenuated fp with the fused MLEM epilogue)
+    # ---- roofline of the dominant kernel (attenuated fp with the fused MLEM epilogue, plain path)
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         peak = float(json.load(open(peaks_path))["hbm_gbs"])
@@ -349,6 +391,11 @@ def run_ours(a):
     fp_avg_s = float(np.mean(fp_keep)) / 1e3 if fp_keep else float("nan")
     bp_avg_s = float(np.mean(bp_keep)) / 1e3 if bp_keep else float("nan")
     achieved = fp_bytes / fp_avg_s / 1e9
+    solver_desc = {
+        "plain": "plain MLEM (cold start)",
+        "learned": "MLEM warm-started by the learned encoder-decoder (10 MLEM iterations, network, MLEM to the residual)",
+        "subsets": f"MLEM warm-started by ordered-subsets EM passes {schedule} (subsets, passes), then MLEM to the residual",
+    }
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": head_s / a.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -356,14 +403,12 @@ def run_ours(a):
         "config": {
             "workload": workload_name(a), "n": n, "angles": a.angles, "slices_per_gpu": S, "maps_dtype": a.maps_dtype,
             "target": f"KL residual of plain MLEM after {a.iters} iterations (per slice)",
-            "solver": "MLEM warm-started by the learned encoder-decoder" if method == "warm" else "plain MLEM (cold start)",
+            "solver": solver_desc[headline],
             "parallelism": f"slices sharded over {world} GPU(s), no collective on the data path",
             "l2": "inputs larger than L2 (maps %.0f MB per slice)" % (a.angles * n * n * map_bytes / 1e6),
             "mean_iterations": head_its, "converged_slices_last_step": converged,
             "fp_variant": "tma" if variant else "ldg",
         },
-        "plain": {"value": total_slices / plain_s, "unit": UNIT, "mean_iterations": plain_its,
-                  "ms_per_step": plain_s / a.steps * 1e3},
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             # DRAM bytes per launch from one ncu capture of this kernel on 2 slices (1.4366 GB), scaled
@@ -377,11 +422,23 @@ def run_ours(a):
         "gpu_launches": head_launches,
         "clocks": clk,
     }
+    for name, r in results.items():
+        line[name] = dict(r, solver=solver_desc[name])
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        plain_its = results.get("plain", {}).get("mean_iterations", float(a.iters))
         line["cpu_baseline"] = cpu_baseline(a, plain_its)
     if rank == 0:
         print(json.dumps(line), flush=True)
     distributed.finalize()
+
+
+def parse_schedule(text: str) -> list[tuple[int, int]]:
+    """'30:10,10:10' -> [(30, 10), (10, 10)] (subsets, passes)."""
+    out = []
+    for part in text.split(","):
+        k, p = part.split(":")
+        out.append((int(k), int(p)))
+    return out
 
 
 def main():

@@ -52,7 +52,9 @@ constexpr int FP_RPT = FP_TR / FP_LR;              // 16 samples per thread per 
 constexpr int FP_BOX_W = 100;
 constexpr int FP_BOX_H = 96;
 constexpr int FP_STRIDE = FP_BOX_W;                // 16-byte rows: conflict-free float4 fills
-constexpr int FP_FILL_BATCH = 4;                   // float4 items whose loads are issued together
+constexpr int FP_MAX_CHUNKS = (8192 + FP_TR - 1) / FP_TR;  // row chunks of the largest n
+static_assert(FP_MAX_CHUNKS <= FP_THREADS, "one thread per chunk box");
+constexpr int FP_FILL_BATCH = 3;                   // float4 items whose loads are issued together
 
 template <bool HAS_MAPS, int MAPS_DTYPE>
 __device__ __forceinline__ float4 fp_load_item(const float* vol, const void* maps, int64_t map_off, int n, int gy,
@@ -90,10 +92,28 @@ __device__ __forceinline__ float4 fp_load_item(const float* vol, const void* map
   return make_float4(e[0], e[1], e[2], e[3]);
 }
 
+// Bounding box of the sample positions of columns [c0, c_last] x rows [r0, r_last] (the corners
+// of a rotated rectangle), widened by the bilinear taps; x origin floored to a multiple of 4.
+__device__ __forceinline__ void chunk_box(float m00, float m01, float m02, float m10, float m11, float m12, int c0,
+                                          int c_last, int r0, int r_last, int& bx0, int& bx1, int& by0, int& by1) {
+  const float fc0 = (float)c0, fc1 = (float)c_last, fr0 = (float)r0, fr1 = (float)r_last;
+  const float xa = sample_x(m00, m01, m02, fc0, fr0), xb = sample_x(m00, m01, m02, fc1, fr0);
+  const float xc = sample_x(m00, m01, m02, fc0, fr1), xd = sample_x(m00, m01, m02, fc1, fr1);
+  const float ya = sample_x(m10, m11, m12, fc0, fr0), yb = sample_x(m10, m11, m12, fc1, fr0);
+  const float yc = sample_x(m10, m11, m12, fc0, fr1), yd = sample_x(m10, m11, m12, fc1, fr1);
+  const float xmin = fminf(fminf(xa, xb), fminf(xc, xd)), xmax = fmaxf(fmaxf(xa, xb), fmaxf(xc, xd));
+  const float ymin = fminf(fminf(ya, yb), fminf(yc, yd)), ymax = fmaxf(fmaxf(ya, yb), fmaxf(yc, yd));
+  bx0 = ((int)floorf(xmin) - 1) & ~3;  // floor to a multiple of 4 (two's complement)
+  bx1 = (int)floorf(xmax) + 2;
+  by0 = (int)floorf(ymin) - 1;
+  by1 = (int)floorf(ymax) + 2;
+}
+
 template <int EPI, bool HAS_MAPS, int MAPS_DTYPE>
-__global__ void __launch_bounds__(FP_THREADS) fp_kernel(FpArgs args) {
+__global__ void __launch_bounds__(FP_THREADS, 5) fp_kernel(FpArgs args) {
   __shared__ __align__(16) float z[FP_BOX_H * FP_STRIDE];
   __shared__ double red_d[FP_TC / FP_LC];
+  __shared__ int4 box_sh[FP_MAX_CHUNKS];  // every chunk's box, computed once per CTA
 
   const int n = args.n;
   const int band = blockIdx.x;
@@ -122,21 +142,20 @@ __global__ void __launch_bounds__(FP_THREADS) fp_kernel(FpArgs args) {
   const float pxc = fmaf(m00, fc, m02);
   const float pyc = fmaf(m10, fc, m12);
 
+  // thread t computes the box of row chunk t (n <= 8192: at most FP_MAX_CHUNKS chunks)
+  if (tid * FP_TR < n) {
+    int4 b;
+    chunk_box(m00, m01, m02, m10, m11, m12, c0, c_last, tid * FP_TR, min((tid + 1) * FP_TR, n) - 1, b.x, b.y, b.z,
+              b.w);
+    box_sh[tid] = b;
+  }
+  __syncthreads();
+
   float acc = 0.f;
   for (int r0 = 0; r0 < n; r0 += FP_TR) {
     const int r_last = min(r0 + FP_TR, n) - 1;
-    // Bounding box of the chunk's sample positions (corners of the rotated rectangle).
-    const float fc0 = (float)c0, fc1 = (float)c_last, fr0 = (float)r0, fr1 = (float)r_last;
-    const float xa = sample_x(m00, m01, m02, fc0, fr0), xb = sample_x(m00, m01, m02, fc1, fr0);
-    const float xc = sample_x(m00, m01, m02, fc0, fr1), xd = sample_x(m00, m01, m02, fc1, fr1);
-    const float ya = sample_x(m10, m11, m12, fc0, fr0), yb = sample_x(m10, m11, m12, fc1, fr0);
-    const float yc = sample_x(m10, m11, m12, fc0, fr1), yd = sample_x(m10, m11, m12, fc1, fr1);
-    const float xmin = fminf(fminf(xa, xb), fminf(xc, xd)), xmax = fmaxf(fmaxf(xa, xb), fmaxf(xc, xd));
-    const float ymin = fminf(fminf(ya, yb), fminf(yc, yd)), ymax = fmaxf(fmaxf(ya, yb), fmaxf(yc, yd));
-    const int bx0 = ((int)floorf(xmin) - 1) & ~3;  // floor to a multiple of 4 (two's complement)
-    const int bx1 = (int)floorf(xmax) + 2;
-    const int by0 = (int)floorf(ymin) - 1;
-    const int by1 = (int)floorf(ymax) + 2;
+    const int4 box = box_sh[r0 / FP_TR];
+    const int bx0 = box.x, bx1 = box.y, by0 = box.z, by1 = box.w;
     const int q4 = (bx1 - bx0) / 4 + 1;  // float4 columns
     const int bh = by1 - by0 + 1;
     if (4 * q4 > FP_BOX_W || bh > FP_BOX_H) {  // cannot happen for valid matrices; never trap
@@ -147,9 +166,9 @@ __global__ void __launch_bounds__(FP_THREADS) fp_kernel(FpArgs args) {
     // Stage z = vol * map over the box (zeros outside the image); every thread takes items
     // tid, tid + 256, ... of the q4 x bh grid, issuing FP_FILL_BATCH items' loads at once.
     const int items = q4 * bh;
-    // it / q4 as a multiply-high: with it < 2^12 and q4 <= 25 the rounding error of
-    // ceil(2^32 / q4) stays below 2^-15 and never reaches the next integer
-    const unsigned magic = (unsigned)((0x100000000ull + (unsigned)q4 - 1) / (unsigned)q4);
+    // it / q4 = (it * ceil(2^20 / q4)) >> 20, exact for it < 2^12 and q4 <= 25 (the error
+    // it * (magic - 2^20 / q4) / 2^20 < 2^-8 stays below 1 / q4), and the product fits 32 bits
+    const unsigned magic = (1048576u + (unsigned)q4 - 1u) / (unsigned)q4;
     for (int base = tid; base < items; base += FP_THREADS * FP_FILL_BATCH) {
       float4 v[FP_FILL_BATCH];
       int dst[FP_FILL_BATCH];
@@ -159,7 +178,7 @@ __global__ void __launch_bounds__(FP_THREADS) fp_kernel(FpArgs args) {
         dst[k] = -1;
         v[k] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (it < items) {
-          const int rr = (int)__umulhi((unsigned)it, magic);
+          const int rr = (int)(((unsigned)it * magic) >> 20);
           const int qq = it - rr * q4;
           const int gy = by0 + rr, gx = bx0 + 4 * qq;
           dst[k] = rr * FP_STRIDE + 4 * qq;

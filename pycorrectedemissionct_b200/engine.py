@@ -19,7 +19,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .core import XrfCore, stream_handle
+from .core import XrfCore, _maps_stride, stream_handle
 
 _BP_MODE_CODES = {"reference": _lib.CCT_BP_REFERENCE, "symmetric": _lib.CCT_BP_SYMMETRIC}
 
@@ -39,6 +39,8 @@ class BatchedSolver:
     tolerance : (S,) array, float, or None
         Stop a slice when ``tolerance > residual`` (the reference's rule).
     x_mask : (n, n) or (S, n, n) tensor or None
+    x_shared : (S, n, n) tensor or None
+        MLEM only: use this tensor as the iterate, in place and without initialising it.
     joint_stop : bool
         The S slices are one 3-D volume: a single stopping test on the residual summed over the
         slices (the reference's norm over the whole volume, compared with ``tolerance[0]``); the
@@ -62,6 +64,7 @@ class BatchedSolver:
         background: float | None = None,
         history_len: int = 0,
         joint_stop: bool = False,
+        x_shared: torch.Tensor | None = None,
     ):
         self.core = core
         self.device = core.device
@@ -91,9 +94,15 @@ class BatchedSolver:
             self.tau = core.bp(ones, "reference")[0].contiguous()
             self.tau_shared = 1
             self.sigma = None
-            self.x = torch.ones((s, n, n), **f32) if x0 is None else x0.to(**f32).clone().contiguous()
-            if x_mask is not None:
-                self.x *= x_mask
+            if x_shared is not None:
+                # iterate owned by the caller (ordered subsets share one x between subset solvers)
+                if tuple(x_shared.shape) != (s, n, n) or x_shared.dtype != torch.float32 or not x_shared.is_contiguous():
+                    raise ValueError(f"x_shared must be a contiguous float32 tensor of shape {(s, n, n)}")
+                self.x = x_shared
+            else:
+                self.x = torch.ones((s, n, n), **f32) if x0 is None else x0.to(**f32).clone().contiguous()
+                if x_mask is not None:
+                    self.x *= x_mask
         else:
             relax = relaxation if relaxation is not None else (1.95 if self.method == "sirt" else 0.95)
             reg_tau = 4.0 if self.method == "pdhg" else 0.0
@@ -166,6 +175,7 @@ class BatchedSolver:
         self.joint_stop = bool(joint_stop)
         self.state = st
         self.desc = core.desc(s, self.maps_dtype)
+        self.desc.maps_slice_stride = _maps_stride(maps)
         self._maps_ptr = None if maps is None else maps.data_ptr()
         self._graph: torch.cuda.CUDAGraph | None = None
         self._graph_steps = 0
@@ -258,3 +268,112 @@ class BatchedSolver:
             iterations=self.iterations,
             active=self.active,
         )
+
+
+# ------------------------------------------------------------------------------ ordered subsets
+def subset_permutation(n_angles: int, levels: list[int]) -> np.ndarray:
+    """Angle order in which every subset of every level is one contiguous range.
+
+    ``levels`` are subset counts, each dividing the one before and all dividing ``n_angles``;
+    a subset of k holds the angles a with a mod k equal to its index (every k-th angle).
+    Angles are grouped by residue modulo the finest count, and those groups by residue modulo
+    each coarser count, so the subsets of a coarser level are unions of consecutive finer ones.
+    """
+    levels = [int(k) for k in levels]
+    if not levels or any(k < 1 or n_angles % k for k in levels):
+        raise ValueError(f"every subset count must divide the {n_angles} angles: {levels}")
+    if any(levels[i] % levels[i + 1] for i in range(len(levels) - 1)):
+        raise ValueError(f"each subset count must divide the previous one: {levels}")
+    finest = levels[0]
+    residues = sorted(range(finest), key=lambda r: tuple(r % k for k in reversed(levels)))
+    return np.concatenate([np.arange(r, n_angles, finest) for r in residues])
+
+
+class OrderedSubsets:
+    """Ordered-subsets EM passes (H. M. Hudson and R. S. Larkin, "Accelerated image reconstruction
+    using ordered subsets of projection data", IEEE TMI 13, 1994) as a warm start for MLEM.
+
+    A pass visits the k subsets of a level in turn and applies the MLEM update of each subset,
+    x *= A_m^T(b_m / A_m x) / A_m^T 1, with the fused MLEM kernels restricted to the subset's
+    angles; one pass costs about one full MLEM iteration.  ``core``, ``maps`` and ``b`` must be in
+    the angle order of ``subset_permutation(A, [k for k, _ in schedule])``.
+
+    schedule : [(subsets, passes), ...], subset counts decreasing, each dividing the previous.
+    """
+
+    def __init__(self, core: XrfCore, maps: torch.Tensor | None, b: torch.Tensor, schedule, x0=None):
+        self.core = core
+        self.device = core.device
+        self.schedule = [(int(k), int(p)) for k, p in schedule]
+        subset_permutation(core.n_angles, [k for k, _ in self.schedule])  # validates the levels
+        s, n = b.shape[0], core.n
+        self.x = torch.ones((s, n, n), dtype=torch.float32, device=self.device)
+        if x0 is not None:
+            self.x.copy_(x0)
+        self.levels: list[list[BatchedSolver]] = []
+        a_all = core.angles_rad32.astype(np.float64)
+        for k, _ in self.schedule:
+            per = core.n_angles // k
+            solvers = []
+            for m in range(k):
+                rng = slice(m * per, (m + 1) * per)
+                sub = XrfCore(n, a_all[rng], n_det=core.n_det, device=self.device, variant=core.variant)
+                if core._base_weights is not None:
+                    sub.set_weights(core._base_weights[rng])
+                if core.intensities_np is not None:
+                    sub.set_intensities(core.intensities_np[rng])
+                if core.psf is not None:
+                    sub.set_psf(core.psf.cpu().numpy())
+                sub_maps = None if maps is None else maps[:, rng]
+                b_sub = b[:, :, rng].contiguous()
+                solvers.append(BatchedSolver(sub, sub_maps, b_sub, "mlem", x_shared=self.x))
+            self.levels.append(solvers)
+        self._graphs: list[torch.cuda.CUDAGraph | None] = [None] * len(self.levels)
+
+    def reset(self, x0: torch.Tensor | None = None) -> None:
+        if x0 is None:
+            self.x.fill_(1.0)
+        else:
+            self.x.copy_(x0)
+        for solvers in self.levels:
+            for sm in solvers:
+                sm.active.fill_(1)
+                sm.iterations.zero_()
+
+    def set_data(self, b: torch.Tensor) -> None:
+        """Refresh every subset's copy of the data from ``b`` (subset-major angle order)."""
+        for level in self.levels:
+            per = self.core.n_angles // len(level)
+            for m, sm in enumerate(level):
+                sm.b.copy_(b[:, :, m * per : (m + 1) * per])
+
+    def _pass(self, level: int) -> None:
+        for sm in self.levels[level]:
+            sm.step()
+
+    def run(self, use_graph: bool = True) -> torch.Tensor:
+        """All passes of the schedule; returns the shared iterate."""
+        for li, (_, passes) in enumerate(self.schedule):
+            if passes <= 0:
+                continue
+            if not use_graph:
+                for _ in range(passes):
+                    self._pass(li)
+                continue
+            if self._graphs[li] is None:
+                self._pass(li)  # eager first pass: every kernel is loaded before capture
+                torch.cuda.synchronize(self.device)
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g):
+                    self._pass(li)
+                self._graphs[li] = g
+                todo = passes - 1
+            else:
+                todo = passes
+            for _ in range(todo):
+                self._graphs[li].replay()
+        return self.x
+
+    @property
+    def passes(self) -> int:
+        return sum(p for _, p in self.schedule)

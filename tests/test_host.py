@@ -116,3 +116,21 @@ def test_compute_paths_need_cuda():
 
     with pytest.raises(RuntimeError, match="CUDA"):
         projectors.ProjectorUncorrected((16, 16), np.linspace(0, np.pi, 4))
+
+
+def test_subset_permutation_nests_levels():
+    from pycorrectedemissionct_b200.engine import subset_permutation
+
+    for n_ang, levels in ((720, [30, 10]), (720, [24, 8, 2]), (360, [12, 4, 1]), (90, [9, 3])):
+        p = subset_permutation(n_ang, levels)
+        assert sorted(p.tolist()) == list(range(n_ang))
+        for k in levels:
+            per = n_ang // k
+            for m in range(k):
+                block = p[m * per : (m + 1) * per]
+                assert len(set((block % k).tolist())) == 1  # one residue class: every k-th angle
+                assert np.all(np.diff(np.sort(block)) == k)
+    with pytest.raises(ValueError):
+        subset_permutation(720, [7])
+    with pytest.raises(ValueError):
+        subset_permutation(720, [10, 4])
