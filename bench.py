@@ -9,7 +9,7 @@ reaches after 200 iterations (calibrated once, untimed).  Three paths are timed:
 * plain: MLEM from the default start;
 * learned: 10 MLEM iterations, the encoder-decoder on them (tensor-core kernels), MLEM to the
   residual (when trained weights are present);
-* subsets: ordered-subsets EM passes (30 subsets x 10 passes, then 10 x 10; each pass costs one
+* subsets: ordered-subsets EM passes (60 subsets x 3 passes, then 30 x 2; each pass costs one
   MLEM iteration), then MLEM to the residual, which judges every slice.
 
 ``value`` = slices converged per second over the timed steps of the headline path (``--method``,
@@ -56,8 +56,13 @@ def parse():
     ap.add_argument("--seed", type=int, default=20240)
     ap.add_argument("--method", default="auto", choices=["auto", "plain", "learned", "subsets"],
                     help="headline path (auto: ordered subsets); the others are timed beside it")
-    ap.add_argument("--subsets", default="30:10,10:10", help="ordered-subsets schedule subsets:passes,...")
+    ap.add_argument("--subsets", default="60:3,30:2", help="ordered-subsets schedule subsets:passes,...")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fp-variant", default="auto", choices=["auto", "ldg", "tma"],
+                    help="fp staging variant: the autotuner's choice (auto) or a fixed one")
+    ap.add_argument("--workload", default="batch", choices=["batch", "ragged"],
+                    help="batch: the 512x720 benchmark (default); ragged: the mixed-size stream")
+    ap.add_argument("--ragged-slices", type=int, default=400)
     ap.add_argument("--cpu-sample-angles", type=int, default=144)
     return ap.parse_args()
 
@@ -228,7 +233,11 @@ def run_ours(a):
         core.compute_maps(mu_in, mu_out, c_os.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
 
     maps_natural()
-    variant = autotune.tune(c, x_true, maps)
+    if a.fp_variant == "auto":
+        variant = autotune.tune(c, x_true, maps)
+    else:
+        variant = 0 if a.fp_variant == "ldg" else core._lib.CCT_VARIANT_FP_TMA
+        c.variant = variant
     c_os.variant = variant
     clean = c.fp(x_true, maps)
     gen = torch.Generator(device=dev)
@@ -432,6 +441,66 @@ def run_ours(a):
     distributed.finalize()
 
 
+def run_ragged(a):
+    """Ragged stream (a seeded sample of the mixed-size workload): slices with sides drawn from
+    {128, 256, 384, 512, 768, 1024} and angle counts uniform in [90, 1440], half SIRT (150
+    iterations), half MLEM to the residual plain MLEM reaches after 200 iterations (calibrated,
+    untimed), solved by ``RaggedStream`` with the ordered-subsets warm start and, for
+    comparison, from the cold start.  Data synthesis is untimed."""
+    import torch
+
+    from pycorrectedemissionct_b200 import core, phantoms, stream
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(a.seed)
+    sizes = (128, 256, 384, 512, 768, 1024)
+    jobs = []
+    for k in range(a.ragged_slices):
+        n = int(rng.choice(sizes))
+        n_ang = int(rng.integers(90, 1441))
+        r = phantoms.slice_rng(a.seed + 7, k)
+        x = phantoms.ellipse_phantom(n, r, 12)
+        mu = phantoms.disk_attenuation(n, r, 0.02)
+        peak = float(10 ** rng.uniform(3, 5))
+        angles = np.linspace(0, 2 * np.pi, n_ang, endpoint=False)
+        c = core.XrfCore(n, angles, device=dev)
+        mu_t = torch.from_numpy(mu).to(dev)[None]
+        maps = core.compute_maps(mu_t, 0.7 * mu_t, c.angles_rad32)
+        clean = c.fp(torch.from_numpy(x).to(dev)[None], maps)
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(a.seed + k)
+        b = torch.poisson(clean / clean.max() * peak, generator=gen)[0, 0].cpu().numpy()
+        del maps, clean
+        jobs.append(stream.Job(n, angles, mu, 0.7 * mu, b, method="sirt" if k % 2 else "mlem"))
+    mlem = [j for j in jobs if j.method == "mlem"]
+    stream.RaggedStream(dev, warm_start=False).solve(mlem, max_iterations=a.iters)  # calibration
+    for j in mlem:
+        j.tolerance = j.extra["residual"] * (1 + 1e-9)
+
+    def reset():
+        for j in jobs:
+            j.x, j.iterations_done, j.finished_s = None, 0, 0.0
+
+    out = {}
+    for name, warm in (("warm", True), ("plain", False)):
+        reset()
+        st = stream.RaggedStream(dev, warm_start=warm)  # schedules follow each slice's angle count
+        r = st.solve(jobs, max_iterations=2 * a.iters)
+        r["launches"] = st.launches
+        r["mlem_mean_passes"] = float(np.mean([j.iterations_done for j in mlem]))
+        r["converged"] = int(sum(j.extra["residual"] <= j.tolerance for j in mlem))
+        out[name] = r
+    line = {
+        "metric": "ragged stream slices/s (mixed sizes and angle counts, half SIRT 150, half MLEM to residual)",
+        "value": out["warm"]["slices_per_s"], "unit": "slices/s", "n_gpus": 1, "higher_is_better": True,
+        "config": {"workload": f"{a.ragged_slices} slices, sides {list(sizes)}, angles U[90, 1440], mu <= 0.02, "
+                               "peaks log-U[1e3, 1e5]", "ragged": "one launch per operator over all groups of a wave"},
+        "p50_s": out["warm"]["p50_s"], "p99_s": out["warm"]["p99_s"], "warm": out["warm"], "plain": out["plain"],
+        "data": "synthetic", "dtype": "f32",
+    }
+    print(json.dumps(line), flush=True)
+
+
 def parse_schedule(text: str) -> list[tuple[int, int]]:
     """'30:10,10:10' -> [(30, 10), (10, 10)] (subsets, passes)."""
     out = []
@@ -445,6 +514,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "ragged":
+        run_ragged(a)
     else:
         run_ours(a)
 

@@ -205,6 +205,37 @@ int cct_reduce_norm(const float* v, int64_t count, int32_t n_slices, int32_t ord
                     double* partials, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * Ragged batches: one launch per operator over groups of slices that differ in size, angle
+ * count, detectors and buffers.  Each group is a uniform batch with its own cct_xrf_desc, maps
+ * and cct_solver_state (as for cct_mlem_step / cct_sirt_step); one cct_ragged_step is one
+ * iteration of every group (fp with the fused epilogue, residuals and stopping tests, bp with
+ * the fused update): three launches for all groups instead of three per group.  No reference
+ * counterpart: the reference solves one slice per call; the per-slice arithmetic is that of
+ * cct_mlem_step (corrct: src/corrct/solvers.py:777-803) and cct_sirt_step (:951-982).
+ * ------------------------------------------------------------------------------------------- */
+#define CCT_METHOD_MLEM 0
+#define CCT_METHOD_SIRT 1
+
+typedef struct cct_ragged_plan cct_ragged_plan; /* opaque host object */
+
+/* Device workspace bytes for a plan of n_groups groups (256-byte aligned tables). */
+int cct_ragged_workspace_size(int32_t n_groups, size_t* bytes);
+
+/* Build a plan: validates every group (one maps type for all, no PSF, per-slice stopping; MLEM
+   uses the reference back projection, SIRT REFERENCE or SYMMETRIC) and copies the launch tables
+   into `workspace` on `stream`.  The plan holds the groups' pointers: it stays valid while their
+   buffers and the workspace live.  maps[g] may be NULL (uncorrected, n_det == 1) for all groups
+   or for none. */
+int cct_ragged_plan_create(int32_t method, int32_t bp_mode, int32_t n_groups, const cct_xrf_desc* descs,
+                           const void* const* maps, const cct_solver_state* states, void* workspace,
+                           size_t workspace_bytes, cct_ragged_plan** plan, void* stream);
+
+/* One iteration of every group (stream-ordered). */
+int cct_ragged_step(const cct_ragged_plan* plan, void* stream);
+
+int cct_ragged_plan_destroy(cct_ragged_plan* plan);
+
+/* ---------------------------------------------------------------------------------------------
  * Learned warm start (no reference counterpart): a small convolutional encoder-decoder whose
  * 3x3 convolutions run as implicit GEMMs on tcgen05 tensor cores (BF16 in, FP32 accumulate in
  * TMEM).  Activations are NHWC bfloat16 with channel counts that are multiples of 16; weights are

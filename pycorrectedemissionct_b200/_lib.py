@@ -29,6 +29,9 @@ CCT_BP_ADJOINT = 2
 
 CCT_VARIANT_FP_TMA = 1
 
+CCT_METHOD_MLEM = 0
+CCT_METHOD_SIRT = 1
+
 c_float_p = ctypes.c_void_p  # device pointers are passed as integers
 
 
@@ -204,6 +207,14 @@ SIGNATURES = {
     ),
     "cct_net_ratio": (ctypes.c_int, [c_float_p, c_float_p, c_float_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p]),
     "cct_net_timeout": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+    "cct_ragged_workspace_size": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_size_t)]),
+    "cct_ragged_plan_create": (
+        ctypes.c_int,
+        [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(XrfDesc), ctypes.POINTER(ctypes.c_void_p),
+         ctypes.POINTER(SolverState), ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p],
+    ),
+    "cct_ragged_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "cct_ragged_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "cct_noise_partials_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int64)]),
     "cct_add_noise": (
         ctypes.c_int,

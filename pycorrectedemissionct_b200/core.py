@@ -129,6 +129,23 @@ class XrfCore:
             self.weights_np = w.astype(np.float32)
             self.weights = torch.from_numpy(np.ascontiguousarray(self.weights_np)).to(self.device)
 
+    def angle_range(self, rng: slice) -> "XrfCore":
+        """The same geometry restricted to a contiguous range of its angles; the device tables are
+        views of this core's (no recomputation, no copies)."""
+        sub = XrfCore.__new__(XrfCore)
+        sub.device, sub.variant, sub.n, sub.n_det = self.device, self.variant, self.n, self.n_det
+        sub.angles_rad32, sub.angles_deg32 = self.angles_rad32[rng], self.angles_deg32[rng]
+        sub.n_angles = len(sub.angles_rad32)
+        sub.fp_mat_np, sub.trig_np = self.fp_mat_np[rng], self.trig_np[rng]
+        sub.fp_mat, sub.trig = self.fp_mat[rng], self.trig[rng]
+        sub.intensities_np = None if self.intensities_np is None else self.intensities_np[rng]
+        sub.line_scale = None if self.line_scale is None else self.line_scale[rng]
+        sub.psf = self.psf
+        sub._base_weights = None if self._base_weights is None else self._base_weights[rng]
+        sub.weights_np = None if self.weights_np is None else self.weights_np[rng]
+        sub.weights = None if self.weights is None else self.weights[rng]
+        return sub
+
     # ------------------------------------------------------------------ descriptors
     def desc(self, n_slices: int, maps_dtype: int = _lib.CCT_DTYPE_F32, angles: slice | None = None) -> _lib.XrfDesc:
         d = _lib.XrfDesc()

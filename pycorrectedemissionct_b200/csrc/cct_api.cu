@@ -2,6 +2,7 @@
 
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "cct_common.cuh"
 #include "cct_internal.cuh"
@@ -283,6 +284,164 @@ int cct_pdhg_step(const cct_xrf_desc* desc, const void* maps, int32_t bp_mode, c
   cct::BpArgs b = make_solver_bp(desc, bp_mode, maps, st, cct::BP_EPI_PDHG);
   cct::launch_bp(b, s);
   return check_launch();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Ragged batches
+// ---------------------------------------------------------------------------------------------
+}  // extern "C"
+
+struct cct_ragged_plan {
+  int method = 0, bp_mode = 0, n_groups = 0, maps_dtype = 0;
+  bool has_maps = false;
+  int64_t fp_ctas = 0, bp_ctas = 0, slices = 0;
+  const cct::FpArgs* d_fp = nullptr;
+  const cct::BpArgs* d_bp = nullptr;
+  const cct::ResidualGroup* d_res = nullptr;
+  const int64_t* d_fp_start = nullptr;
+  const int64_t* d_bp_start = nullptr;
+  const int64_t* d_res_start = nullptr;
+  std::vector<unsigned char> host;  // the tables as copied to the workspace
+};
+
+// Workspace layout: FpArgs[G], BpArgs[G], ResidualGroup[G], then three int64 offset tables of
+// G + 1 entries, each part 256-byte aligned.
+static size_t ragged_layout(int g, size_t off[7]) {
+  auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  size_t o = 0;
+  off[0] = o; o = up(o + sizeof(cct::FpArgs) * g);
+  off[1] = o; o = up(o + sizeof(cct::BpArgs) * g);
+  off[2] = o; o = up(o + sizeof(cct::ResidualGroup) * g);
+  off[3] = o; o = up(o + sizeof(int64_t) * (g + 1));
+  off[4] = o; o = up(o + sizeof(int64_t) * (g + 1));
+  off[5] = o; o = up(o + sizeof(int64_t) * (g + 1));
+  off[6] = o;
+  return o;
+}
+
+extern "C" {
+
+int cct_ragged_workspace_size(int32_t n_groups, size_t* bytes) {
+  CCT_REQUIRE(bytes != nullptr, "bytes is required");
+  CCT_REQUIRE(n_groups >= 1 && n_groups <= (1 << 20), "n_groups must be in [1, 2^20]");
+  size_t off[7];
+  *bytes = ragged_layout(n_groups, off);
+  return CCT_OK;
+}
+
+int cct_ragged_plan_create(int32_t method, int32_t bp_mode, int32_t n_groups, const cct_xrf_desc* descs,
+                           const void* const* maps, const cct_solver_state* states, void* workspace,
+                           size_t workspace_bytes, cct_ragged_plan** plan, void* stream) {
+  CCT_REQUIRE(plan != nullptr && descs != nullptr && maps != nullptr && states != nullptr && workspace != nullptr,
+              "descs, maps, states, workspace and plan are required");
+  *plan = nullptr;
+  CCT_REQUIRE(method == CCT_METHOD_MLEM || method == CCT_METHOD_SIRT, "method must be CCT_METHOD_MLEM or CCT_METHOD_SIRT");
+  CCT_REQUIRE(bp_mode == CCT_BP_REFERENCE || (method == CCT_METHOD_SIRT && bp_mode == CCT_BP_SYMMETRIC),
+              "bp_mode must be REFERENCE (or SYMMETRIC for SIRT)");
+  size_t off[7];
+  int rc = cct_ragged_workspace_size(n_groups, &off[6]);
+  if (rc != CCT_OK) return rc;
+  const size_t need = ragged_layout(n_groups, off);
+  CCT_REQUIRE(workspace_bytes >= need, "workspace is smaller than cct_ragged_workspace_size()");
+  CCT_REQUIRE(reinterpret_cast<uintptr_t>(workspace) % 256 == 0, "workspace must be 256-byte aligned");
+
+  cct_ragged_plan* p = new cct_ragged_plan();
+  p->method = method;
+  p->bp_mode = bp_mode;
+  p->n_groups = n_groups;
+  p->has_maps = maps[0] != nullptr;
+  p->maps_dtype = descs[0].maps_dtype;
+  p->host.assign(need, 0);
+  auto* fp = reinterpret_cast<cct::FpArgs*>(p->host.data() + off[0]);
+  auto* bp = reinterpret_cast<cct::BpArgs*>(p->host.data() + off[1]);
+  auto* res = reinterpret_cast<cct::ResidualGroup*>(p->host.data() + off[2]);
+  auto* fps = reinterpret_cast<int64_t*>(p->host.data() + off[3]);
+  auto* bps = reinterpret_cast<int64_t*>(p->host.data() + off[4]);
+  auto* rss = reinterpret_cast<int64_t*>(p->host.data() + off[5]);
+  auto fail = [&](int code) {
+    delete p;
+    return code;
+  };
+  fps[0] = bps[0] = rss[0] = 0;
+  for (int g = 0; g < n_groups; ++g) {
+    const cct_xrf_desc* d = descs + g;
+    const cct_solver_state* st = states + g;
+    if ((rc = validate_desc(d)) != CCT_OK) return fail(rc);
+    if ((rc = validate_state(d, st)) != CCT_OK) return fail(rc);
+    if (d->psf != nullptr || st->joint_stop || d->maps_dtype != p->maps_dtype || (maps[g] != nullptr) != p->has_maps) {
+      cct_set_last_error("ragged groups need one maps type, no PSF and per-slice stopping");
+      return fail(CCT_ERR_UNSUPPORTED);
+    }
+    if (maps[g] == nullptr && d->n_det != 1) {
+      cct_set_last_error("a group without maps needs n_det == 1");
+      return fail(CCT_ERR_VALUE);
+    }
+    if (method == CCT_METHOD_SIRT && st->sigma == nullptr) {
+      cct_set_last_error("SIRT needs sigma in every group");
+      return fail(CCT_ERR_VALUE);
+    }
+    if (bp_mode == CCT_BP_SYMMETRIC && maps[g] == nullptr) {
+      cct_set_last_error("the symmetric back projection needs maps");
+      return fail(CCT_ERR_VALUE);
+    }
+    cct::FpArgs f = make_fp_args(d, st->x, maps[g], st->sino_buf);
+    f.epi = method == CCT_METHOD_SIRT ? cct::FP_EPI_SIRT : cct::FP_EPI_MLEM;
+    f.b = st->b; f.sigma = st->sigma; f.background = st->background; f.has_background = st->has_background;
+    f.partials = st->partials; f.active = st->active;
+    f.vec4 = cct::fp_vec4_ok(f) ? 1 : 0;
+    fp[g] = f;
+    bp[g] = make_solver_bp(d, method == CCT_METHOD_SIRT ? bp_mode : CCT_BP_REFERENCE,
+                           method == CCT_METHOD_SIRT ? maps[g] : nullptr, st,
+                           method == CCT_METHOD_SIRT ? cct::BP_EPI_SIRT : cct::BP_EPI_MLEM);
+    const int64_t bands = (d->n + 63) / 64;
+    const int64_t per_slice = bands * d->n_angles * d->n_det;
+    res[g] = cct::ResidualGroup{st->partials, per_slice, st->residuals, st->active, st->iterations, st->tolerance,
+                                st->residual_history, st->history_len};
+    const int64_t tiles = (int64_t)((d->n + 31) / 32) * ((d->n + 63) / 64);
+    fps[g + 1] = fps[g] + per_slice * d->n_slices;
+    bps[g + 1] = bps[g] + tiles * d->n_slices;
+    rss[g + 1] = rss[g] + d->n_slices;
+  }
+  p->fp_ctas = fps[n_groups];
+  p->bp_ctas = bps[n_groups];
+  p->slices = rss[n_groups];
+  if (p->fp_ctas > 0x7fffffffLL || p->bp_ctas > 0x7fffffffLL || p->slices > 0x7fffffffLL) {
+    cct_set_last_error("a ragged batch may hold at most 2^31 - 1 CTAs per launch");
+    return fail(CCT_ERR_VALUE);
+  }
+  unsigned char* w = reinterpret_cast<unsigned char*>(workspace);
+  p->d_fp = reinterpret_cast<const cct::FpArgs*>(w + off[0]);
+  p->d_bp = reinterpret_cast<const cct::BpArgs*>(w + off[1]);
+  p->d_res = reinterpret_cast<const cct::ResidualGroup*>(w + off[2]);
+  p->d_fp_start = reinterpret_cast<const int64_t*>(w + off[3]);
+  p->d_bp_start = reinterpret_cast<const int64_t*>(w + off[4]);
+  p->d_res_start = reinterpret_cast<const int64_t*>(w + off[5]);
+  const cudaError_t e = cudaMemcpyAsync(workspace, p->host.data(), need, cudaMemcpyHostToDevice,
+                                        reinterpret_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) {
+    cct_set_last_error(cudaGetErrorString(e));
+    return fail(CCT_ERR_CUDA);
+  }
+  *plan = p;
+  return CCT_OK;
+}
+
+int cct_ragged_step(const cct_ragged_plan* plan, void* stream) {
+  CCT_REQUIRE(plan != nullptr, "plan is NULL");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const bool sirt = plan->method == CCT_METHOD_SIRT;
+  cct::launch_fp_ragged(plan->d_fp, plan->d_fp_start, plan->n_groups, plan->fp_ctas,
+                        sirt ? cct::FP_EPI_SIRT : cct::FP_EPI_MLEM, plan->has_maps, plan->maps_dtype, s);
+  cct::launch_residual_ragged(plan->d_res, plan->d_res_start, plan->n_groups, plan->slices, s);
+  cct::launch_bp_ragged(plan->d_bp, plan->d_bp_start, plan->n_groups, plan->bp_ctas,
+                        sirt ? cct::BP_EPI_SIRT : cct::BP_EPI_MLEM, plan->bp_mode == CCT_BP_SYMMETRIC,
+                        plan->maps_dtype, s);
+  return check_launch();
+}
+
+int cct_ragged_plan_destroy(cct_ragged_plan* plan) {
+  delete plan;
+  return CCT_OK;
 }
 
 int cct_reduce_norm(const float* v, int64_t count, int32_t n_slices, int32_t ord, double* out, double* partials,

@@ -136,9 +136,31 @@ __device__ __forceinline__ void bp_epilogue(const BpArgs& a, int s, int i, int j
 }
 
 void launch_fp(const FpArgs& a, cudaStream_t st);
+bool fp_vec4_ok(const FpArgs& a);  // may the fp staging use 16-byte loads for these pointers
 // PSF convolution of finished sinogram lines (a.vol = input sinogram) with the fp epilogue EPI
 void launch_psf(const FpArgs& a, const float* psf, int psf_len, cudaStream_t st);
 int read_device_error(int clear, int* value);
 void launch_bp(const BpArgs& a, cudaStream_t st);
+
+// Ragged launches: one grid over groups of slices (tables in device memory, CTA offsets
+// start[0..n_groups], start[n_groups] = total CTAs).  Every group shares the epilogue, the
+// presence and the storage type of the maps (and, for bp, the mode).
+void launch_fp_ragged(const FpArgs* groups, const int64_t* start, int n_groups, int64_t ctas, int epi, bool has_maps,
+                      int maps_dtype, cudaStream_t st);
+void launch_bp_ragged(const BpArgs* groups, const int64_t* start, int n_groups, int64_t ctas, int epi, bool sym,
+                      int maps_dtype, cudaStream_t st);
+
+struct ResidualGroup {
+  const double* partials;
+  int64_t per_slice;
+  double* residuals;
+  int* active;
+  int* iterations;
+  const double* tolerance;
+  double* history;
+  int history_len;
+};
+void launch_residual_ragged(const ResidualGroup* groups, const int64_t* slice_start, int n_groups, int64_t slices,
+                            cudaStream_t st);
 
 }  // namespace cct

@@ -85,19 +85,19 @@ __device__ __forceinline__ bool net_mbar_wait(uint64_t* bar, uint32_t phase) {
 
 __device__ __forceinline__ uint4 zero4() { return make_uint4(0u, 0u, 0u, 0u); }
 
-// 8 consecutive k of the im2col row of output pixel m (k = tap * cin + ci, cin % 8 == 0)
-__device__ __forceinline__ uint4 load_im2col(const ConvArgs& a, const __nv_bfloat16* src, int64_t m, int64_t k) {
-  if (m >= a.m_total || k >= a.k_total) return zero4();
+// 8 consecutive k of the im2col row of output pixel m (k = tap * cin + ci, cin % 8 == 0), with the
+// pixel's coordinates hoisted out of the K loop: px points at input pixel (b, y, x) of output row
+// m (valid = m < m_total).  tap / 3 for tap < 9 is (tap * 11) >> 5.
+__device__ __forceinline__ uint4 load_im2col_row(const ConvArgs& a, const __nv_bfloat16* px, int y, int x, bool valid,
+                                                 int64_t k) {
+  if (!valid || k >= a.k_total) return zero4();
   const int tap = (int)(k >> a.log2_cin);
-  const int ci = (int)(k - ((int64_t)tap << a.log2_cin));
-  const int hw = a.h * a.w;
-  const int b = (int)(m / hw);
-  const int rem = (int)(m - (int64_t)b * hw);
-  const int y = rem / a.w, x = rem - (rem / a.w) * a.w;
-  const int ys = y + tap / 3 - 1, xs = x + tap % 3 - 1;
-  if (ys < 0 || ys >= a.h || xs < 0 || xs >= a.w) return zero4();
-  const __nv_bfloat16* p = src + (((int64_t)b * a.h + ys) * a.w + xs) * a.cin + ci;
-  return __ldg(reinterpret_cast<const uint4*>(p));
+  const int ci = (int)(k & (int64_t)(a.cin - 1));
+  const int ty = (tap * 11) >> 5;
+  const int dy = ty - 1, dx = tap - 3 * ty - 1;
+  const int ys = y + dy, xs = x + dx;
+  if ((unsigned)ys >= (unsigned)a.h || (unsigned)xs >= (unsigned)a.w) return zero4();
+  return __ldg(reinterpret_cast<const uint4*>(px + ((int64_t)dy * a.w + dx) * a.cin + ci));
 }
 
 __device__ __forceinline__ uint4 pack8(const __nv_bfloat16 v[8]) {
@@ -160,6 +160,19 @@ __global__ void __launch_bounds__(NET_THREADS) conv_umma_kernel(ConvArgs a) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t m0 = (int64_t)blockIdx.x * NET_BM;
   const int64_t n0 = (int64_t)blockIdx.y * BN;
+  // forward gather: this thread's output pixel, decomposed once
+  const int64_t m_row = m0 + tid;
+  const bool row_valid = MODE == NET_FWD && m_row < a.m_total;
+  int py = 0, px_ = 0;
+  const __nv_bfloat16* prow = a.x;
+  if (row_valid) {
+    const int hw = a.h * a.w;
+    const int b = (int)(m_row / hw);
+    const int rem = (int)(m_row - (int64_t)b * hw);
+    py = rem / a.w;
+    px_ = rem - py * a.w;
+    prow = a.x + m_row * a.cin;
+  }
   int64_t k_begin = 0, k_end = a.k_total;
   if (MODE == NET_WGRAD) {
     k_begin = (int64_t)blockIdx.z * a.k_split;
@@ -200,7 +213,7 @@ __global__ void __launch_bounds__(NET_THREADS) conv_umma_kernel(ConvArgs a) {
         const int64_t k = k0 + 8 * kc;
         uint4 v;
         if (MODE == NET_FWD) {
-          v = load_im2col(a, a.x, m, k);
+          v = load_im2col_row(a, prow, py, px_, row_valid, k);
         } else {
           v = (k < k_end) ? load_wgrad_a(a, m, k) : zero4();
         }
@@ -311,8 +324,10 @@ __global__ void __launch_bounds__(NET_THREADS) conv_umma_kernel(ConvArgs a) {
 
 template <int MODE, int BN>
 static int launch_conv_bn(const ConvArgs& a, cudaStream_t st) {
-  // operand buffers + 32 KB of slack: descriptor-addressed reads can never leave the CTA's window
-  const size_t smem = 2 * (NET_BM * NET_BK * 2) + 2 * (BN * NET_BK * 2) + 32768;
+  // the double-buffered operands; every MMA descriptor addresses inside them (K chunks at
+  // LBO = rows * 16 bytes, core matrices at SBO = 128 bytes), so 3-6 CTAs fit per SM, whose TMEM
+  // columns (BN, at least 32, each) stay within the SM's 512
+  const size_t smem = 2 * (NET_BM * NET_BK * 2) + 2 * (BN * NET_BK * 2);
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(conv_umma_kernel<MODE, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=

@@ -109,16 +109,17 @@ __device__ __forceinline__ void chunk_box(float m00, float m01, float m02, float
   by1 = (int)floorf(ymax) + 2;
 }
 
+// One CTA of the forward projection: detector band `band` of (angle, detector) `ad` of slice
+// `s`; `n_bands` and `n_ad` are the batch's band and (angle, detector) counts (the residual
+// partials are indexed by them).
 template <int EPI, bool HAS_MAPS, int MAPS_DTYPE>
-__global__ void __launch_bounds__(FP_THREADS, 5) fp_kernel(FpArgs args) {
+__device__ __forceinline__ void fp_cta(const FpArgs& args, const int band, const int ad, const int s, const int n_bands,
+                                       const int n_ad) {
   __shared__ __align__(16) float z[FP_BOX_H * FP_STRIDE];
   __shared__ double red_d[FP_TC / FP_LC];
   __shared__ int4 box_sh[FP_MAX_CHUNKS];  // every chunk's box, computed once per CTA
 
   const int n = args.n;
-  const int band = blockIdx.x;
-  const int ad = blockIdx.y;
-  const int s = blockIdx.z;
   if (args.active != nullptr && args.active[s] == 0) return;
   const int a = ad / args.n_det;
   const int d = ad - a * args.n_det;
@@ -268,10 +269,43 @@ __global__ void __launch_bounds__(FP_THREADS, 5) fp_kernel(FpArgs args) {
       double t = 0.0;
 #pragma unroll
       for (int w = 0; w < FP_TC / FP_LC; ++w) t += red_d[w];
-      const int64_t per_slice = (int64_t)gridDim.x * gridDim.y;
-      args.partials[(int64_t)s * per_slice + (int64_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
+      const int64_t per_slice = (int64_t)n_bands * n_ad;
+      args.partials[(int64_t)s * per_slice + (int64_t)ad * n_bands + band] = t;
     }
   }
+}
+
+template <int EPI, bool HAS_MAPS, int MAPS_DTYPE>
+__global__ void __launch_bounds__(FP_THREADS, 5) fp_kernel(FpArgs args) {
+  fp_cta<EPI, HAS_MAPS, MAPS_DTYPE>(args, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y);
+}
+
+// Group g of a ragged launch owns CTAs [start[g], start[g + 1]); binary search over the groups.
+__device__ __forceinline__ int ragged_group(const int64_t* __restrict__ start, int n_groups, int64_t cta) {
+  int lo = 0, hi = n_groups - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(start + mid) <= cta) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Forward projection over groups of slices with different sizes, angle counts and buffers, in
+// one launch: group g's CTAs are (band, angle * detector, slice) in band-fastest order.
+template <int EPI, bool HAS_MAPS, int MAPS_DTYPE>
+__global__ void __launch_bounds__(FP_THREADS, 5) fp_ragged_kernel(const FpArgs* __restrict__ groups,
+                                                                  const int64_t* __restrict__ start, int n_groups) {
+  const int64_t cta = blockIdx.x;
+  const int g = ragged_group(start, n_groups, cta);
+  const FpArgs& a = groups[g];
+  const int n_bands = (a.n + FP_TC - 1) / FP_TC;
+  const int n_ad = a.n_angles * a.n_det;
+  const int64_t local = cta - start[g];
+  const int band = (int)(local % n_bands);
+  const int64_t rest = local / n_bands;
+  const int ad = (int)(rest % n_ad);
+  const int sl = (int)(rest / n_ad);
+  fp_cta<EPI, HAS_MAPS, MAPS_DTYPE>(a, band, ad, sl, n_bands, n_ad);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -497,19 +531,19 @@ constexpr float BP_EDGE_GUARD = 0.01f;
 
 enum : int { LINE_FAST = 0, LINE_CHECKED = 1, LINE_EMPTY = 2 };
 
+// One CTA of the back projection: pixel tile `tile` of slice `s`.
 template <int EPI, bool SYM, int MAPS_DTYPE>
-__global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
+__device__ __forceinline__ void bp_cta(const BpArgs& args, const int tile, const int s) {
   __shared__ __align__(16) float2 pairs[BP_LINES][BP_KW];
   __shared__ float4 linfo[BP_LINES];  // cos, sin, offset (K - kbase), weight
   __shared__ int lkind[BP_LINES];
   __shared__ int lkbase[BP_LINES];
 
   const int n = args.n;
-  const int s = blockIdx.y;
   if (args.active != nullptr && args.active[s] == 0) return;
   const int tiles_j = (n + BP_TJ - 1) / BP_TJ;
-  const int ti = blockIdx.x / tiles_j;
-  const int tj = blockIdx.x - ti * tiles_j;
+  const int ti = tile / tiles_j;
+  const int tj = tile - ti * tiles_j;
   const int i0 = ti * BP_TI, j0 = tj * BP_TJ;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int j = j0 + lane;
@@ -639,6 +673,24 @@ __global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
     const int i = i0 + warp + 8 * k;
     if (i < n && j < n) bp_epilogue<EPI>(args, s, i, j, acc[k]);
   }
+}
+
+template <int EPI, bool SYM, int MAPS_DTYPE>
+__global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
+  bp_cta<EPI, SYM, MAPS_DTYPE>(args, blockIdx.x, blockIdx.y);
+}
+
+// Back projection over groups of slices in one launch: group g's CTAs are (tile, slice),
+// tile fastest.
+template <int EPI, bool SYM, int MAPS_DTYPE>
+__global__ void __launch_bounds__(BP_THREADS) bp_ragged_kernel(const BpArgs* __restrict__ groups,
+                                                               const int64_t* __restrict__ start, int n_groups) {
+  const int64_t cta = blockIdx.x;
+  const int g = ragged_group(start, n_groups, cta);
+  const BpArgs& a = groups[g];
+  const int tiles = ((a.n + BP_TJ - 1) / BP_TJ) * ((a.n + BP_TI - 1) / BP_TI);
+  const int64_t local = cta - start[g];
+  bp_cta<EPI, SYM, MAPS_DTYPE>(a, (int)(local % tiles), (int)(local / tiles));
 }
 
 // ------------------------------------------------------------------------------------------
@@ -804,6 +856,14 @@ static bool launch_fp_tma_inst(const FpArgs& a, const dim3& grid, cudaStream_t s
   return true;
 }
 
+// 16-byte staging loads need a 16-byte aligned volume, maps at 16 (FP32) or 8 (BF16) bytes and
+// map images that stay aligned (n % 4 == 0, slice stride a multiple of 4 elements)
+bool fp_vec4_ok(const FpArgs& a) {
+  const uintptr_t map_align = a.maps_dtype == CCT_DTYPE_BF16 ? 8 : 16;
+  return (a.n % 4) == 0 && (reinterpret_cast<uintptr_t>(a.vol) % 16) == 0 &&
+         (a.maps == nullptr || ((reinterpret_cast<uintptr_t>(a.maps) % map_align) == 0 && a.maps_slice_stride % 4 == 0));
+}
+
 template <int EPI>
 static void launch_fp_epi(const FpArgs& a, cudaStream_t st) {
   const dim3 grid((a.n + FP_TC - 1) / FP_TC, a.n_angles * a.n_det, a.n_slices);
@@ -823,12 +883,8 @@ static void launch_fp_epi(const FpArgs& a, cudaStream_t st) {
     }
     if (ok) return;
   }
-  // 16-byte staging loads need a 16-byte aligned volume, maps at 16 (FP32) or 8 (BF16) bytes and
-  // map images that stay aligned (n % 4 == 0, slice stride a multiple of 4 elements)
   FpArgs v = a;
-  const uintptr_t map_align = a.maps_dtype == CCT_DTYPE_BF16 ? 8 : 16;
-  v.vec4 = (a.n % 4) == 0 && (reinterpret_cast<uintptr_t>(a.vol) % 16) == 0 &&
-           (a.maps == nullptr || ((reinterpret_cast<uintptr_t>(a.maps) % map_align) == 0 && a.maps_slice_stride % 4 == 0));
+  v.vec4 = fp_vec4_ok(a) ? 1 : 0;
   if (a.maps == nullptr) {
     fp_kernel<EPI, false, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(v);
   } else if (a.maps_dtype == CCT_DTYPE_BF16) {
@@ -858,6 +914,50 @@ static void launch_bp_epi(const BpArgs& a, cudaStream_t st) {
     bp_kernel<EPI, true, CCT_DTYPE_BF16><<<grid, BP_THREADS, 0, st>>>(a);
   } else {
     bp_kernel<EPI, true, CCT_DTYPE_F32><<<grid, BP_THREADS, 0, st>>>(a);
+  }
+}
+
+template <int EPI>
+static void launch_fp_ragged_epi(const FpArgs* g, const int64_t* start, int ng, int64_t ctas, bool has_maps, int dt,
+                                 cudaStream_t st) {
+  const dim3 grid((unsigned)ctas);
+  if (!has_maps) {
+    fp_ragged_kernel<EPI, false, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(g, start, ng);
+  } else if (dt == CCT_DTYPE_BF16) {
+    fp_ragged_kernel<EPI, true, CCT_DTYPE_BF16><<<grid, FP_THREADS, 0, st>>>(g, start, ng);
+  } else {
+    fp_ragged_kernel<EPI, true, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(g, start, ng);
+  }
+}
+
+void launch_fp_ragged(const FpArgs* groups, const int64_t* start, int n_groups, int64_t ctas, int epi, bool has_maps,
+                      int maps_dtype, cudaStream_t st) {
+  if (epi == FP_EPI_SIRT) {
+    launch_fp_ragged_epi<FP_EPI_SIRT>(groups, start, n_groups, ctas, has_maps, maps_dtype, st);
+  } else {
+    launch_fp_ragged_epi<FP_EPI_MLEM>(groups, start, n_groups, ctas, has_maps, maps_dtype, st);
+  }
+}
+
+template <int EPI>
+static void launch_bp_ragged_epi(const BpArgs* g, const int64_t* start, int ng, int64_t ctas, bool sym, int dt,
+                                 cudaStream_t st) {
+  const dim3 grid((unsigned)ctas);
+  if (!sym) {
+    bp_ragged_kernel<EPI, false, CCT_DTYPE_F32><<<grid, BP_THREADS, 0, st>>>(g, start, ng);
+  } else if (dt == CCT_DTYPE_BF16) {
+    bp_ragged_kernel<EPI, true, CCT_DTYPE_BF16><<<grid, BP_THREADS, 0, st>>>(g, start, ng);
+  } else {
+    bp_ragged_kernel<EPI, true, CCT_DTYPE_F32><<<grid, BP_THREADS, 0, st>>>(g, start, ng);
+  }
+}
+
+void launch_bp_ragged(const BpArgs* groups, const int64_t* start, int n_groups, int64_t ctas, int epi, bool sym,
+                      int maps_dtype, cudaStream_t st) {
+  if (epi == BP_EPI_SIRT) {
+    launch_bp_ragged_epi<BP_EPI_SIRT>(groups, start, n_groups, ctas, sym, maps_dtype, st);
+  } else {
+    launch_bp_ragged_epi<BP_EPI_MLEM>(groups, start, n_groups, ctas, sym, maps_dtype, st);
   }
 }
 

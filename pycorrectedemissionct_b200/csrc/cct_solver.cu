@@ -127,6 +127,37 @@ void launch_residual_step(const double* partials, int64_t per_slice, int n_slice
                                                    history_len);
 }
 
+// residual_step_kernel over groups of slices in one launch (one CTA per slice of every group).
+__global__ void __launch_bounds__(RED_THREADS) residual_ragged_kernel(const ResidualGroup* __restrict__ groups,
+                                                                      const int64_t* __restrict__ start,
+                                                                      int n_groups) {
+  const int64_t gs = blockIdx.x;
+  int lo = 0, hi = n_groups - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (start[mid] <= gs) lo = mid; else hi = mid - 1;
+  }
+  const ResidualGroup& g = groups[lo];
+  const int s = (int)(gs - start[lo]);
+  if (g.active[s] == 0) return;
+  double v = 0.0;
+  const double* p = g.partials + (int64_t)s * g.per_slice;
+  for (int64_t k = threadIdx.x; k < g.per_slice; k += RED_THREADS) v += p[k];
+  v = block_sum_double(v);
+  if (threadIdx.x == 0) {
+    g.residuals[s] = v;
+    const int it = g.iterations[s];
+    if (g.history != nullptr && it < g.history_len) g.history[(int64_t)s * g.history_len + it] = v;
+    g.iterations[s] = it + 1;
+    if (g.tolerance != nullptr && g.tolerance[s] > v) g.active[s] = 0;
+  }
+}
+
+void launch_residual_ragged(const ResidualGroup* groups, const int64_t* slice_start, int n_groups, int64_t slices,
+                            cudaStream_t st) {
+  residual_ragged_kernel<<<(unsigned)slices, RED_THREADS, 0, st>>>(groups, slice_start, n_groups);
+}
+
 void launch_tv_dual(const float* x_relax, float* q, int n, int n_slices, float lam, const int* active,
                     cudaStream_t st) {
   const dim3 grid((unsigned)(((int64_t)n * n + 255) / 256), n_slices);

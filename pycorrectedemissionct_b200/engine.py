@@ -274,19 +274,33 @@ class BatchedSolver:
 def subset_permutation(n_angles: int, levels: list[int]) -> np.ndarray:
     """Angle order in which every subset of every level is one contiguous range.
 
-    ``levels`` are subset counts, each dividing the one before and all dividing ``n_angles``;
-    a subset of k holds the angles a with a mod k equal to its index (every k-th angle).
-    Angles are grouped by residue modulo the finest count, and those groups by residue modulo
-    each coarser count, so the subsets of a coarser level are unions of consecutive finer ones.
+    ``levels`` are subset counts, each dividing the one before (and none above ``n_angles``);
+    a subset of k holds the angles a with a mod k equal to its index (every k-th angle; subsets
+    differ in size by at most one when k does not divide ``n_angles``).  Angles are grouped by
+    residue modulo the finest count, and those groups by residue modulo each coarser count, so
+    the subsets of a coarser level are unions of consecutive finer ones.
     """
     levels = [int(k) for k in levels]
-    if not levels or any(k < 1 or n_angles % k for k in levels):
-        raise ValueError(f"every subset count must divide the {n_angles} angles: {levels}")
+    if not levels or any(k < 1 or k > n_angles for k in levels):
+        raise ValueError(f"subset counts must be in [1, {n_angles}]: {levels}")
     if any(levels[i] % levels[i + 1] for i in range(len(levels) - 1)):
         raise ValueError(f"each subset count must divide the previous one: {levels}")
     finest = levels[0]
     residues = sorted(range(finest), key=lambda r: tuple(r % k for k in reversed(levels)))
     return np.concatenate([np.arange(r, n_angles, finest) for r in residues])
+
+
+def subset_ranges(n_angles: int, levels: list[int]) -> list[list[slice]]:
+    """Per level, the ranges of ``subset_permutation(n_angles, levels)`` that hold its subsets."""
+    perm = subset_permutation(n_angles, levels)
+    out = []
+    for k in levels:
+        res = perm % k
+        cuts = [0] + [i for i in range(1, n_angles) if res[i] != res[i - 1]] + [n_angles]
+        out.append([slice(cuts[i], cuts[i + 1]) for i in range(len(cuts) - 1)])
+        if len(out[-1]) != k:
+            raise AssertionError("subset ranges are not contiguous")
+    return out
 
 
 class OrderedSubsets:
@@ -305,25 +319,17 @@ class OrderedSubsets:
         self.core = core
         self.device = core.device
         self.schedule = [(int(k), int(p)) for k, p in schedule]
-        subset_permutation(core.n_angles, [k for k, _ in self.schedule])  # validates the levels
+        ranges = subset_ranges(core.n_angles, [k for k, _ in self.schedule])  # validates the levels
         s, n = b.shape[0], core.n
         self.x = torch.ones((s, n, n), dtype=torch.float32, device=self.device)
         if x0 is not None:
             self.x.copy_(x0)
         self.levels: list[list[BatchedSolver]] = []
-        a_all = core.angles_rad32.astype(np.float64)
-        for k, _ in self.schedule:
-            per = core.n_angles // k
+        self.ranges = ranges
+        for level_ranges in ranges:
             solvers = []
-            for m in range(k):
-                rng = slice(m * per, (m + 1) * per)
-                sub = XrfCore(n, a_all[rng], n_det=core.n_det, device=self.device, variant=core.variant)
-                if core._base_weights is not None:
-                    sub.set_weights(core._base_weights[rng])
-                if core.intensities_np is not None:
-                    sub.set_intensities(core.intensities_np[rng])
-                if core.psf is not None:
-                    sub.set_psf(core.psf.cpu().numpy())
+            for rng in level_ranges:
+                sub = core.angle_range(rng)
                 sub_maps = None if maps is None else maps[:, rng]
                 b_sub = b[:, :, rng].contiguous()
                 solvers.append(BatchedSolver(sub, sub_maps, b_sub, "mlem", x_shared=self.x))
@@ -342,10 +348,9 @@ class OrderedSubsets:
 
     def set_data(self, b: torch.Tensor) -> None:
         """Refresh every subset's copy of the data from ``b`` (subset-major angle order)."""
-        for level in self.levels:
-            per = self.core.n_angles // len(level)
-            for m, sm in enumerate(level):
-                sm.b.copy_(b[:, :, m * per : (m + 1) * per])
+        for level, level_ranges in zip(self.levels, self.ranges):
+            for sm, rng in zip(level, level_ranges):
+                sm.b.copy_(b[:, :, rng])
 
     def _pass(self, level: int) -> None:
         for sm in self.levels[level]:
@@ -377,3 +382,67 @@ class OrderedSubsets:
     @property
     def passes(self) -> int:
         return sum(p for _, p in self.schedule)
+
+
+# ------------------------------------------------------------------------------- ragged batches
+class RaggedSolvers:
+    """One iteration of many uniform batches (different n, angle counts, detectors) in three
+    launches: the fp with its fused epilogue, the residuals and stopping tests, and the bp with
+    its fused update run once over all groups' CTAs (``cct_ragged_step``).
+
+    ``solvers``: BatchedSolver objects, all MLEM or all SIRT (same bp mode), one maps type, no
+    PSF.  Each keeps its own buffers; their iterates, residuals and active flags evolve exactly
+    as if each were stepped on its own.
+    """
+
+    def __init__(self, solvers: list[BatchedSolver]):
+        if not solvers:
+            raise ValueError("no solvers")
+        methods = {sv.method for sv in solvers}
+        if len(methods) != 1 or next(iter(methods)) not in ("mlem", "sirt"):
+            raise ValueError("a ragged batch steps MLEM solvers or SIRT solvers, not a mix")
+        self.solvers = list(solvers)
+        self.method = next(iter(methods))
+        self.device = solvers[0].device
+        g = len(solvers)
+        bp_modes = {sv.bp_mode for sv in solvers}
+        if len(bp_modes) != 1:
+            raise ValueError("every group must use the same back-projection mode")
+        self.bp_mode = next(iter(bp_modes))
+        lib = _lib.load()
+        nbytes = ctypes.c_size_t(0)
+        _lib.check(lib.cct_ragged_workspace_size(g, ctypes.byref(nbytes)))
+        self.workspace = torch.empty(int(nbytes.value) + 256, dtype=torch.uint8, device=self.device)
+        base = self.workspace.data_ptr()
+        self._ws_ptr = (base + 255) & ~255
+        descs = (_lib.XrfDesc * g)(*[sv.desc for sv in solvers])
+        maps = (ctypes.c_void_p * g)(*[sv._maps_ptr for sv in solvers])
+        states = (_lib.SolverState * g)(*[sv.state for sv in solvers])
+        plan = ctypes.c_void_p(0)
+        method = _lib.CCT_METHOD_MLEM if self.method == "mlem" else _lib.CCT_METHOD_SIRT
+        _lib.check(
+            lib.cct_ragged_plan_create(
+                method, _BP_MODE_CODES[self.bp_mode], g, descs, maps, states, self._ws_ptr, int(nbytes.value),
+                ctypes.byref(plan), stream_handle(self.device),
+            )
+        )
+        self._plan = plan
+        self._lib = lib
+
+    def step(self) -> None:
+        """One iteration of every group, queued on the current stream."""
+        _lib.check(self._lib.cct_ragged_step(self._plan, stream_handle(self.device)))
+
+    def active(self) -> int:
+        return int(sum(int(sv.active.sum().item()) for sv in self.solvers))
+
+    def close(self) -> None:
+        if getattr(self, "_plan", None):
+            self._lib.cct_ragged_plan_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,215 @@
+"""Ragged streams: many slices of different sizes and angle counts, solved in waves.
+
+Every slice is a job: its side n, its rotation angles, its incident / emitted attenuation and its
+data, solved either by SIRT for a fixed number of iterations or by MLEM to a data-residual
+tolerance (the reference's stopping rule).  Jobs are packed into waves whose device memory (maps
+and solver buffers) fits a budget; inside a wave, jobs with the same (n, angles, method) form a
+uniform group, and every operator of every iteration runs as ONE ragged launch over all groups
+(``cct_ragged_step``): SIRT groups together, MLEM groups together, and for the MLEM warm start
+every ordered-subsets step over all groups' subset m together.  With ``warm_start=False`` MLEM
+starts from the reference's default (the plain cold-start path).
+
+The per-slice arithmetic is that of ``BatchedSolver`` (and so of corrct's solvers), which the
+ragged kernels reproduce bit for bit.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import core as _core
+from .engine import BatchedSolver, OrderedSubsets, RaggedSolvers, subset_permutation
+
+
+@dataclass
+class Job:
+    """One slice.  ``b`` is (A, n) float32 data in the order of ``angles``."""
+
+    n: int
+    angles: np.ndarray
+    mu_in: np.ndarray | None
+    mu_out: np.ndarray | None
+    b: np.ndarray
+    method: str = "mlem"          # "mlem" (to `tolerance`) or "sirt" (`iterations`)
+    tolerance: float | None = None
+    iterations: int = 150
+    # results
+    x: np.ndarray | None = None
+    iterations_done: int = 0
+    finished_s: float = 0.0
+    extra: dict = field(default_factory=dict)
+
+
+def job_bytes(job: Job, maps_bytes: int = 4) -> int:
+    """Device bytes a job holds while its wave runs (maps, data and solver buffers)."""
+    a, n = len(job.angles), job.n
+    return a * n * n * maps_bytes + 6 * a * n * 4 + 8 * n * n * 4
+
+
+def default_schedule(n_angles: int, angles_per_subset: int = 12) -> list[tuple[int, int]]:
+    """Ordered-subsets schedule for a slice of ``n_angles`` angles: 3 passes over subsets of about
+    ``angles_per_subset`` angles (an even count), then 2 passes over half as many subsets (twice
+    the angles); 720 angles give [(60, 3), (30, 2)]."""
+    k = max(2, (n_angles // angles_per_subset) // 2 * 2)
+    return [(k, 3), (k // 2, 2)]
+
+
+class _Group:
+    def __init__(self, jobs: list[Job], device, maps_dtype: str, schedule, warm: bool, workspace: torch.Tensor):
+        j0 = jobs[0]
+        self.jobs = jobs
+        self.method = j0.method
+        angles = np.asarray(j0.angles, dtype=np.float64)
+        if schedule is None:
+            schedule = default_schedule(len(angles))
+        self.schedule = None if schedule is None else [(int(k), int(p)) for k, p in schedule]
+        levels = [k for k, _ in self.schedule]
+        self.perm = None
+        if self.method == "mlem" and warm:
+            self.perm = subset_permutation(len(angles), levels)
+            angles = angles[self.perm]
+        self.core = _core.XrfCore(j0.n, angles, device=device)
+        f32 = dict(dtype=torch.float32, device=device)
+        mu_in = None if j0.mu_in is None else torch.from_numpy(np.stack([j.mu_in for j in jobs])).to(**f32)
+        mu_out = None if j0.mu_out is None else torch.from_numpy(np.stack([j.mu_out for j in jobs])).to(**f32)
+        self.maps = _core.compute_maps(mu_in, mu_out, self.core.angles_rad32, maps_dtype=maps_dtype,
+                                       workspace=workspace)
+        b = np.stack([j.b for j in jobs])[:, None]
+        if self.perm is not None:
+            b = b[:, :, self.perm]
+        self.b = torch.from_numpy(np.ascontiguousarray(b, dtype=np.float32)).to(device)
+        if self.method == "sirt":
+            self.solver = BatchedSolver(self.core, self.maps, self.b, "sirt")
+            self.subsets = None
+        else:
+            tol = np.array([j.tolerance for j in jobs], dtype=np.float64)
+            self.subsets = OrderedSubsets(self.core, self.maps, self.b, self.schedule) if warm else None
+            x_shared = None if self.subsets is None else self.subsets.x
+            self.solver = BatchedSolver(self.core, self.maps, self.b, "mlem", tolerance=tol, x_shared=x_shared)
+
+
+class RaggedStream:
+    """Solve a list of jobs in waves of at most ``memory_budget`` device bytes.
+
+    schedule : ordered-subsets warm start of the MLEM jobs, [(subsets, passes), ...] for every
+        job, or None for ``default_schedule`` of each job's angle count.
+    check_every : MLEM iterations between two host checks of the stopping flags.
+    """
+
+    def __init__(self, device=None, memory_budget: int = 100 << 30, schedule=None,
+                 maps_dtype: str = "float32", warm_start: bool = True, check_every: int = 2):
+        self.device = _core.require_cuda(device)
+        self.memory_budget = int(memory_budget)
+        self.schedule = None if schedule is None else [(int(k), int(p)) for k, p in schedule]
+        self.maps_dtype = maps_dtype
+        self.warm = bool(warm_start)
+        self.check_every = int(check_every)
+        self.launches = 0
+
+    def waves(self, jobs: list[Job]) -> list[list[Job]]:
+        mb = 2 if self.maps_dtype == "bfloat16" else 4
+        order = sorted(jobs, key=lambda j: (j.method, j.n, len(j.angles)))
+        out, cur, used = [], [], 0
+        for j in order:
+            need = job_bytes(j, mb)
+            if cur and used + need > self.memory_budget:
+                out.append(cur)
+                cur, used = [], 0
+            cur.append(j)
+            used += need
+        if cur:
+            out.append(cur)
+        return out
+
+    def solve(self, jobs: list[Job], max_iterations: int = 1000) -> dict:
+        """Solve every job (results in ``job.x``, ``job.iterations_done``, ``job.finished_s`` =
+        seconds from the start of the stream to the slice's completion).  Returns totals."""
+        torch.cuda.synchronize(self.device)
+        t0 = time.perf_counter()
+        ws = torch.empty(_core.DEFAULT_MAPS_WORKSPACE, dtype=torch.uint8, device=self.device)
+        for wave in self.waves(jobs):
+            groups = {}
+            for j in wave:
+                if j.method not in ("mlem", "sirt"):
+                    raise ValueError(f"unknown method {j.method!r}")
+                key = (j.method, j.n, len(j.angles), tuple(np.round(np.asarray(j.angles, np.float64), 9)))
+                groups.setdefault(key, []).append(j)
+            gs = [_Group(js, self.device, self.maps_dtype, self.schedule, self.warm, ws) for js in groups.values()]
+            self._run_sirt([g for g in gs if g.method == "sirt"], t0)
+            self._run_mlem([g for g in gs if g.method == "mlem"], t0, max_iterations)
+            del gs
+        torch.cuda.synchronize(self.device)
+        total = time.perf_counter() - t0
+        done = np.array([j.finished_s for j in jobs])
+        return dict(seconds=total, slices=len(jobs), slices_per_s=len(jobs) / total,
+                    p50_s=float(np.percentile(done, 50)), p99_s=float(np.percentile(done, 99)))
+
+    def _finish(self, g: _Group, t0: float) -> None:
+        x = g.solver.x.cpu().numpy()
+        its = g.solver.iterations.cpu().numpy()
+        res = g.solver.residuals.cpu().numpy()
+        for k, j in enumerate(g.jobs):
+            j.x = x[k]
+            j.extra["residual"] = float(res[k])
+            j.iterations_done = int(its[k]) + (g.subsets.passes if g.subsets is not None else 0)
+            if j.finished_s == 0.0:
+                j.finished_s = time.perf_counter() - t0
+
+    def _run_sirt(self, gs: list[_Group], t0: float) -> None:
+        if not gs:
+            return
+        rag = RaggedSolvers([g.solver for g in gs])
+        iters = max(j.iterations for g in gs for j in g.jobs)
+        for _ in range(iters):
+            rag.step()
+            self.launches += 3
+        torch.cuda.synchronize(self.device)
+        for g in gs:
+            self._finish(g, t0)
+        rag.close()
+
+    def _run_mlem(self, gs: list[_Group], t0: float, max_iterations: int) -> None:
+        if not gs:
+            return
+        if self.warm:
+            # step t of a level applies subset t mod k_g of every group g still in its passes, all
+            # groups in one ragged launch per operator
+            for li in range(max(len(g.schedule) for g in gs)):
+                live = [g for g in gs if li < len(g.schedule)]
+                steps = max(g.schedule[li][0] * g.schedule[li][1] for g in live)
+                for t in range(steps):
+                    members = [g.subsets.levels[li][t % g.schedule[li][0]] for g in live
+                               if t < g.schedule[li][0] * g.schedule[li][1]]
+                    p = RaggedSolvers(members)
+                    p.step()
+                    self.launches += 3
+                    p.close()
+        rag = RaggedSolvers([g.solver for g in gs])
+        its = 0
+        pending = list(gs)
+        while pending and its < max_iterations:
+            for _ in range(self.check_every):
+                rag.step()
+                self.launches += 3
+            its += self.check_every
+            flags = torch.cat([g.solver.active for g in pending]).cpu().numpy()  # one copy per check
+            now = time.perf_counter() - t0
+            still, pos = [], 0
+            for g in pending:
+                act = flags[pos : pos + len(g.jobs)]
+                pos += len(g.jobs)
+                for k, j in enumerate(g.jobs):
+                    if act[k] == 0 and j.finished_s == 0.0:
+                        j.finished_s = now
+                if act.any():
+                    still.append(g)
+                else:
+                    self._finish(g, t0)
+            pending = still
+        for g in pending:
+            self._finish(g, t0)
+        rag.close()

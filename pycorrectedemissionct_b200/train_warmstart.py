@@ -20,7 +20,7 @@ import numpy as np
 import torch
 
 from . import _lib, core, phantoms
-from .engine import BatchedSolver
+from .engine import BatchedSolver, OrderedSubsets, subset_permutation
 from .warmstart import N_ITERATES, WarmStartNet
 
 
@@ -60,14 +60,28 @@ def first_iterates(solver: BatchedSolver, count: int = N_ITERATES) -> list[torch
     return its
 
 
-def synth_batch(n: int, n_angles: int, seeds: list[int], mu_max: float, peak: float, device, textured: bool = True):
-    """Phantoms, attenuation, maps and Poisson data for one batch of slices."""
+def subsets_iterates(os_: OrderedSubsets, count: int = N_ITERATES) -> list[torch.Tensor]:
+    """Run `count` passes of a one-level ordered-subsets schedule, keeping the iterate after each."""
+    its = []
+    for _ in range(count):
+        os_.run()
+        its.append(os_.x.clone())
+    return its
+
+
+def synth_batch(n: int, n_angles: int, seeds: list[int], mu_max: float, peak: float, device, textured: bool = True,
+                subsets: int = 0):
+    """Phantoms, attenuation, maps and Poisson data for one batch of slices (angles in the
+    ``subset_permutation`` order of ``subsets`` subsets when ``subsets`` > 0)."""
     xs, mus = [], []
     for sd in seeds:
         rng = phantoms.slice_rng(sd, 0)
         xs.append(textured_phantom(n, rng) if textured else phantoms.ellipse_phantom(n, rng, 12))
         mus.append(phantoms.disk_attenuation(n, rng, mu_max))
-    c = core.XrfCore(n, phantoms.angles(n_angles), device=device)
+    angles = phantoms.angles(n_angles)
+    if subsets > 0:
+        angles = angles[subset_permutation(n_angles, [subsets])]
+    c = core.XrfCore(n, angles, device=device)
     mu = torch.from_numpy(np.stack(mus)).to(device)
     maps = core.compute_maps(mu, 0.7 * mu, c.angles_rad32)
     x = torch.from_numpy(np.stack(xs)).to(device)
@@ -84,13 +98,19 @@ def generate_pairs(n_slices: int, n: int = 256, n_angles: int = 360, seed: int =
     device = core.require_cuda(device)
     helper = net if net is not None else WarmStartNet(device=device)
     inputs, targets = [], []
+    n_sub = helper.first_subsets
     for s0 in range(0, n_slices, batch):
         seeds = [seed + k for k in range(s0, min(n_slices, s0 + batch))]
-        c, maps, b, _ = synth_batch(n, n_angles, seeds, mu_max, peak, device)
+        c, maps, b, _ = synth_batch(n, n_angles, seeds, mu_max, peak, device, subsets=n_sub)
         solver = BatchedSolver(c, maps, b, "mlem")
-        its = first_iterates(solver)
-        bpn = normalized_backprojection(c, b, solver.tau)
-        solver.run(target_iterations - N_ITERATES, check_every=target_iterations, use_graph=False)
+        if n_sub > 0:
+            its = subsets_iterates(OrderedSubsets(c, maps, b, [(n_sub, 1)]))
+            bpn = normalized_backprojection(c, b, solver.tau)
+            solver.run(target_iterations, check_every=target_iterations, use_graph=False)
+        else:
+            its = first_iterates(solver)
+            bpn = normalized_backprojection(c, b, solver.tau)
+            solver.run(target_iterations - N_ITERATES, check_every=target_iterations, use_graph=False)
         scale = slice_means(its[-1])
         inputs.append(helper.pack(its + [bpn], scale))
         sc = scale[:, None, None]
@@ -132,11 +152,16 @@ def train(net: WarmStartNet, inputs: torch.Tensor, targets: torch.Tensor, steps:
 
 def warm_started_solve(net: WarmStartNet, c: core.XrfCore, maps: torch.Tensor, b: torch.Tensor, tolerance,
                        max_iterations: int = 400, check_every: int = 5, history_len: int = 0):
-    """10 plain MLEM iterations -> network -> MLEM from the prediction until `tolerance`.
+    """10 plain MLEM iterations (or ordered-subsets passes, by the network's inputs) -> network ->
+    MLEM from the prediction until `tolerance`.  With ordered-subsets inputs, ``c``, ``maps`` and
+    ``b`` must be in ``subset_permutation(A, [net.first_subsets])`` angle order.
 
-    Returns (solver, total iterations per slice as a numpy array)."""
+    Returns (solver, total full-data passes per slice as a numpy array)."""
     first = BatchedSolver(c, maps, b, "mlem")
-    its = first_iterates(first)
+    if net.first_subsets > 0:
+        its = subsets_iterates(OrderedSubsets(c, maps, b, [(net.first_subsets, 1)]))
+    else:
+        its = first_iterates(first)
     bpn = normalized_backprojection(c, b, first.tau)
     scale = slice_means(its[-1])
     x0 = net.predict(its + [bpn], base=its[-1], slice_scale=scale)
@@ -156,6 +181,8 @@ def main():
     ap.add_argument("--target-iterations", type=int, default=500)
     ap.add_argument("--additive", action="store_true", help="additive instead of log-ratio (multiplicative) targets")
     ap.add_argument("--log-floor", type=float, default=1e-3, help="floor of the log-ratio target, in slice means")
+    ap.add_argument("--first-subsets", type=int, default=0,
+                    help="inputs from ordered-subsets passes over this many subsets (0: MLEM iterates)")
     ap.add_argument("--out", default="warmstart.pt")
     a = ap.parse_args()
     dev = core.require_cuda()
@@ -163,6 +190,7 @@ def main():
     net = WarmStartNet(seed=0, device=dev)
     net.multiplicative = not a.additive
     net.log_floor = a.log_floor
+    net.first_subsets = a.first_subsets
     inputs, targets = generate_pairs(a.slices, a.n, a.angles, target_iterations=a.target_iterations, device=dev, net=net)
     torch.cuda.synchronize()
     t1 = time.time()

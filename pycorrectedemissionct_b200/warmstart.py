@@ -87,6 +87,9 @@ class WarmStartNet:
         # log((x_target + floor * scale) / (x10 + floor * scale))
         self.multiplicative = False
         self.log_floor = 1e-2
+        # inputs: 0 = the first 10 MLEM iterates; k > 0 = the iterates after each of the first 10
+        # ordered-subsets passes over k subsets
+        self.first_subsets = 0
 
     # ------------------------------------------------------------------ helpers
     def n_params(self) -> int:
@@ -250,7 +253,8 @@ class WarmStartNet:
     def save(self, path: str) -> None:
         """BF16 weights, FP32 biases and the target parameterisation."""
         st = {k: (l.w.to(BF16).cpu(), l.b.cpu()) for k, l in self.layers.items()}
-        st.update(step=self.step_count, multiplicative=self.multiplicative, log_floor=self.log_floor)
+        st.update(step=self.step_count, multiplicative=self.multiplicative, log_floor=self.log_floor,
+                  first_subsets=self.first_subsets)
         torch.save(st, path)
 
     def load(self, path: str) -> None:
@@ -262,3 +266,4 @@ class WarmStartNet:
         self.step_count = int(st.get("step", 0))
         self.multiplicative = bool(st.get("multiplicative", False))
         self.log_floor = float(st.get("log_floor", 1e-2))
+        self.first_subsets = int(st.get("first_subsets", 0))

@@ -131,6 +131,19 @@ def test_subset_permutation_nests_levels():
                 assert len(set((block % k).tolist())) == 1  # one residue class: every k-th angle
                 assert np.all(np.diff(np.sort(block)) == k)
     with pytest.raises(ValueError):
-        subset_permutation(720, [7])
+        subset_permutation(720, [721])
     with pytest.raises(ValueError):
         subset_permutation(720, [10, 4])
+
+
+def test_subset_ranges_for_any_angle_count():
+    from pycorrectedemissionct_b200.engine import subset_permutation, subset_ranges
+
+    for n_ang, levels in ((737, [60, 30]), (91, [9, 3]), (720, [60, 30]), (97, [7])):
+        p = subset_permutation(n_ang, levels)
+        for k, ranges in zip(levels, subset_ranges(n_ang, levels)):
+            assert len(ranges) == k
+            sizes = [r.stop - r.start for r in ranges]
+            assert sum(sizes) == n_ang and max(sizes) - min(sizes) <= 1
+            for r in ranges:
+                assert len(set((p[r] % k).tolist())) == 1
