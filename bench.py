@@ -423,7 +423,7 @@ def run_ours(a):
             # DRAM bytes per launch from one ncu capture of this kernel on 2 slices (1.4366 GB), scaled
             # by the slices per launch; only for the capture's own configuration
             "traffic": (1.4366e9 / 2 * S) if (n == 512 and a.angles == 720 and a.maps_dtype == "float32") else None,
-            "kernel": "fp_kernel<MLEM> (attenuated fp + ratio + KL residual)",
+            "kernel": ("fp_tma_kernel" if variant else "fp_kernel") + "<MLEM> (attenuated fp + ratio + KL residual)",
             "peak_source": peak_src, "fp_launch_us": fp_avg_s * 1e6, "bp_launch_us": bp_avg_s * 1e6,
             "algorithmic_bytes_per_launch": fp_bytes,
         },
@@ -489,6 +489,7 @@ def run_ragged(a):
         r["launches"] = st.launches
         r["mlem_mean_passes"] = float(np.mean([j.iterations_done for j in mlem]))
         r["converged"] = int(sum(j.extra["residual"] <= j.tolerance for j in mlem))
+        r["restarted"] = int(sum(bool(j.extra.get("restarted")) for j in mlem))
         out[name] = r
     line = {
         "metric": "ragged stream slices/s (mixed sizes and angle counts, half SIRT 150, half MLEM to residual)",

@@ -73,6 +73,8 @@ class _Group:
             self.perm = subset_permutation(len(angles), levels)
             angles = angles[self.perm]
         self.core = _core.XrfCore(j0.n, angles, device=device)
+        self.restarted = False
+        self.judge_its = self.spent = 0
         f32 = dict(dtype=torch.float32, device=device)
         mu_in = None if j0.mu_in is None else torch.from_numpy(np.stack([j.mu_in for j in jobs])).to(**f32)
         mu_out = None if j0.mu_out is None else torch.from_numpy(np.stack([j.mu_out for j in jobs])).to(**f32)
@@ -98,16 +100,19 @@ class RaggedStream:
     schedule : ordered-subsets warm start of the MLEM jobs, [(subsets, passes), ...] for every
         job, or None for ``default_schedule`` of each job's angle count.
     check_every : MLEM iterations between two host checks of the stopping flags.
+    fallback_after : judging MLEM iterations after which a warm-started group that has not met
+        its residual restarts from the default start (plain MLEM is the fallback).
     """
 
     def __init__(self, device=None, memory_budget: int = 100 << 30, schedule=None,
-                 maps_dtype: str = "float32", warm_start: bool = True, check_every: int = 2):
+                 maps_dtype: str = "float32", warm_start: bool = True, check_every: int = 2, fallback_after: int = 200):
         self.device = _core.require_cuda(device)
         self.memory_budget = int(memory_budget)
         self.schedule = None if schedule is None else [(int(k), int(p)) for k, p in schedule]
         self.maps_dtype = maps_dtype
         self.warm = bool(warm_start)
         self.check_every = int(check_every)
+        self.fallback_after = int(fallback_after)
         self.launches = 0
 
     def waves(self, jobs: list[Job]) -> list[list[Job]]:
@@ -155,7 +160,8 @@ class RaggedStream:
         for k, j in enumerate(g.jobs):
             j.x = x[k]
             j.extra["residual"] = float(res[k])
-            j.iterations_done = int(its[k]) + (g.subsets.passes if g.subsets is not None else 0)
+            j.iterations_done = int(its[k]) + (g.spent if g.restarted else (g.subsets.passes if g.subsets is not None else 0))
+            j.extra["restarted"] = g.restarted
             if j.finished_s == 0.0:
                 j.finished_s = time.perf_counter() - t0
 
@@ -191,11 +197,22 @@ class RaggedStream:
         rag = RaggedSolvers([g.solver for g in gs])
         its = 0
         pending = list(gs)
+        for g in gs:
+            g.judge_its, g.spent = 0, 0
         while pending and its < max_iterations:
             for _ in range(self.check_every):
                 rag.step()
                 self.launches += 3
             its += self.check_every
+            # the plain solver is the fallback: a warm-started group whose slices have not met their
+            # residual after `fallback_after` judging iterations restarts from the default start
+            for g in pending:
+                g.judge_its += self.check_every
+                if self.warm and g.subsets is not None and g.judge_its >= self.fallback_after and not g.restarted:
+                    if int(g.solver.active.sum().item()) > 0:
+                        g.spent = g.subsets.passes + g.judge_its
+                        g.solver.reset()
+                        g.restarted = True
             flags = torch.cat([g.solver.active for g in pending]).cpu().numpy()  # one copy per check
             now = time.perf_counter() - t0
             still, pos = [], 0
