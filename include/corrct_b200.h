@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define CCT_ABI_VERSION 2
+#define CCT_ABI_VERSION 3
 
 /* Status codes. */
 #define CCT_OK 0
@@ -37,6 +37,15 @@ extern "C" {
 /* Map storage types. */
 #define CCT_DTYPE_F32 0
 #define CCT_DTYPE_BF16 1
+#define CCT_DTYPE_FIELDS_F32 2 /* line-integral fields instead of maps: [S/C][A][1 + D][n][n] float32 with
+                                  plane 0 = L_in and plane 1 + d = L_out of detector d for the emitted
+                                  attenuation of the slice's first channel; channel c of a slice uses the
+                                  map exp(-(L_in + channel_scale[c] * L_out)).  Slices are channel-major
+                                  within a field slice (slice s = field slice s / C, channel s % C).  For
+                                  fluorescence channels whose emitted attenuation is a multiple of one
+                                  volume (mu_out,c = s_c * mu_out) the line integrals are linear in mu
+                                  (corrct: src/corrct/_projector_backends.py:43-99 is linear up to the
+                                  exp), so C channels need two fields instead of C maps. */
 
 /* Back-projection modes. */
 #define CCT_BP_REFERENCE 0 /* scikit-image iradon discretisation, no maps, no weights
@@ -70,10 +79,11 @@ typedef struct cct_xrf_desc {
                              the back projection ignores it, as the reference's default is_symm=False
                              makes its adjoint the identity), or NULL */
   int32_t psf_len;
-  int32_t reserved;
-  int64_t maps_slice_stride; /* elements between the maps of consecutive slices; 0 = dense
-                                (n_angles * n_det * n * n).  Lets a call read the maps of an angle
-                                range out of a larger [S][A_total][D][n][n] array. */
+  int32_t n_channels;        /* CCT_DTYPE_FIELDS_F32: channels per field slice (n_slices % n_channels == 0) */
+  int64_t maps_slice_stride; /* elements between the maps (or fields) of consecutive slices (field
+                                slices); 0 = dense (n_angles * n_det * n * n, or n_angles * (1 + n_det)
+                                * n * n for fields).  Lets a call read an angle range of a larger array. */
+  const float* channel_scale; /* device [n_channels]: s_c of CCT_DTYPE_FIELDS_F32 */
 } cct_xrf_desc;
 
 /* Library identity. */
@@ -124,7 +134,9 @@ typedef struct cct_maps_desc {
 int cct_maps_workspace_size(const cct_maps_desc* desc, int32_t angles_per_pass, size_t* bytes);
 
 /* Compute maps.  mu_in / mu_out: device [S][n][n] float32 (NULL when absent).  The number of
-   angles per pass is the largest that fits in workspace_bytes. */
+   angles per pass is the largest that fits in workspace_bytes.  maps_dtype = CCT_DTYPE_FIELDS_F32
+   writes the line-integral fields [S][A][1 + D][n][n] (L_in, then L_out per detector; zero for an
+   absent volume; needs n_sub == 1) instead of maps. */
 int cct_compute_maps(const cct_maps_desc* desc, const float* mu_in, const float* mu_out, void* maps,
                      void* workspace, size_t workspace_bytes, void* stream);
 

@@ -13,7 +13,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcorrct_b200.so")
 
-ABI_VERSION = 2  # CCT_ABI_VERSION of include/corrct_b200.h
+ABI_VERSION = 3  # CCT_ABI_VERSION of include/corrct_b200.h
 
 CCT_OK = 0
 CCT_ERR_VALUE = 1
@@ -22,6 +22,7 @@ CCT_ERR_UNSUPPORTED = 3
 
 CCT_DTYPE_F32 = 0
 CCT_DTYPE_BF16 = 1
+CCT_DTYPE_FIELDS_F32 = 2
 
 CCT_BP_REFERENCE = 0
 CCT_BP_SYMMETRIC = 1
@@ -49,8 +50,9 @@ class XrfDesc(ctypes.Structure):
         ("line_scale", ctypes.c_void_p),
         ("psf", ctypes.c_void_p),
         ("psf_len", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("n_channels", ctypes.c_int32),
         ("maps_slice_stride", ctypes.c_int64),
+        ("channel_scale", ctypes.c_void_p),
     ]
 
 

@@ -14,7 +14,13 @@ import torch
 
 from . import _lib, geometry
 
-MAPS_DTYPES = {"float32": (torch.float32, _lib.CCT_DTYPE_F32), "bfloat16": (torch.bfloat16, _lib.CCT_DTYPE_BF16)}
+MAPS_DTYPES = {
+    "float32": (torch.float32, _lib.CCT_DTYPE_F32),
+    "bfloat16": (torch.bfloat16, _lib.CCT_DTYPE_BF16),
+    # line-integral fields (S, A, 1 + D, n, n): L_in, then L_out per detector; channel c of a field
+    # slice uses exp(-(L_in + s_c L_out)) (``XrfCore.set_channels``)
+    "fields-float32": (torch.float32, _lib.CCT_DTYPE_FIELDS_F32),
+}
 
 BP_MODES = {"reference": _lib.CCT_BP_REFERENCE, "symmetric": _lib.CCT_BP_SYMMETRIC, "adjoint": _lib.CCT_BP_ADJOINT}
 
@@ -88,8 +94,22 @@ class XrfCore:
         self.intensities_np = None
         self.line_scale = None
         self.psf = None
+        self.n_channels = 0
+        self.channel_scale = None
         self._base_weights = None
         self.set_weights(weights)
+
+    def set_channels(self, scales) -> None:
+        """Fluorescence channels read from line-integral fields: slice s of a batch is channel
+        s % C of field slice s // C, with map exp(-(L_in + scales[c] * L_out)).  None clears."""
+        if scales is None:
+            self.n_channels, self.channel_scale = 0, None
+            return
+        sc = np.asarray(scales, dtype=np.float32).reshape(-1)
+        if sc.size < 1:
+            raise ValueError("at least one channel scale is required")
+        self.n_channels = int(sc.size)
+        self.channel_scale = torch.from_numpy(np.ascontiguousarray(sc)).to(self.device)
 
     def set_weights(self, weights) -> None:
         """Detector x angle weights ``w_det[d] * w_angle[a, d]`` (None = ones)."""
@@ -141,6 +161,7 @@ class XrfCore:
         sub.intensities_np = None if self.intensities_np is None else self.intensities_np[rng]
         sub.line_scale = None if self.line_scale is None else self.line_scale[rng]
         sub.psf = self.psf
+        sub.n_channels, sub.channel_scale = self.n_channels, self.channel_scale
         sub._base_weights = None if self._base_weights is None else self._base_weights[rng]
         sub.weights_np = None if self.weights_np is None else self.weights_np[rng]
         sub.weights = None if self.weights is None else self.weights[rng]
@@ -169,6 +190,9 @@ class XrfCore:
             d.line_scale = None if self.line_scale is None else self.line_scale[a0:a1].data_ptr()
         d.psf = _ptr(self.psf)
         d.psf_len = 0 if self.psf is None else int(self.psf.numel())
+        if maps_dtype == _lib.CCT_DTYPE_FIELDS_F32:
+            d.n_channels = self.n_channels
+            d.channel_scale = _ptr(self.channel_scale)
         return d
 
     # ------------------------------------------------------------------ projections
@@ -233,7 +257,20 @@ class XrfCore:
     def _check_maps(self, maps: torch.Tensor, s: int, n_angles: int | None = None) -> int:
         """Maps (S, A', D, n, n): each slice's block contiguous; the slices may be further apart
         (an angle range of larger maps, ``maps[:, a0:a1]``)."""
-        shape = (s, self.n_angles if n_angles is None else n_angles, self.n_det, self.n, self.n)
+        na = self.n_angles if n_angles is None else n_angles
+        if self.n_channels > 0 and maps.dim() == 5 and maps.shape[2] == self.n_det + 1:
+            # line-integral fields of s / C field slices
+            if s % self.n_channels:
+                raise ValueError(f"{s} slices are not a whole number of {self.n_channels}-channel field slices")
+            fshape = (s // self.n_channels, na, self.n_det + 1, self.n, self.n)
+            if maps.shape[0] > 1 and maps[0].is_contiguous() and maps.stride(0) >= maps[0].numel():
+                _check_tensor(maps[0], fshape[1:], torch.float32, self.device, "fields")
+                if tuple(maps.shape) != fshape:
+                    raise ValueError(f"fields have shape {tuple(maps.shape)}, expected {fshape}")
+            else:
+                _check_tensor(maps, fshape, torch.float32, self.device, "fields")
+            return _lib.CCT_DTYPE_FIELDS_F32
+        shape = (s, na, self.n_det, self.n, self.n)
         dtype = torch.bfloat16 if maps.dtype == torch.bfloat16 else torch.float32
         if maps.dim() == 5 and maps.shape[0] > 1 and maps[0].is_contiguous() and maps.stride(0) >= maps[0].numel():
             _check_tensor(maps[0], shape[1:], dtype, self.device, "maps")
@@ -292,10 +329,11 @@ def compute_maps(
         # at least 8 angles (of the whole batch) per pass, at most all of them
         nbytes = min(max(int(workspace_bytes), 8 * int(need.value)), int(need.value) * n_ang)
         workspace = torch.empty(nbytes, dtype=torch.uint8, device=device)
+    planes = n_det + 1 if cdt == _lib.CCT_DTYPE_FIELDS_F32 else n_det
     if out is None:
-        maps = torch.empty((s, n_ang, n_det, n, n), dtype=tdt, device=device)
+        maps = torch.empty((s, n_ang, planes, n, n), dtype=tdt, device=device)
     else:
-        _check_tensor(out, (s, n_ang, n_det, n, n), tdt, device, "out")
+        _check_tensor(out, (s, n_ang, planes, n, n), tdt, device, "out")
         maps = out
     compute_maps.last_passes = -(-n_ang // max(1, (workspace.numel() * workspace.element_size()) // int(need.value)))
     _lib.call(

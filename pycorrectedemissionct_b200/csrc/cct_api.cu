@@ -33,25 +33,32 @@ static int check_launch() {
   return CCT_OK;
 }
 
+static int64_t dense_maps_stride(const cct_xrf_desc* d) {
+  const int64_t planes = d->maps_dtype == CCT_DTYPE_FIELDS_F32 ? 1 + d->n_det : d->n_det;
+  return (int64_t)d->n_angles * planes * d->n * d->n;
+}
+
 static int validate_desc(const cct_xrf_desc* d) {
   CCT_REQUIRE(d != nullptr, "descriptor is NULL");
   CCT_REQUIRE(d->n >= 2 && d->n <= 8192, "volume side n must be in [2, 8192]");
   CCT_REQUIRE(d->n_angles >= 1 && d->n_det >= 1 && d->n_slices >= 1, "n_angles, n_det and n_slices must be >= 1");
   CCT_REQUIRE((int64_t)d->n_angles * d->n_det <= 65535, "n_angles * n_det must be <= 65535");
   CCT_REQUIRE(d->n_slices <= 65535, "n_slices must be <= 65535");
-  CCT_REQUIRE(d->maps_dtype == CCT_DTYPE_F32 || d->maps_dtype == CCT_DTYPE_BF16, "maps_dtype must be F32 or BF16");
+  CCT_REQUIRE(d->maps_dtype == CCT_DTYPE_F32 || d->maps_dtype == CCT_DTYPE_BF16 || d->maps_dtype == CCT_DTYPE_FIELDS_F32,
+              "maps_dtype must be F32, BF16 or FIELDS_F32");
+  CCT_REQUIRE(d->maps_dtype != CCT_DTYPE_FIELDS_F32 ||
+                  (d->n_channels >= 1 && d->channel_scale != nullptr && d->n_slices % d->n_channels == 0),
+              "fields need n_channels >= 1 dividing n_slices and channel_scale");
   CCT_REQUIRE(d->fp_matrix != nullptr && d->bp_trig != nullptr, "fp_matrix and bp_trig are required");
   CCT_REQUIRE(d->psf == nullptr || (d->psf_len >= 1 && d->psf_len <= 1024), "psf_len must be in [1, 1024]");
   CCT_REQUIRE(d->maps_slice_stride >= 0, "maps_slice_stride must be >= 0");
-  CCT_REQUIRE(d->maps_slice_stride == 0 ||
-                  d->maps_slice_stride >= (int64_t)d->n_angles * d->n_det * d->n * d->n,
-              "maps_slice_stride must be 0 or at least n_angles * n_det * n * n");
+  CCT_REQUIRE(d->maps_slice_stride == 0 || d->maps_slice_stride >= dense_maps_stride(d),
+              "maps_slice_stride must be 0 or at least one slice's maps (fields)");
   return CCT_OK;
 }
 
 static int64_t maps_stride(const cct_xrf_desc* d) {
-  const int64_t dense = (int64_t)d->n_angles * d->n_det * d->n * d->n;
-  return d->maps_slice_stride > 0 ? d->maps_slice_stride : dense;
+  return d->maps_slice_stride > 0 ? d->maps_slice_stride : dense_maps_stride(d);
 }
 
 static cct::FpArgs make_fp_args(const cct_xrf_desc* d, const float* vol, const void* maps, float* out) {
@@ -61,6 +68,8 @@ static cct::FpArgs make_fp_args(const cct_xrf_desc* d, const float* vol, const v
   a.maps_dtype = d->maps_dtype; a.epi = cct::FP_EPI_STORE; a.variant = d->variant;
   a.fp_matrix = d->fp_matrix; a.weights = d->weights; a.vol = vol; a.maps = maps; a.out = out;
   a.maps_slice_stride = maps_stride(d);
+  a.n_channels = d->n_channels > 0 ? d->n_channels : 1;
+  a.chan_scale = d->channel_scale;
   return a;
 }
 
@@ -72,6 +81,8 @@ static cct::BpArgs make_bp_args(const cct_xrf_desc* d, int mode, const float* si
   a.fp_matrix = d->fp_matrix; a.bp_trig = d->bp_trig; a.weights = d->weights; a.line_scale = d->line_scale;
   a.sino = sino; a.maps = maps; a.out = out;
   a.maps_slice_stride = maps_stride(d);
+  a.n_channels = d->n_channels > 0 ? d->n_channels : 1;
+  a.chan_scale = d->channel_scale;
   return a;
 }
 
@@ -125,8 +136,11 @@ int cct_compute_maps(const cct_maps_desc* desc, const float* mu_in, const float*
   size_t need = 0;
   int rc = cct_maps_workspace_size(desc, 1, &need);
   if (rc != CCT_OK) return rc;
-  CCT_REQUIRE(desc->maps_dtype == CCT_DTYPE_F32 || desc->maps_dtype == CCT_DTYPE_BF16,
-              "maps_dtype must be F32 or BF16");
+  CCT_REQUIRE(desc->maps_dtype == CCT_DTYPE_F32 || desc->maps_dtype == CCT_DTYPE_BF16 ||
+                  desc->maps_dtype == CCT_DTYPE_FIELDS_F32,
+              "maps_dtype must be F32, BF16 or FIELDS_F32");
+  CCT_REQUIRE(desc->maps_dtype != CCT_DTYPE_FIELDS_F32 || desc->n_sub == 1,
+              "line-integral fields need one emitted direction per detector (n_sub == 1)");
   CCT_REQUIRE(!desc->has_in || (mu_in != nullptr && desc->rot_in != nullptr), "incident volume or matrices missing");
   CCT_REQUIRE(!desc->has_out || (mu_out != nullptr && desc->rot_out != nullptr), "emitted volume or matrices missing");
   CCT_REQUIRE(maps != nullptr && workspace != nullptr, "maps and workspace are required");

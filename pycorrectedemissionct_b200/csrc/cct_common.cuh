@@ -21,6 +21,63 @@ __device__ __forceinline__ float load_map(const void* base, int dtype, int64_t i
   return __ldg(reinterpret_cast<const float*>(base) + idx);
 }
 
+// The map of one (slice, angle, detector): an image of stored maps, or the two line-integral
+// planes of a fields slice and the channel's scale (map = exp(-(L_in + scale * L_out))).
+struct MapRef {
+  const void* base;
+  int64_t off;     // map image, or the L_out plane
+  int64_t off_in;  // fields: the L_in plane
+  float scale;     // fields: the channel's s_c
+};
+
+__device__ __forceinline__ MapRef make_map_ref(const void* maps, int dtype, int64_t slice_stride, int n_angles,
+                                               int n_det, int n, int s, int a, int d, int n_channels,
+                                               const float* channel_scale) {
+  const int64_t plane = (int64_t)n * n;
+  MapRef r;
+  r.base = maps;
+  if (dtype == CCT_DTYPE_FIELDS_F32) {
+    const int fs = s / n_channels;
+    const int c = s - fs * n_channels;
+    r.off_in = (int64_t)fs * slice_stride + (int64_t)a * (1 + n_det) * plane;
+    r.off = r.off_in + (int64_t)(1 + d) * plane;
+    r.scale = __ldg(channel_scale + c);
+  } else {
+    r.off = (int64_t)s * slice_stride + ((int64_t)a * n_det + d) * plane;
+    r.off_in = 0;
+    r.scale = 0.f;
+  }
+  return r;
+}
+
+template <int DT>
+__device__ __forceinline__ float map_at(const MapRef& m, int64_t pix) {
+  if (DT == CCT_DTYPE_FIELDS_F32) {
+    const float* f = reinterpret_cast<const float*>(m.base);
+    return expf(-fmaf(m.scale, __ldg(f + m.off + pix), __ldg(f + m.off_in + pix)));
+  }
+  return load_map(m.base, DT, m.off + pix);
+}
+
+// Four consecutive map values (pix % 4 == 0, 16-byte aligned FP32 / 8-byte aligned BF16 data).
+template <int DT>
+__device__ __forceinline__ float4 map_at4(const MapRef& m, int64_t pix) {
+  if (DT == CCT_DTYPE_BF16) {
+    const uint2 raw = __ldg(reinterpret_cast<const uint2*>(reinterpret_cast<const __nv_bfloat16*>(m.base) + m.off + pix));
+    const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.x));
+    const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.y));
+    return make_float4(lo.x, lo.y, hi.x, hi.y);
+  }
+  const float* f = reinterpret_cast<const float*>(m.base);
+  if (DT == CCT_DTYPE_FIELDS_F32) {
+    const float4 li = __ldg(reinterpret_cast<const float4*>(f + m.off_in + pix));
+    const float4 lo = __ldg(reinterpret_cast<const float4*>(f + m.off + pix));
+    return make_float4(expf(-fmaf(m.scale, lo.x, li.x)), expf(-fmaf(m.scale, lo.y, li.y)),
+                       expf(-fmaf(m.scale, lo.z, li.z)), expf(-fmaf(m.scale, lo.w, li.w)));
+  }
+  return __ldg(reinterpret_cast<const float4*>(f + m.off + pix));
+}
+
 // floor() of a coordinate in [-2^22, 2^22) without the conversion pipe:
 // adding 1.5*2^23 with round-down leaves floor(x) in the low mantissa bits.
 struct FloorSplit {

@@ -19,7 +19,9 @@ enum BpEpilogue : int { BP_EPI_STORE = 0, BP_EPI_MLEM = 1, BP_EPI_SIRT = 2, BP_E
 struct FpArgs {
   int n, n_angles, n_det, n_slices, maps_dtype, epi, variant;
   int vec4;                    // 16-byte staging loads allowed (n % 4 == 0 and aligned pointers)
-  int64_t maps_slice_stride;   // elements between consecutive slices' maps
+  int64_t maps_slice_stride;   // elements between consecutive slices' maps (field slices' fields)
+  int n_channels;              // CCT_DTYPE_FIELDS_F32: channels per field slice
+  const float* chan_scale;
   const float* fp_matrix;
   const float* weights;
   const float* vol;
@@ -35,7 +37,9 @@ struct FpArgs {
 
 struct BpArgs {
   int n, n_angles, n_det, n_slices, maps_dtype, mode, epi;
-  int64_t maps_slice_stride;   // elements between consecutive slices' maps
+  int64_t maps_slice_stride;   // elements between consecutive slices' maps (field slices' fields)
+  int n_channels;
+  const float* chan_scale;
   const float* fp_matrix;
   const float* bp_trig;
   const float* weights;

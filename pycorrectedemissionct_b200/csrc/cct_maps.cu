@@ -144,6 +144,14 @@ __global__ void __launch_bounds__(256) maps_resample_kernel(MapsPass p) {
     return bilin_zero(wbase + (int64_t)job * P * P, P, P, x, y);
   };
 
+  if (p.maps_dtype == CCT_DTYPE_FIELDS_F32) {
+    // line-integral fields: plane 0 = L_in, plane 1 + d = L_out of detector d (n_sub == 1)
+    float* fo = reinterpret_cast<float*>(p.maps) + ((int64_t)s * p.n_angles + a) * (1 + p.n_det) * (int64_t)n * n + pix;
+    fo[0] = p.has_in ? sample_job(0) : 0.f;
+    for (int d = 0; d < p.n_det; ++d)
+      fo[(int64_t)(1 + d) * n * n] = p.has_out ? sample_job((p.has_in ? 1 : 0) + d) : 0.f;
+    return;
+  }
   float f_in = 1.f;
   int job = 0;
   if (p.has_in) {

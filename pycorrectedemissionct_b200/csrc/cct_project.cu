@@ -57,24 +57,15 @@ static_assert(FP_MAX_CHUNKS <= FP_THREADS, "one thread per chunk box");
 constexpr int FP_FILL_BATCH = 3;                   // float4 items whose loads are issued together
 
 template <bool HAS_MAPS, int MAPS_DTYPE>
-__device__ __forceinline__ float4 fp_load_item(const float* vol, const void* maps, int64_t map_off, int n, int gy,
-                                               int gx, bool vec4) {
+__device__ __forceinline__ float4 fp_load_item(const float* vol, const MapRef& mref, int n, int gy, int gx, bool vec4) {
   float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
   if (gy < 0 || gy >= n || gx + 3 < 0 || gx >= n) return v;
   const int off = gy * n + gx;  // < 2^31 for n <= 8192... n*n <= 2^26
   if (vec4 && gx >= 0 && gx + 3 < n) {
     v = __ldg(reinterpret_cast<const float4*>(vol + off));
     if (HAS_MAPS) {
-      if (MAPS_DTYPE == CCT_DTYPE_BF16) {
-        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(
-            reinterpret_cast<const __nv_bfloat16*>(maps) + map_off + off));
-        const float2 flo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.x));
-        const float2 fhi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.y));
-        v.x *= flo.x; v.y *= flo.y; v.z *= fhi.x; v.w *= fhi.y;
-      } else {
-        const float4 mv = __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const float*>(maps) + map_off + off));
-        v.x *= mv.x; v.y *= mv.y; v.z *= mv.z; v.w *= mv.w;
-      }
+      const float4 mv = map_at4<MAPS_DTYPE>(mref, off);
+      v.x *= mv.x; v.y *= mv.y; v.z *= mv.z; v.w *= mv.w;
     }
     return v;
   }
@@ -85,7 +76,7 @@ __device__ __forceinline__ float4 fp_load_item(const float* vol, const void* map
     float val = 0.f;
     if (xx >= 0 && xx < n) {
       val = __ldg(vol + off + k);
-      if (HAS_MAPS) val *= load_map(maps, MAPS_DTYPE, map_off + off + k);
+      if (HAS_MAPS) val *= map_at<MAPS_DTYPE>(mref, off + k);
     }
     e[k] = val;
   }
@@ -137,7 +128,8 @@ __device__ __forceinline__ void fp_cta(const FpArgs& args, const int band, const
   const int c_last = min(c0 + FP_TC, n) - 1;
 
   const float* vol = args.vol + (int64_t)s * n * n;
-  const int64_t map_off = (int64_t)s * args.maps_slice_stride + ((int64_t)a * args.n_det + d) * (int64_t)n * n;
+  const MapRef mref = make_map_ref(args.maps, MAPS_DTYPE, args.maps_slice_stride, args.n_angles, args.n_det, n, s, a,
+                                   d, args.n_channels, args.chan_scale);
   const bool vec4 = args.vec4 != 0;
   const float fc = (float)c;
   const float pxc = fmaf(m00, fc, m02);
@@ -189,21 +181,12 @@ __device__ __forceinline__ void fp_cta(const FpArgs& args, const int band, const
               const int off = gy * n + gx;
               v[k] = __ldg(reinterpret_cast<const float4*>(vol + off));
               if (HAS_MAPS) {
-                if (MAPS_DTYPE == CCT_DTYPE_BF16) {
-                  const uint2 raw = __ldg(reinterpret_cast<const uint2*>(
-                      reinterpret_cast<const __nv_bfloat16*>(args.maps) + map_off + off));
-                  const float2 flo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.x));
-                  const float2 fhi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.y));
-                  v[k].x *= flo.x; v[k].y *= flo.y; v[k].z *= fhi.x; v[k].w *= fhi.y;
-                } else {
-                  const float4 mv = __ldg(reinterpret_cast<const float4*>(
-                      reinterpret_cast<const float*>(args.maps) + map_off + off));
-                  v[k].x *= mv.x; v[k].y *= mv.y; v[k].z *= mv.z; v[k].w *= mv.w;
-                }
+                const float4 mv = map_at4<MAPS_DTYPE>(mref, off);
+                v[k].x *= mv.x; v[k].y *= mv.y; v[k].z *= mv.z; v[k].w *= mv.w;
               }
             }
           } else {
-            v[k] = fp_load_item<HAS_MAPS, MAPS_DTYPE>(vol, args.maps, map_off, n, gy, gx, false);
+            v[k] = fp_load_item<HAS_MAPS, MAPS_DTYPE>(vol, mref, n, gy, gx, false);
           }
         }
       }
@@ -657,9 +640,9 @@ __device__ __forceinline__ void bp_cta(const BpArgs& args, const int tile, const
         }
         if (SYM) {
           if (i < n && j < n) {
-            const int64_t moff = (int64_t)s * args.maps_slice_stride + ((int64_t)a * args.n_det + d) * (int64_t)n * n +
-                                 (int64_t)i * n + j;
-            v *= load_map(args.maps, MAPS_DTYPE, moff);
+            const MapRef mr = make_map_ref(args.maps, MAPS_DTYPE, args.maps_slice_stride, args.n_angles, args.n_det, n,
+                                           s, a, d, args.n_channels, args.chan_scale);
+            v *= map_at<MAPS_DTYPE>(mr, (int64_t)i * n + j);
           }
         }
         acc[k] += v;
@@ -737,8 +720,9 @@ __global__ void __launch_bounds__(256) bp_adjoint_kernel(BpArgs args) {
     float w = args.weights != nullptr ? args.weights[a * args.n_det + d] : 1.f;
     double contrib = lsum * w;
     if (HAS_MAPS) {
-      const int64_t moff = (int64_t)s * args.maps_slice_stride + ((int64_t)a * args.n_det + d) * (int64_t)n * n + pix;
-      contrib *= load_map(args.maps, MAPS_DTYPE, moff);
+      const MapRef mr = make_map_ref(args.maps, MAPS_DTYPE, args.maps_slice_stride, args.n_angles, args.n_det, n, s, a, d,
+                                     args.n_channels, args.chan_scale);
+      contrib *= map_at<MAPS_DTYPE>(mr, pix);
     }
     acc += contrib;
   }
@@ -871,7 +855,7 @@ static void launch_fp_epi(const FpArgs& a, cudaStream_t st) {
   const int64_t dense = (int64_t)a.n_angles * a.n_det * a.n * a.n;
   const bool aligned = (a.n % 8) == 0 && (reinterpret_cast<uintptr_t>(a.vol) % 16) == 0 &&
                        (a.maps == nullptr || (reinterpret_cast<uintptr_t>(a.maps) % 16) == 0) &&
-                       a.maps_slice_stride == dense;
+                       a.maps_slice_stride == dense && a.maps_dtype != CCT_DTYPE_FIELDS_F32;
   if (aligned && (a.variant & CCT_VARIANT_FP_TMA)) {
     bool ok;
     if (a.maps == nullptr) {
@@ -889,6 +873,8 @@ static void launch_fp_epi(const FpArgs& a, cudaStream_t st) {
     fp_kernel<EPI, false, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(v);
   } else if (a.maps_dtype == CCT_DTYPE_BF16) {
     fp_kernel<EPI, true, CCT_DTYPE_BF16><<<grid, FP_THREADS, 0, st>>>(v);
+  } else if (a.maps_dtype == CCT_DTYPE_FIELDS_F32) {
+    fp_kernel<EPI, true, CCT_DTYPE_FIELDS_F32><<<grid, FP_THREADS, 0, st>>>(v);
   } else {
     fp_kernel<EPI, true, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(v);
   }
@@ -912,6 +898,8 @@ static void launch_bp_epi(const BpArgs& a, cudaStream_t st) {
     bp_kernel<EPI, false, CCT_DTYPE_F32><<<grid, BP_THREADS, 0, st>>>(a);
   } else if (a.maps_dtype == CCT_DTYPE_BF16) {
     bp_kernel<EPI, true, CCT_DTYPE_BF16><<<grid, BP_THREADS, 0, st>>>(a);
+  } else if (a.maps_dtype == CCT_DTYPE_FIELDS_F32) {
+    bp_kernel<EPI, true, CCT_DTYPE_FIELDS_F32><<<grid, BP_THREADS, 0, st>>>(a);
   } else {
     bp_kernel<EPI, true, CCT_DTYPE_F32><<<grid, BP_THREADS, 0, st>>>(a);
   }
@@ -925,6 +913,8 @@ static void launch_fp_ragged_epi(const FpArgs* g, const int64_t* start, int ng, 
     fp_ragged_kernel<EPI, false, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(g, start, ng);
   } else if (dt == CCT_DTYPE_BF16) {
     fp_ragged_kernel<EPI, true, CCT_DTYPE_BF16><<<grid, FP_THREADS, 0, st>>>(g, start, ng);
+  } else if (dt == CCT_DTYPE_FIELDS_F32) {
+    fp_ragged_kernel<EPI, true, CCT_DTYPE_FIELDS_F32><<<grid, FP_THREADS, 0, st>>>(g, start, ng);
   } else {
     fp_ragged_kernel<EPI, true, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(g, start, ng);
   }
@@ -947,6 +937,8 @@ static void launch_bp_ragged_epi(const BpArgs* g, const int64_t* start, int ng, 
     bp_ragged_kernel<EPI, false, CCT_DTYPE_F32><<<grid, BP_THREADS, 0, st>>>(g, start, ng);
   } else if (dt == CCT_DTYPE_BF16) {
     bp_ragged_kernel<EPI, true, CCT_DTYPE_BF16><<<grid, BP_THREADS, 0, st>>>(g, start, ng);
+  } else if (dt == CCT_DTYPE_FIELDS_F32) {
+    bp_ragged_kernel<EPI, true, CCT_DTYPE_FIELDS_F32><<<grid, BP_THREADS, 0, st>>>(g, start, ng);
   } else {
     bp_ragged_kernel<EPI, true, CCT_DTYPE_F32><<<grid, BP_THREADS, 0, st>>>(g, start, ng);
   }
@@ -968,6 +960,8 @@ void launch_bp(const BpArgs& a, cudaStream_t st) {
       bp_adjoint_kernel<false, CCT_DTYPE_F32><<<grid, 256, 0, st>>>(a);
     } else if (a.maps_dtype == CCT_DTYPE_BF16) {
       bp_adjoint_kernel<true, CCT_DTYPE_BF16><<<grid, 256, 0, st>>>(a);
+    } else if (a.maps_dtype == CCT_DTYPE_FIELDS_F32) {
+      bp_adjoint_kernel<true, CCT_DTYPE_FIELDS_F32><<<grid, 256, 0, st>>>(a);
     } else {
       bp_adjoint_kernel<true, CCT_DTYPE_F32><<<grid, 256, 0, st>>>(a);
     }

@@ -96,3 +96,50 @@ def test_channel_pdhg_tv(batch):
         bp = lambda y: port.bp_xrf(y, m, deg32)  # noqa: E731
         ref = port.pdhg_kl_tv(fp, bp, b[idx, 0].double().cpu().numpy(), 10, (N, N), 1e-2)
         assert rel_l2(got[idx], ref) < 1e-4
+
+
+@pytest.fixture(scope="module")
+def fields_core(batch):
+    from pycorrectedemissionct_b200 import core
+
+    cr, maps, x, b, mus, xs, angles = batch
+    cf = core.XrfCore(N, angles, device=maps.device)
+    cf.set_channels(SCALES)
+    mu = torch.from_numpy(np.stack(mus).astype(np.float32)).to(maps.device)
+    fields = core.compute_maps(mu, mu, cf.angles_rad32, maps_dtype="fields-float32")
+    return cf, fields
+
+
+def test_fields_hold_the_line_integrals(batch, fields_core):
+    from pycorrectedemissionct_b200 import core
+
+    cf, fields = fields_core
+    assert tuple(fields.shape) == (SLICES, A, 2, N, N)
+    mu = torch.from_numpy(batch[4][1].astype(np.float32)).to(fields.device)[None]
+    l_in = -torch.log(core.compute_maps(mu, None, cf.angles_rad32).double())[0, :, 0]
+    l_out = -torch.log(core.compute_maps(None, mu, cf.angles_rad32).double())[0, :, 0]
+    assert rel_l2(fields[1, :, 0].double().cpu().numpy(), l_in.cpu().numpy()) < 1e-5
+    assert rel_l2(fields[1, :, 1].double().cpu().numpy(), l_out.cpu().numpy()) < 1e-5
+
+
+def test_fields_projections_equal_channel_maps(batch, fields_core):
+    """fp, symmetric / adjoint bp and MLEM with 2 fields per slice equal those with 8 channel maps."""
+    from pycorrectedemissionct_b200 import engine
+
+    cr, maps, x, b, *_ = batch
+    cf, fields = fields_core
+    assert rel_l2(cf.fp(x, fields).cpu().numpy(), cr.fp(x, maps).cpu().numpy()) < 1e-6
+    y = cr.fp(x, maps)
+    for mode in ("symmetric", "adjoint"):
+        assert rel_l2(cf.bp(y, mode, fields).cpu().numpy(), cr.bp(y, mode, maps).cpu().numpy()) < 1e-6
+    a = engine.BatchedSolver(cr, maps, b, "mlem")
+    f = engine.BatchedSolver(cf, fields, b, "mlem")
+    for _ in range(10):
+        a.step()
+        f.step()
+    assert rel_l2(f.x.cpu().numpy(), a.x.cpu().numpy()) < 1e-5
+    # angle ranges of fields (a view with a slice stride) as for maps
+    sub = cf.angle_range(slice(5, 17))
+    sub_ref = cr.angle_range(slice(5, 17))
+    got = sub.fp(x, fields[:, 5:17], angles=None)
+    assert rel_l2(got.cpu().numpy(), sub_ref.fp(x, maps[:, 5:17]).cpu().numpy()) < 1e-6
