@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define CCT_ABI_VERSION 3
+#define CCT_ABI_VERSION 4
 
 /* Status codes. */
 #define CCT_OK 0
@@ -185,6 +185,14 @@ typedef struct cct_solver_state {
                             is the reference's norm of the whole volume's residual) is compared with
                             tolerance[0] and all slices stop together; its history is row 0 of
                             residual_history.  0: every slice has its own stopping test. */
+  const float* b_mask;      /* [S][D][A][n] data mask (corrct: solvers.py:497-508, 731-736, 788, 1168-1169):
+                               masks the residual (its norm, SIRT's update) and PDHG's dual; NULL = none */
+  const float* b_test_mask; /* [S][D][A][n] cross-validation mask (solvers.py:333-343, 783-785): the test
+                               residual of every iterate is reduced separately by MLEM and SIRT; PDHG
+                               takes NULL; NULL = none */
+  double* partials_test;    /* like partials; required with b_test_mask */
+  double* residuals_test;   /* [S] test residual of the last evaluated iterate */
+  double* history_test;     /* [S][history_len] test residuals (SolutionInfo.residuals_cv), or NULL */
 } cct_solver_state;
 
 /* Number of doubles the `partials` workspace must hold. */

@@ -376,33 +376,48 @@ def divergence(q: NDArray) -> NDArray:
     return np.sum(np.stack(d, axis=0), axis=0)
 
 
-def diagonal_scaling(fp, bp, b: NDArray, x_shape, reg_tau: float = 0.0, relax_tau: float = 1.0, relax_sigma: float = 1.0):
+def diagonal_scaling(fp, bp, b: NDArray, x_shape, reg_tau: float = 0.0, relax_tau: float = 1.0, relax_sigma: float = 1.0, b_mask=None, x_mask=None):
     """``compute_diagonal_scaling`` (``solvers.py:60-117``) for one TV regularizer contribution ``reg_tau``."""
-    tau = np.abs(bp(np.ones_like(b)))
+    b_ones = np.ones_like(b) if b_mask is None else np.ones_like(b) * b_mask
+    tau = np.abs(bp(b_ones))
     tau = tau + reg_tau
     tau[(tau / np.max(tau)) < 1e-5] = 1
     tau = relax_tau / tau
-    sigma = np.abs(fp(np.ones(x_shape, dtype=tau.dtype)))
+    x_ones = np.ones(x_shape, dtype=tau.dtype) if x_mask is None else np.ones(x_shape, dtype=tau.dtype) * x_mask
+    sigma = np.abs(fp(x_ones))
     sigma[(sigma / np.max(sigma)) < 1e-5] = 1.0
     sigma = relax_sigma / sigma
     return sigma, tau
 
 
-def mlem(fp, bp, b: NDArray, iterations: int, x0=None, tolerance=None, lower_limit=None, upper_limit=None, x_mask=None):
+def b_masks(b: NDArray, b_mask, b_test_mask):
+    """``Solver._initialize_b_masks`` (``solvers.py:333-343``)."""
+    if b_test_mask is not None:
+        if b_mask is None:
+            b_mask = np.ones_like(b)
+        b_mask, b_test_mask = b_mask * (1 - b_test_mask), b_test_mask * b_mask
+    return b_mask, b_test_mask
+
+
+def mlem(fp, bp, b: NDArray, iterations: int, x0=None, tolerance=None, lower_limit=None, upper_limit=None, x_mask=None,
+         b_mask=None, b_test_mask=None, residuals_cv=None):
     """MLEM update loop of ``solvers.py:725-805`` (KL data term, no background).
 
-    Returns (x, residuals list).
+    Returns (x, residuals list); the test-mask residuals go to the list ``residuals_cv``.
     """
     b = np.array(b)
-    tau = bp(np.ones_like(b))
+    b_mask, b_test_mask = b_masks(b, b_mask, b_test_mask)
+    tau = bp(np.ones_like(b) if b_mask is None else np.ones_like(b) * b_mask)
     x = np.ones_like(tau) if x0 is None else np.array(x0).copy()
     if x_mask is not None:
         x *= x_mask
     residuals = []
     for _ in range(iterations):
         ax = fp(x)
+        if b_test_mask is not None and residuals_cv is not None:
+            residuals_cv.append(kl_residual_norm(kl_residual(ax, b, mask=b_test_mask)))
         if tolerance is not None:
-            r = kl_residual_norm(kl_residual(ax, b))
+            r = kl_residual_norm(kl_residual(ax, b, mask=b_mask))
             residuals.append(r)
             if tolerance > r:
                 break
@@ -416,12 +431,20 @@ def mlem(fp, bp, b: NDArray, iterations: int, x0=None, tolerance=None, lower_lim
     return x, residuals
 
 
-def sirt(fp, bp, b: NDArray, iterations: int, x_shape, relaxation: float = 1.95, x0=None, lower_limit=None, upper_limit=None, x_mask=None):
-    """SIRT update loop of ``solvers.py:895-984`` (l2 data term, no regularizer)."""
-    sigma, tau = diagonal_scaling(fp, bp, b, x_shape, relax_tau=relaxation)
+def sirt(fp, bp, b: NDArray, iterations: int, x_shape, relaxation: float = 1.95, x0=None, lower_limit=None, upper_limit=None, x_mask=None,
+         b_mask=None, b_test_mask=None, residuals_cv=None):
+    """SIRT update loop of ``solvers.py:895-984`` (l2 data term, no regularizer).
+
+    The test-mask residuals (squared l2 norms) go to the list ``residuals_cv``.
+    """
+    b_mask, b_test_mask = b_masks(b, b_mask, b_test_mask)
+    sigma, tau = diagonal_scaling(fp, bp, b, x_shape, relax_tau=relaxation, b_mask=b_mask, x_mask=x_mask)
     x = np.zeros_like(tau) if x0 is None else np.array(x0).copy()
     for _ in range(iterations):
-        res = l2_residual(fp(x), b)
+        ax = fp(x)
+        if b_test_mask is not None and residuals_cv is not None:
+            residuals_cv.append(float(np.sum(l2_residual(ax, b, mask=b_test_mask) ** 2)))
+        res = l2_residual(ax, b, mask=b_mask)
         x += bp(res * sigma) * tau
         if lower_limit is not None or upper_limit is not None:
             x = x.clip(lower_limit, upper_limit)
@@ -430,23 +453,30 @@ def sirt(fp, bp, b: NDArray, iterations: int, x_shape, relaxation: float = 1.95,
     return x
 
 
-def pdhg_kl_tv(fp, bp, b: NDArray, iterations: int, x_shape, lam: float, relaxation: float = 0.95, lower_limit=None, upper_limit=None, x_mask=None):
+def pdhg_kl_tv(fp, bp, b: NDArray, iterations: int, x_shape, lam: float, relaxation: float = 0.95, lower_limit=None, upper_limit=None, x_mask=None,
+               x0=None, b_mask=None, b_test_mask=None, tolerance=None, residuals=None, residuals_cv=None):
     """PDHG with KL data term and isotropic TV2D (``solvers.py:1099-1206``).
 
     Dual KL prox ``data_terms.py:682-692``; TV via ``Regularizer_Grad``
     (``regularizers.py:260-273``, sigma = 0.5, tau contribution 2*ndims = 4) with
-    the l12 dual prox (``data_terms.py:549-555, 607-608``).
+    the l12 dual prox (``data_terms.py:549-555, 607-608``).  With a tolerance or a test mask
+    the KL residuals (with the dual scaling sigma) of every iterate go to the lists
+    ``residuals`` / ``residuals_cv``.
     """
     b = np.array(b)
-    sigma, tau = diagonal_scaling(fp, bp, b, x_shape, reg_tau=4.0, relax_tau=relaxation, relax_sigma=relaxation)
-    x = np.zeros(x_shape, dtype=tau.dtype)
+    b_mask, b_test_mask = b_masks(b, b_mask, b_test_mask)
+    sigma, tau = diagonal_scaling(fp, bp, b, x_shape, reg_tau=4.0, relax_tau=relaxation, relax_sigma=relaxation, x_mask=x_mask, b_mask=b_mask)
+    x = np.zeros(x_shape, dtype=tau.dtype) if x0 is None else np.array(x0).copy()
     x_relax = x.copy()
     sigma_data = 4 * sigma * np.fmax(b, 0.0)
     p = np.zeros_like(b)
     q = np.zeros((2, *x_shape), dtype=tau.dtype)
+    track = tolerance is not None or b_test_mask is not None
     for _ in range(iterations):
         p += fp(x_relax) * sigma
         p[:] = (1 + p - np.sqrt((p - 1) ** 2 + sigma_data)) / 2
+        if b_mask is not None:
+            p *= b_mask
         q += 0.5 * gradient(x_relax)
         qn = np.linalg.norm(q, ord=2, axis=0, keepdims=True)
         q /= np.fmax(qn, lam)
@@ -459,6 +489,51 @@ def pdhg_kl_tv(fp, bp, b: NDArray, iterations: int, x_shape, lam: float, relaxat
             x_new *= x_mask
         x_relax = x_new + (x_new - x)
         x = x_new
+        if track:
+            ax = fp(x)
+            r = kl_residual_norm(kl_residual(ax, b, sigma, mask=b_mask))
+            if residuals is not None:
+                residuals.append(r)
+            if b_test_mask is not None and residuals_cv is not None:
+                residuals_cv.append(kl_residual_norm(kl_residual(ax, b, sigma, mask=b_test_mask)))
+            if tolerance is not None and tolerance > r:
+                break
+    return x
+
+
+def fista(fp, bp, b: NDArray, iterations: int, x_shape, relaxation: float = 1.0, x0=None, lower_limit=None, upper_limit=None,
+          x_mask=None, b_mask=None, b_test_mask=None, tolerance=None, restart_period=None, residuals=None, residuals_cv=None):
+    """FISTA, l2 data term, diagonal preconditioning, no regularizer (``solvers.py:1395-1513``)."""
+    b = np.array(b)
+    b_mask, b_test_mask = b_masks(b, b_mask, b_test_mask)
+    sigma, tau = diagonal_scaling(fp, bp, b, x_shape, relax_tau=relaxation, x_mask=x_mask, b_mask=b_mask)
+    x = np.zeros(x_shape, dtype=tau.dtype) if x0 is None else np.array(x0).copy()
+    if x_mask is not None:
+        x *= x_mask
+    y = x.copy()
+    t = 1.0
+    track = tolerance is not None or b_test_mask is not None
+    for ii in range(iterations):
+        grad = bp(l2_residual(fp(y), b, mask=b_mask) * sigma)
+        x_new = y + tau * grad
+        if lower_limit is not None or upper_limit is not None:
+            x_new = x_new.clip(lower_limit, upper_limit)
+        if x_mask is not None:
+            x_new *= x_mask
+        t_new = float(1.0 + np.sqrt(1.0 + 4.0 * t * t)) / 2.0
+        if restart_period is not None and (ii + 1) % restart_period == 0:
+            t_new = 1.0
+        y = x_new + (t - 1.0) / t_new * (x_new - x)
+        x, t = x_new, t_new
+        if track:
+            ax = fp(x)
+            r = float(np.sum(l2_residual(ax, b, mask=b_mask) ** 2))
+            if residuals is not None:
+                residuals.append(r)
+            if b_test_mask is not None and residuals_cv is not None:
+                residuals_cv.append(float(np.sum(l2_residual(ax, b, mask=b_test_mask) ** 2)))
+            if tolerance is not None and tolerance > r:
+                break
     return x
 
 

@@ -13,7 +13,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcorrct_b200.so")
 
-ABI_VERSION = 3  # CCT_ABI_VERSION of include/corrct_b200.h
+ABI_VERSION = 4  # CCT_ABI_VERSION of include/corrct_b200.h
 
 CCT_OK = 0
 CCT_ERR_VALUE = 1
@@ -125,6 +125,11 @@ class SolverState(ctypes.Structure):
         ("history_len", ctypes.c_int32),
         ("x_mask_per_slice", ctypes.c_int32),
         ("joint_stop", ctypes.c_int32),
+        ("b_mask", ctypes.c_void_p),
+        ("b_test_mask", ctypes.c_void_p),
+        ("partials_test", ctypes.c_void_p),
+        ("residuals_test", ctypes.c_void_p),
+        ("history_test", ctypes.c_void_p),
     ]
 
 

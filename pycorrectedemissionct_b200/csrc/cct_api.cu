@@ -16,6 +16,9 @@ void launch_residual_step(const double* partials, int64_t per_slice, int n_slice
                           cudaStream_t st);
 void launch_tv_dual(const float* x_relax, float* q, int n, int n_slices, float lam, const int* active,
                     cudaStream_t st);
+void launch_residual_test(const double* partials, int64_t per_slice, int n_slices, double* residuals,
+                          const int* active, const int* iterations, double* history, int history_len,
+                          cudaStream_t st);
 void launch_norm(const float* v, int64_t count, int n_slices, int ord, double* out, double* partials,
                  cudaStream_t st);
 }  // namespace cct
@@ -177,6 +180,8 @@ static int validate_state(const cct_xrf_desc* d, const cct_solver_state* st) {
   CCT_REQUIRE(st->x && st->b && st->tau && st->sino_buf && st->partials && st->residuals && st->active &&
                   st->iterations,
               "solver state is missing a required buffer");
+  CCT_REQUIRE(st->b_test_mask == nullptr || (st->partials_test != nullptr && st->residuals_test != nullptr),
+              "b_test_mask needs partials_test and residuals_test");
   (void)d;
   return CCT_OK;
 }
@@ -202,6 +207,8 @@ int cct_mlem_fp(const cct_xrf_desc* desc, const void* maps, cct_solver_state* st
   cct::FpArgs f = make_fp_args(desc, st->x, maps, st->sino_buf);
   f.epi = cct::FP_EPI_MLEM; f.b = st->b; f.background = st->background; f.has_background = st->has_background;
   f.partials = st->partials; f.active = st->active;
+  f.b_mask = st->b_mask; f.b_test_mask = st->b_test_mask;
+  f.partials_test = st->b_test_mask != nullptr ? st->partials_test : nullptr;
   int64_t per_slice = 0;
   if (desc->psf == nullptr) {
     cct::launch_fp(f, s);
@@ -216,6 +223,9 @@ int cct_mlem_fp(const cct_xrf_desc* desc, const void* maps, cct_solver_state* st
     cct::launch_psf(f, desc->psf, desc->psf_len, s);
     per_slice = (int64_t)desc->n_det * desc->n_angles;
   }
+  if (st->b_test_mask != nullptr)
+    cct::launch_residual_test(st->partials_test, per_slice, desc->n_slices, st->residuals_test, st->active,
+                              st->iterations, st->history_test, st->history_len, s);
   cct::launch_residual_step(st->partials, per_slice, desc->n_slices, st->residuals, st->active, st->iterations,
                             st->tolerance, st->residual_history, st->history_len, st->joint_stop, s);
   return check_launch();
@@ -250,6 +260,8 @@ int cct_sirt_step(const cct_xrf_desc* desc, const void* maps, int32_t bp_mode, c
   cct::FpArgs f = make_fp_args(desc, st->x, maps, st->sino_buf);
   f.epi = cct::FP_EPI_SIRT; f.b = st->b; f.sigma = st->sigma; f.background = st->background;
   f.has_background = st->has_background; f.partials = st->partials; f.active = st->active;
+  f.b_mask = st->b_mask; f.b_test_mask = st->b_test_mask;
+  f.partials_test = st->b_test_mask != nullptr ? st->partials_test : nullptr;
   int64_t per_slice = 0;
   if (desc->psf == nullptr) {
     cct::launch_fp(f, s);
@@ -263,6 +275,9 @@ int cct_sirt_step(const cct_xrf_desc* desc, const void* maps, int32_t bp_mode, c
     cct::launch_psf(f, desc->psf, desc->psf_len, s);
     per_slice = (int64_t)desc->n_det * desc->n_angles;
   }
+  if (st->b_test_mask != nullptr)
+    cct::launch_residual_test(st->partials_test, per_slice, desc->n_slices, st->residuals_test, st->active,
+                              st->iterations, st->history_test, st->history_len, s);
   cct::launch_residual_step(st->partials, per_slice, desc->n_slices, st->residuals, st->active, st->iterations,
                             st->tolerance, st->residual_history, st->history_len, st->joint_stop, s);
   cct::BpArgs b = make_solver_bp(desc, bp_mode, maps, st, cct::BP_EPI_SIRT);
@@ -280,10 +295,11 @@ int cct_pdhg_step(const cct_xrf_desc* desc, const void* maps, int32_t bp_mode, c
   CCT_REQUIRE(st->vol_buf != nullptr, "PDHG needs vol_buf");
   CCT_REQUIRE(bp_mode == CCT_BP_REFERENCE || bp_mode == CCT_BP_SYMMETRIC, "PDHG bp_mode must be REFERENCE or SYMMETRIC");
   CCT_REQUIRE(bp_mode != CCT_BP_SYMMETRIC || maps != nullptr, "the symmetric back projection needs maps");
+  CCT_REQUIRE(st->b_test_mask == nullptr, "the PDHG step keeps no test residual (b_test_mask must be NULL)");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   cct::FpArgs f = make_fp_args(desc, st->x_relax, maps, st->sino_buf);
   f.epi = cct::FP_EPI_PDHG; f.b = st->b; f.sigma = st->sigma; f.background = st->background;
-  f.has_background = st->has_background; f.active = st->active;
+  f.has_background = st->has_background; f.active = st->active; f.b_mask = st->b_mask;
   if (desc->psf == nullptr) {
     cct::launch_fp(f, s);
   } else {
@@ -382,8 +398,9 @@ int cct_ragged_plan_create(int32_t method, int32_t bp_mode, int32_t n_groups, co
     const cct_solver_state* st = states + g;
     if ((rc = validate_desc(d)) != CCT_OK) return fail(rc);
     if ((rc = validate_state(d, st)) != CCT_OK) return fail(rc);
-    if (d->psf != nullptr || st->joint_stop || d->maps_dtype != p->maps_dtype || (maps[g] != nullptr) != p->has_maps) {
-      cct_set_last_error("ragged groups need one maps type, no PSF and per-slice stopping");
+    if (d->psf != nullptr || st->joint_stop || st->b_test_mask != nullptr || d->maps_dtype != p->maps_dtype ||
+        (maps[g] != nullptr) != p->has_maps) {
+      cct_set_last_error("ragged groups need one maps type, no PSF, no test mask and per-slice stopping");
       return fail(CCT_ERR_UNSUPPORTED);
     }
     if (maps[g] == nullptr && d->n_det != 1) {
@@ -402,6 +419,7 @@ int cct_ragged_plan_create(int32_t method, int32_t bp_mode, int32_t n_groups, co
     f.epi = method == CCT_METHOD_SIRT ? cct::FP_EPI_SIRT : cct::FP_EPI_MLEM;
     f.b = st->b; f.sigma = st->sigma; f.background = st->background; f.has_background = st->has_background;
     f.partials = st->partials; f.active = st->active;
+    f.b_mask = st->b_mask;
     f.vec4 = cct::fp_vec4_ok(f) ? 1 : 0;
     fp[g] = f;
     bp[g] = make_solver_bp(d, method == CCT_METHOD_SIRT ? bp_mode : CCT_BP_REFERENCE,

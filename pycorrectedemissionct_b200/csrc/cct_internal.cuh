@@ -33,6 +33,9 @@ struct FpArgs {
   int has_background;
   double* partials;    // per-CTA residual partial sums (MLEM, SIRT)
   const int* active;
+  const float* b_mask;       // data mask of the residual, or nullptr
+  const float* b_test_mask;  // cross-validation mask, or nullptr
+  double* partials_test;     // per-CTA test residual partials (with b_test_mask)
 };
 
 struct BpArgs {
@@ -61,35 +64,47 @@ struct BpArgs {
 };
 
 // Fused forward-projection epilogue for one final value `ax` = (A x)[idx].
-// Returns this element's contribution to the slice residual (FP64).
+// Returns this element's contribution to the slice residual (FP64) and adds its contribution
+// to the cross-validation residual to *test (with b_test_mask).
 template <int EPI>
-__device__ __forceinline__ double fp_epilogue(const FpArgs& a, int64_t idx, float ax) {
+__device__ __forceinline__ double fp_epilogue(const FpArgs& a, int64_t idx, float ax, double* test) {
   if (EPI == FP_EPI_STORE) {
     a.out[idx] = ax;
     return 0.0;
   } else if (EPI == FP_EPI_MLEM) {
-    // corrct solvers.py:787-796 and data_terms.py:720-742 (KL, sigma = 1)
+    // corrct solvers.py:787-796 and data_terms.py:720-742 (KL, sigma = 1); the masks scale the
+    // residual only, the MLEM ratio is unmasked (solvers.py:797)
     const float bb = a.b[idx];
     const float proj = a.has_background ? ax + a.background : ax;
     const float clipped = fmaxf(proj, EPS32);
     a.out[idx] = bb / clipped;
     const double r = (double)clipped;
     const double sd = 4.0 * fmax((double)bb, 0.0);
-    const double res = (1.0 + r - sqrt((r - 1.0) * (r - 1.0) + sd)) * 0.5;
-    return fabs(res);
+    const double res = fabs((1.0 + r - sqrt((r - 1.0) * (r - 1.0) + sd)) * 0.5);
+    if (a.b_test_mask != nullptr) *test += res * (double)fabsf(a.b_test_mask[idx]);
+    return a.b_mask != nullptr ? res * (double)fabsf(a.b_mask[idx]) : res;
   } else if (EPI == FP_EPI_SIRT) {
-    // corrct data_terms.py:136-161 (l2 residual), solvers.py:954-977
+    // corrct data_terms.py:136-161 (l2 residual), solvers.py:954-977; the masked residual drives
+    // the update
     const float proj = a.has_background ? ax + a.background : ax;
-    const float res = a.b[idx] - proj;
+    const float raw = a.b[idx] - proj;
+    const float res = a.b_mask != nullptr ? raw * a.b_mask[idx] : raw;
     a.out[idx] = res * a.sigma[idx];
+    if (a.b_test_mask != nullptr) {
+      const double t = (double)(raw * a.b_test_mask[idx]);
+      *test += t * t;
+    }
     return (double)res * (double)res;
   } else {
-    // PDHG dual update + KL prox (corrct data_terms.py:262-276, 682-692)
+    // PDHG dual update + KL prox (corrct data_terms.py:262-276, 682-692), then p *= b_mask
+    // (solvers.py:1168-1169)
     const float proj = a.has_background ? ax + a.background : ax;
     const double sg = (double)a.sigma[idx];
     const double p = (double)a.out[idx] + (double)proj * sg;
     const double sd = 4.0 * sg * fmax((double)a.b[idx], 0.0);
-    a.out[idx] = (float)((1.0 + p - sqrt((p - 1.0) * (p - 1.0) + sd)) * 0.5);
+    float pn = (float)((1.0 + p - sqrt((p - 1.0) * (p - 1.0) + sd)) * 0.5);
+    if (a.b_mask != nullptr) pn *= a.b_mask[idx];
+    a.out[idx] = pn;
     return 0.0;
   }
 }

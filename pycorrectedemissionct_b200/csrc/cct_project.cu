@@ -100,6 +100,22 @@ __device__ __forceinline__ void chunk_box(float m00, float m01, float m02, float
   by1 = (int)floorf(ymax) + 2;
 }
 
+// CTA sum of one residual partial per thread (FP64, fixed order) into partials[slot]; red
+// holds one double per warp.  Every thread of the CTA calls it.
+__device__ __forceinline__ void fp_write_partial(double v, double* partials, int64_t slot, double* red, int lane,
+                                                 int warp, int tid) {
+  v = warp_sum_double(v);
+  __syncthreads();  // red may still be read by a previous call
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < FP_TC / FP_LC; ++w) t += red[w];
+    partials[slot] = t;
+  }
+}
+
 // One CTA of the forward projection: detector band `band` of (angle, detector) `ad` of slice
 // `s`; `n_bands` and `n_ad` are the batch's band and (angle, detector) counts (the residual
 // partials are indexed by them).
@@ -236,25 +252,18 @@ __device__ __forceinline__ void fp_cta(const FpArgs& args, const int band, const
   // column sum over the 4 row-lanes of the 8x4 lane block (lanes lc, lc+8, lc+16, lc+24)
   acc += __shfl_xor_sync(0xffffffffu, acc, 8);
   acc += __shfl_xor_sync(0xffffffffu, acc, 16);
-  double part = 0.0;
+  double part = 0.0, ptest = 0.0;
   if (lr == 0 && c <= c_last) {
     float total = acc;
     if (args.weights != nullptr) total *= args.weights[a * args.n_det + d];
     const int64_t idx = (((int64_t)s * args.n_det + d) * args.n_angles + a) * n + c;
-    part = fp_epilogue<EPI>(args, idx, total);
+    part = fp_epilogue<EPI>(args, idx, total, &ptest);
   }
   // only the MLEM and SIRT epilogues produce residual partials (PDHG passes none)
   if (EPI == FP_EPI_MLEM || EPI == FP_EPI_SIRT) {
-    part = warp_sum_double(part);
-    if (lane == 0) red_d[warp] = part;
-    __syncthreads();
-    if (tid == 0) {
-      double t = 0.0;
-#pragma unroll
-      for (int w = 0; w < FP_TC / FP_LC; ++w) t += red_d[w];
-      const int64_t per_slice = (int64_t)n_bands * n_ad;
-      args.partials[(int64_t)s * per_slice + (int64_t)ad * n_bands + band] = t;
-    }
+    const int64_t slot = (int64_t)s * n_bands * n_ad + (int64_t)ad * n_bands + band;
+    fp_write_partial(part, args.partials, slot, red_d, lane, warp, tid);
+    if (args.partials_test != nullptr) fp_write_partial(ptest, args.partials_test, slot, red_d, lane, warp, tid);
   }
 }
 
@@ -480,24 +489,17 @@ __global__ void __launch_bounds__(FP_THREADS, 2)
 
   acc += __shfl_xor_sync(0xffffffffu, acc, 8);
   acc += __shfl_xor_sync(0xffffffffu, acc, 16);
-  double part = 0.0;
+  double part = 0.0, ptest = 0.0;
   if (lr == 0 && c <= c_last) {
     float total = acc;
     if (args.weights != nullptr) total *= args.weights[a * args.n_det + d];
     const int64_t idx = (((int64_t)s * args.n_det + d) * args.n_angles + a) * n + c;
-    part = fp_epilogue<EPI>(args, idx, total);
+    part = fp_epilogue<EPI>(args, idx, total, &ptest);
   }
   if (EPI == FP_EPI_MLEM || EPI == FP_EPI_SIRT) {
-    part = warp_sum_double(part);
-    if (lane == 0) red_d[warp] = part;
-    __syncthreads();
-    if (tid == 0) {
-      double t = 0.0;
-#pragma unroll
-      for (int w = 0; w < FP_TC / FP_LC; ++w) t += red_d[w];
-      const int64_t per_slice = (int64_t)gridDim.x * gridDim.y;
-      args.partials[(int64_t)s * per_slice + (int64_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
-    }
+    const int64_t slot = (int64_t)s * gridDim.x * gridDim.y + (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+    fp_write_partial(part, args.partials, slot, red_d, lane, warp, tid);
+    if (args.partials_test != nullptr) fp_write_partial(ptest, args.partials_test, slot, red_d, lane, warp, tid);
   }
 }
 
@@ -748,7 +750,7 @@ __global__ void __launch_bounds__(PSF_THREADS) psf_kernel(FpArgs args, const flo
   for (int i = threadIdx.x; i < n; i += PSF_THREADS) line_sh[i] = in[i];
   __syncthreads();
   const int p = (len - 1) / 2;
-  double part = 0.0;
+  double part = 0.0, ptest = 0.0;
   for (int i = threadIdx.x; i < n; i += PSF_THREADS) {
     float acc = 0.f;
     for (int j = 0; j < len; ++j) {
@@ -756,17 +758,22 @@ __global__ void __launch_bounds__(PSF_THREADS) psf_kernel(FpArgs args, const flo
       q = q < 0 ? 0 : (q >= n ? n - 1 : q);
       acc = fmaf(line_sh[q], __ldg(k + j), acc);
     }
-    part += fp_epilogue<EPI>(args, line * n + i, acc);
+    part += fp_epilogue<EPI>(args, line * n + i, acc, &ptest);
   }
   if (EPI == FP_EPI_MLEM || EPI == FP_EPI_SIRT) {
-    part = warp_sum_double(part);
-    if ((threadIdx.x & 31) == 0) red_d[threadIdx.x >> 5] = part;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int w = 0; w < PSF_THREADS / 32; ++w) t += red_d[w];
-      // one partial per (detector, angle) line of the slice
-      args.partials[line] = t;
+    // one partial per (detector, angle) line of the slice
+    for (int which = 0; which < 2; ++which) {
+      double* dst = which == 0 ? args.partials : args.partials_test;
+      if (dst == nullptr) continue;  // uniform across the CTA
+      double v = warp_sum_double(which == 0 ? part : ptest);
+      __syncthreads();
+      if ((threadIdx.x & 31) == 0) red_d[threadIdx.x >> 5] = v;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < PSF_THREADS / 32; ++w) t += red_d[w];
+        dst[line] = t;
+      }
     }
   }
 }

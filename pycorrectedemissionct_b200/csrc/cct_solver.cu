@@ -91,6 +91,33 @@ __global__ void __launch_bounds__(RED_THREADS) norm_final_kernel(const double* p
   if (threadIdx.x == 0) out[s] = acc;
 }
 
+// Cross-validation residual of the iterate just projected (corrct solvers.py:783-785): the sum
+// of the slice's test partials; recorded at the iteration index before residual_step_kernel
+// counts the iteration.  No stopping test.
+__global__ void __launch_bounds__(RED_THREADS) residual_test_kernel(const double* partials, int64_t per_slice,
+                                                                    double* residuals, const int* active,
+                                                                    const int* iterations, double* history,
+                                                                    int history_len) {
+  const int s = blockIdx.x;
+  if (active[s] == 0) return;
+  double v = 0.0;
+  const double* p = partials + (int64_t)s * per_slice;
+  for (int64_t k = threadIdx.x; k < per_slice; k += RED_THREADS) v += p[k];
+  v = block_sum_double(v);
+  if (threadIdx.x == 0) {
+    residuals[s] = v;
+    const int it = iterations[s];
+    if (history != nullptr && it < history_len) history[(int64_t)s * history_len + it] = v;
+  }
+}
+
+void launch_residual_test(const double* partials, int64_t per_slice, int n_slices, double* residuals,
+                          const int* active, const int* iterations, double* history, int history_len,
+                          cudaStream_t st) {
+  residual_test_kernel<<<n_slices, RED_THREADS, 0, st>>>(partials, per_slice, residuals, active, iterations, history,
+                                                          history_len);
+}
+
 // A 3-D volume solved as a stack of slices: the reference computes one residual norm over the
 // whole volume, which for its additive norms (sum |r|, sum r^2) is the sum of the slice residuals.
 // Runs after residual_step_kernel of the same iteration; one CTA, fixed summation order.

@@ -39,6 +39,11 @@ class BatchedSolver:
     tolerance : (S,) array, float, or None
         Stop a slice when ``tolerance > residual`` (the reference's rule).
     x_mask : (n, n) or (S, n, n) tensor or None
+    b_mask, b_test_mask : (S, D, A, n) tensors (or broadcastable) or None
+        Data mask (masks the residual and its norm, SIRT's update, PDHG's dual and the scaling
+        tau) and cross-validation mask (MLEM / SIRT: its residual per iterate goes to
+        ``residuals_test`` / ``history_test``), as the reference's ``b_mask`` / ``b_test_mask``
+        after ``_initialize_b_masks``.
     x_shared : (S, n, n) tensor or None
         MLEM only: use this tensor as the iterate, in place and without initialising it.
     joint_stop : bool
@@ -65,6 +70,8 @@ class BatchedSolver:
         history_len: int = 0,
         joint_stop: bool = False,
         x_shared: torch.Tensor | None = None,
+        b_mask: torch.Tensor | None = None,
+        b_test_mask: torch.Tensor | None = None,
     ):
         self.core = core
         self.device = core.device
@@ -86,13 +93,22 @@ class BatchedSolver:
         self.b = b.contiguous()
         dev = self.device
         f32 = dict(dtype=torch.float32, device=dev)
+        if self.method == "pdhg" and b_test_mask is not None:
+            raise NotImplementedError("the PDHG step keeps no test residual: evaluate A x apart")
+        self.b_mask = None if b_mask is None else b_mask.to(**f32).expand(expect).contiguous()
+        self.b_test_mask = None if b_test_mask is None else b_test_mask.to(**f32).expand(expect).contiguous()
 
         bp_maps = maps if bp_mode == "symmetric" else None
         if self.method == "mlem":
             # tau = A^T 1 (solvers.py:734-737); the default XRF bp ignores maps, so tau is shared
-            ones = torch.ones((1, core.n_det, core.n_angles, n), **f32)
-            self.tau = core.bp(ones, "reference")[0].contiguous()
-            self.tau_shared = 1
+            if self.b_mask is None:
+                ones = torch.ones((1, core.n_det, core.n_angles, n), **f32)
+                self.tau = core.bp(ones, "reference")[0].contiguous()
+                self.tau_shared = 1
+            else:
+                # tau = A^T b_mask per slice (solvers.py:734-737)
+                self.tau = core.bp(self.b_mask, "reference").contiguous()
+                self.tau_shared = 0
             self.sigma = None
             if x_shared is not None:
                 # iterate owned by the caller (ordered subsets share one x between subset solvers)
@@ -106,7 +122,7 @@ class BatchedSolver:
         else:
             relax = relaxation if relaxation is not None else (1.95 if self.method == "sirt" else 0.95)
             reg_tau = 4.0 if self.method == "pdhg" else 0.0
-            ones_b = torch.ones_like(self.b)
+            ones_b = torch.ones_like(self.b) if self.b_mask is None else self.b_mask.clone()
             tau = core.bp(ones_b, bp_mode, bp_maps).abs_()
             tau += reg_tau
             # the reference scales by the maximum over its whole volume: per slice for independent
@@ -171,6 +187,17 @@ class BatchedSolver:
         st.residual_history = None if self.history is None else self.history.data_ptr()
         st.history_len = int(history_len)
         st.x_mask_per_slice = int(self.x_mask is not None and self.x_mask.dim() == 3)
+        st.b_mask = None if self.b_mask is None else self.b_mask.data_ptr()
+        self.residuals_test = self.history_test = self.partials_test = None
+        if self.b_test_mask is not None:
+            st.b_test_mask = self.b_test_mask.data_ptr()
+            self.partials_test = torch.zeros_like(self.partials)
+            self.residuals_test = torch.zeros(s, dtype=torch.float64, device=dev)
+            st.partials_test = self.partials_test.data_ptr()
+            st.residuals_test = self.residuals_test.data_ptr()
+            if history_len > 0:
+                self.history_test = torch.zeros((s, history_len), dtype=torch.float64, device=dev)
+                st.history_test = self.history_test.data_ptr()
         st.joint_stop = int(joint_stop)
         self.joint_stop = bool(joint_stop)
         self.state = st
@@ -227,6 +254,10 @@ class BatchedSolver:
         self.residuals.zero_()
         if self.history is not None:
             self.history.zero_()
+        if self.residuals_test is not None:
+            self.residuals_test.zero_()
+        if self.history_test is not None:
+            self.history_test.zero_()
 
     def capture(self, steps: int) -> None:
         """Capture `steps` iterations into a CUDA graph.  Call after at least one eager

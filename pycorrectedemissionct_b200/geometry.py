@@ -103,6 +103,9 @@ def attenuation_rotations(
     distances = np.ones(n_det) if distances_mm is None else np.array(distances_mm, ndmin=1, dtype=np.float64)
     subs = [detector_sub_angles(surfaces[d], distances[d], sub_sampling) for d in range(n_det)]
     n_sub = max(len(s) for s in subs)
+    # a point detector next to finite ones has one direction: repeating it keeps one sub-angle
+    # count for the kernels (the mean of identical factors is the factor, up to rounding)
+    subs = [np.resize(sa, n_sub) if len(sa) == 1 else sa for sa in subs]
     if any(len(s) != n_sub for s in subs):
         raise ValueError("All detectors must use the same number of emitted sub-angles")
     angles = np.array(angles_rot_rad32, ndmin=1)

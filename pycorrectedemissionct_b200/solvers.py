@@ -116,7 +116,10 @@ class Solver:
         self.tolerance = tolerance
         self.data_term, self.background = _data_term_name(data_term)
         if data_term_test is not None:
-            raise NotImplementedError("data_term_test (cross-validation residuals) is not supported by the B200 solvers")
+            name, bg = _data_term_name(data_term_test)
+            if name != self.data_term:
+                raise NotImplementedError("the cross-validation data term must be of the solver's data term type")
+            # the reference gives the test term the solver's background (solvers.py:762-765)
 
     def info(self) -> str:
         return type(self).__name__
@@ -128,9 +131,36 @@ class Solver:
         return type(self).__name__.lower()
 
     @staticmethod
-    def _reject_masks(b_mask, b_test_mask) -> None:
-        if b_mask is not None or b_test_mask is not None:
-            raise NotImplementedError("b_mask / b_test_mask are not supported by the B200 solvers yet")
+    def _masks(A, b_mask, b_test_mask):
+        """Device (S, D, A, n) masks after ``_initialize_b_masks`` (solvers.py:333-343)."""
+        if b_test_mask is not None and b_mask is None:
+            b_mask = np.ones(1, dtype=np.float32)
+        if b_mask is None:
+            return None, None
+        dev = A.projector_backend.device
+        n = int(A.vol_shape[-1])
+        z = A.projector_backend.n_slices
+        n_det = A._n_det() if isinstance(A, ProjectorAttenuationXRF) else 1
+        shape = (n_det, z, len(A.angles_rot_rad), n)
+
+        def dev_mask(m):
+            t = _tensor(m, dev)
+            t = t.expand(shape) if t.numel() == 1 else t.reshape(shape)
+            return t.permute(1, 0, 2, 3).contiguous()
+
+        bm = dev_mask(b_mask)
+        if b_test_mask is None:
+            return bm, None
+        bt = dev_mask(b_test_mask)
+        return bm * (1 - bt), bt * bm
+
+    @staticmethod
+    def _cv_info(solver: BatchedSolver, info, iterations: int, volume: bool) -> None:
+        if solver.history_test is None:
+            return
+        h = solver.history_test.sum(dim=0) if volume else solver.history_test[0]
+        k = min(info.iterations, iterations)
+        info.residuals_cv[:k] = h.cpu().numpy()[:k]
 
 
 class MLEM(Solver):
@@ -143,20 +173,26 @@ class MLEM(Solver):
 
     def __call__(self, A, b, iterations: int, x0=None, lower_limit=None, upper_limit=None, x_mask=None, b_mask=None, b_test_mask=None):
         _check_projector(A)
-        self._reject_masks(b_mask, b_test_mask)
         if getattr(A, "is_symmetric", False) or getattr(A, "bp_mode", "reference") != "reference":
             raise NotImplementedError("the fused MLEM uses the reference (non-symmetric) back projection")
         bt, x0t, mt, maps, as_np = _as_batch(A, b, x0, x_mask)
+        bm, btm = self._masks(A, b_mask, b_test_mask)
         solver = BatchedSolver(
             A.core, maps, bt, "mlem", tolerance=self.tolerance, x0=x0t, x_mask=mt,
             lower_limit=lower_limit, upper_limit=upper_limit, background=self.background, history_len=iterations,
-            joint_stop=_is_volume(A),
+            joint_stop=_is_volume(A), b_mask=bm, b_test_mask=btm,
         )
         info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
-        if self.tolerance is not None:
-            info.residual0 = _kl_residual_norm(A.core.fp(solver.x, maps), bt, self.background)
+        if self.tolerance is not None or btm is not None:
+            ax0 = A.core.fp(solver.x, maps)
+            if self.tolerance is not None:
+                info.residual0 = _kl_residual_norm(ax0, bt, self.background, bm)
+            if btm is not None:
+                info.residual0_cv = _kl_residual_norm(ax0, bt, self.background, btm)
         solver.run(iterations, check_every=10 if self.tolerance is not None else max(iterations, 1))
-        return _finish(solver, info, iterations, as_np, _is_volume(A))
+        x, info = _finish(solver, info, iterations, as_np, _is_volume(A))
+        self._cv_info(solver, info, iterations, _is_volume(A))
+        return x, info
 
 
 class SIRT(Solver):
@@ -171,55 +207,81 @@ class SIRT(Solver):
 
     def __call__(self, A, b, iterations: int, x0=None, lower_limit=None, upper_limit=None, x_mask=None, b_mask=None, b_test_mask=None):
         _check_projector(A)
-        self._reject_masks(b_mask, b_test_mask)
         bt, x0t, mt, maps, as_np = _as_batch(A, b, x0, x_mask)
+        bm, btm = self._masks(A, b_mask, b_test_mask)
         bp_mode = "symmetric" if getattr(A, "is_symmetric", False) else "reference"
         solver = BatchedSolver(
             A.core, maps, bt, "sirt", tolerance=self.tolerance, x0=x0t, x_mask=mt, lower_limit=lower_limit,
             upper_limit=upper_limit, relaxation=self.relaxation, bp_mode=bp_mode, background=self.background,
-            history_len=iterations, joint_stop=_is_volume(A),
+            history_len=iterations, joint_stop=_is_volume(A), b_mask=bm, b_test_mask=btm,
         )
         info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
+        if self.tolerance is not None or btm is not None:
+            r0 = bt - (A.core.fp(solver.x, maps) + (0.0 if self.background is None else self.background))
+            if self.tolerance is not None:
+                rm = r0 if bm is None else r0 * bm
+                info.residual0 = float(torch.sum(rm.double() ** 2).item())
+            if btm is not None:
+                info.residual0_cv = float(torch.sum((r0 * btm).double() ** 2).item())
         solver.run(iterations, check_every=10 if self.tolerance is not None else max(iterations, 1))
-        return _finish(solver, info, iterations, as_np, _is_volume(A))
+        x, info = _finish(solver, info, iterations, as_np, _is_volume(A))
+        self._cv_info(solver, info, iterations, _is_volume(A))
+        return x, info
 
 
 class PDHG(Solver):
     """Chambolle-Pock PDHG with the KL data term and optional isotropic TV2D (corrct ``solvers.py:987-1206``).
 
-    ``regularizer`` is ``None`` or an object with ``__reg_name__ == "TV2D"`` (or a float
-    TV weight); ``tolerance`` is not supported yet.
+    ``regularizer`` is an object with ``__reg_name__ == "TV2D"`` (or a float TV weight).  With a
+    ``tolerance`` or a ``b_test_mask`` every iterate is projected once more for its residuals, as
+    the reference does (solvers.py:1192-1204).
     """
 
     def __init__(self, verbose: bool = False, leave_progress: bool = True, tolerance=None, relaxation: float = 0.95, regularizer=None, data_term="kl", data_term_test=None):
         super().__init__(verbose=verbose, leave_progress=leave_progress, relaxation=relaxation, tolerance=tolerance, data_term=data_term, data_term_test=data_term_test)
         if self.data_term != "kl":
             raise NotImplementedError("the fused PDHG uses the KL data term")
-        if tolerance is not None:
-            raise NotImplementedError("PDHG tolerance is not supported by the B200 solvers yet")
         self.tv_weight = _tv_weight(regularizer)
 
     def __call__(self, A, b, iterations: int, x0=None, lower_limit=None, upper_limit=None, x_mask=None, b_mask=None, b_test_mask=None, precondition: bool = True):
         _check_projector(A)
-        self._reject_masks(b_mask, b_test_mask)
         if not precondition:
             raise NotImplementedError("PDHG without diagonal preconditioning is not supported by the B200 solvers")
-        if x0 is not None:
-            raise NotImplementedError("PDHG x0 is not supported by the B200 solvers yet")
-        bt, _, mt, maps, as_np = _as_batch(A, b, None, x_mask)
+        bt, x0t, mt, maps, as_np = _as_batch(A, b, x0, x_mask)
+        bm, btm = self._masks(A, b_mask, b_test_mask)
         bp_mode = "symmetric" if getattr(A, "is_symmetric", False) else "reference"
         if self.tv_weight is None:
             raise NotImplementedError("the fused PDHG needs a TV2D regularizer")
         solver = BatchedSolver(
-            A.core, maps, bt, "pdhg", x_mask=mt, lower_limit=lower_limit, upper_limit=upper_limit,
+            A.core, maps, bt, "pdhg", x0=x0t, x_mask=mt, lower_limit=lower_limit, upper_limit=upper_limit,
             relaxation=self.relaxation, tv_lambda=self.tv_weight, bp_mode=bp_mode, background=self.background,
-            joint_stop=_is_volume(A),
+            joint_stop=_is_volume(A), b_mask=bm,
         )
         info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
-        solver.run(iterations, check_every=max(iterations, 1))
-        x, info = _finish(solver, info, iterations, as_np, _is_volume(A))
-        info.iterations = iterations
-        return x, info
+        if self.tolerance is None and btm is None:
+            solver.run(iterations, check_every=max(iterations, 1))
+            x, info = _finish(solver, info, iterations, as_np, _is_volume(A))
+            info.iterations = iterations
+            return x, info
+
+        def residuals(x):
+            # KL residuals with the dual scaling sigma (data_terms.py:720-742, solvers.py:1137)
+            ax = A.core.fp(x, maps)
+            r = _kl_residual_norm(ax, bt, self.background, bm, solver.sigma)
+            r_cv = None if btm is None else _kl_residual_norm(ax, bt, self.background, btm, solver.sigma)
+            return r, r_cv
+
+        info.residual0, info.residual0_cv = residuals(solver.x)
+        for ii in range(iterations):
+            info.iterations += 1
+            solver.step()
+            info.residuals[ii], r_cv = residuals(solver.x)
+            if r_cv is not None:
+                info.residuals_cv[ii] = r_cv
+            if self.tolerance is not None and self.tolerance > info.residuals[ii]:
+                break
+        x = solver.x if _is_volume(A) else solver.x[0]
+        return (x.cpu().numpy() if as_np else x.clone()), info
 
 
 def _tv_weight(regularizer):
@@ -232,11 +294,18 @@ def _tv_weight(regularizer):
     raise NotImplementedError("only the isotropic TV2D regularizer is supported by the B200 PDHG")
 
 
-def _kl_residual_norm(ax: torch.Tensor, b: torch.Tensor, background) -> float:
-    """||KL residual||_1 in FP64 (corrct ``data_terms.py:720-742`` with sigma = 1)."""
+def _kl_residual_norm(ax: torch.Tensor, b: torch.Tensor, background, mask: torch.Tensor | None = None,
+                      sigma: torch.Tensor | None = None) -> float:
+    """||KL residual * mask||_1 in FP64 (corrct ``data_terms.py:720-742``; sigma = 1 unless given)."""
     proj = ax.double() if background is None else ax.double() + background
     r = torch.clamp(proj, min=float(eps))
-    res = (1 + r - torch.sqrt((r - 1) ** 2 + 4 * torch.clamp(b.double(), min=0))) / 2
+    sd = 4 * torch.clamp(b.double(), min=0)
+    if sigma is not None:
+        r = r * sigma.double()
+        sd = sd * sigma.double()
+    res = (1 + r - torch.sqrt((r - 1) ** 2 + sd)) / 2
+    if mask is not None:
+        res = res * mask.double()
     return float(res.abs().sum().item())
 
 
@@ -245,8 +314,6 @@ class SART(Solver):
 
     def __call__(self, A, b, iterations: int, A_num_rows=None, At=None, x0=None, lower_limit=None, upper_limit=None, x_mask=None, b_mask=None):
         _check_projector(A)
-        if b_mask is not None:
-            raise NotImplementedError("b_mask is not supported by the B200 SART")
         dev = A.projector_backend.device
         n_ang = len(A.angles_rot_rad)
         as_np = not isinstance(b, torch.Tensor)
@@ -254,7 +321,8 @@ class SART(Solver):
         xrf = isinstance(A, ProjectorAttenuationXRF)
         fpa = lambda x, ii: A.fp_angle(x, ii)  # noqa: E731
         bpa = (lambda y, ii: A.bp_angle(y, ii, single_line=True)) if xrf else (lambda y, ii: A.bp_angle(y, ii))  # noqa: E731
-        b_ones = torch.ones_like(bt)
+        bm = None if b_mask is None else _tensor(b_mask, dev).expand(bt.shape).contiguous()
+        b_ones = torch.ones_like(bt) if bm is None else bm.clone()
         tau = torch.stack([bpa(b_ones[..., ii, :].contiguous(), ii) for ii in range(n_ang)], dim=-2).abs()
         tau = torch.where(tau / tau.max() < 1e-5, torch.ones_like(tau), tau)
         tau = self.relaxation / tau
@@ -268,11 +336,23 @@ class SART(Solver):
         x = torch.zeros(vol_shape, device=dev) if x0 is None else _tensor(x0, dev).reshape(vol_shape).clone()
         mask = None if x_mask is None else _tensor(x_mask, dev)
         info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
+
+        def residual_norm(v):
+            # compute_residual (solvers.py:476-508): all angles' projections minus the data, masked
+            r = torch.stack([fpa(v, a) for a in range(n_ang)], dim=-2) - bt
+            if bm is not None:
+                r = r * bm
+            return float(torch.linalg.norm(r.double()).item())
+
+        if self.tolerance is not None:
+            info.residual0 = residual_norm(x)
         rows_sequence = np.random.permutation(n_ang)
         for ii in range(iterations):
             info.iterations += 1
             for a in rows_sequence:
                 res = fpa(x, int(a)) - bt[..., a, :]
+                if bm is not None:
+                    res = res * bm[..., a, :]
                 x = x - bpa((res * sigma[..., a, :]).contiguous(), int(a)) * tau[..., a, :]
                 if lower_limit is not None:
                     x = torch.clamp(x, min=lower_limit)
@@ -281,9 +361,7 @@ class SART(Solver):
                 if mask is not None:
                     x = x * mask
             if self.tolerance is not None:
-                fp = torch.stack([fpa(x, a) for a in range(n_ang)], dim=-1)
-                r = fp - torch.movedim(bt, -2, -1)
-                info.residuals[ii] = float(torch.linalg.norm(r.double()).item())
+                info.residuals[ii] = residual_norm(x)
                 if self.tolerance > info.residuals[ii]:
                     break
         return (x.cpu().numpy() if as_np else x), info
@@ -302,10 +380,10 @@ class FISTA(Solver):
 
     def __call__(self, A, b, iterations: int, x0=None, lower_limit=None, upper_limit=None, x_mask=None, b_mask=None, b_test_mask=None, precondition: bool = True):
         _check_projector(A)
-        self._reject_masks(b_mask, b_test_mask)
         if not precondition:
             raise NotImplementedError("FISTA without diagonal preconditioning is not supported by the B200 solvers")
         bt, x0t, mt, maps, as_np = _as_batch(A, b, x0, x_mask)
+        bm, btm = self._masks(A, b_mask, b_test_mask)
         core = A.core
         bp_mode = "symmetric" if getattr(A, "is_symmetric", False) else "reference"
         fp = lambda v: core.fp(v, maps)  # noqa: E731
@@ -313,7 +391,7 @@ class FISTA(Solver):
         n = core.n
         z = bt.shape[0]
         # compute_diagonal_scaling (solvers.py:60-117), relaxation on tau
-        tau = bp(torch.ones_like(bt)).abs()
+        tau = bp(torch.ones_like(bt) if bm is None else bm.clone()).abs()
         tau = torch.where(tau / tau.max() < 1e-5, torch.ones_like(tau), tau)
         tau = self.relaxation / tau
         x_ones = torch.ones((z, n, n), device=core.device)
@@ -329,9 +407,24 @@ class FISTA(Solver):
         t = 1.0
         bg = 0.0 if self.background is None else self.background
         info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
+        track = self.tolerance is not None or btm is not None
+
+        def residuals(v):
+            # squared l2 norms of the masked residuals (data_terms.py:136-161)
+            r = bt - (fp(v.contiguous()) + bg)
+            rm = r if bm is None else r * bm
+            r_cv = None if btm is None else float(torch.sum((r * btm).double() ** 2).item())
+            return float(torch.sum(rm.double() ** 2).item()), r_cv
+
+        if track:
+            info.residual0, r_cv = residuals(x)
+            if r_cv is not None:
+                info.residual0_cv = r_cv
         for ii in range(iterations):
             info.iterations += 1
             residual = bt - (fp(y.contiguous()) + bg)
+            if bm is not None:
+                residual = residual * bm
             grad = bp((residual * sigma).contiguous())
             x_new = y + tau * grad
             if lower_limit is not None or upper_limit is not None:
@@ -344,10 +437,11 @@ class FISTA(Solver):
             momentum = (t - 1.0) / t_new
             y = x_new + momentum * (x_new - x)
             x, t = x_new, t_new
-            if self.tolerance is not None:
-                r = bt - (fp(x.contiguous()) + bg)
-                info.residuals[ii] = float(torch.sum(r.double() ** 2).item())
-                if self.tolerance > info.residuals[ii]:
+            if track:
+                info.residuals[ii], r_cv = residuals(x)
+                if r_cv is not None:
+                    info.residuals_cv[ii] = r_cv
+                if self.tolerance is not None and self.tolerance > info.residuals[ii]:
                     break
         x = x if _is_volume(A) else x[0]
         return (x.cpu().numpy() if as_np else x), info

@@ -114,6 +114,72 @@ def make_case(corrct, name, n, n_ang, det_angles, det_weights, rand_ang_w, seed,
     print(f"{name}: maps {maps.shape} fp {fp_att.shape}")
 
 
+def make_surface_case(corrct):
+    """Finite-surface detectors with emitted sub-sampling (attenuation.py:105-120, xrf.py:243-258):
+    one 10 mm^2 detector at 50 mm and 90 degrees next to a point detector at 60 degrees, 3 sub-angles."""
+    n, n_ang, sub = 32, 12, 3
+    rng = phantoms.slice_rng(17, 0)
+    x = phantoms.ellipse_phantom(n, rng, num_ellipses=6, dtype=np.float64)
+    mu_in = phantoms.disk_attenuation(n, rng, mu_max=0.05, num_disks=3, dtype=np.float64)
+    mu_out = 0.7 * mu_in
+    angles32 = np.array(phantoms.angles(n_ang), dtype=np.float32)
+    det = corrct.physics.xrf.DetectorXRF
+    detectors = [det(surface_mm2=10.0, distance_mm=50.0, angle_rad=np.pi / 2), det(surface_mm2=0.0, distance_mm=1.0, angle_rad=np.pi / 3)]
+    att = corrct.physics.attenuation.AttenuationVolume(mu_in, mu_out, angles32, detectors, emitted_sub_sampling=sub, dtype=np.float64)
+    att.compute_maps(use_multithreading=False, verbose=False)
+    maps = att.get_maps()
+    det_angles = np.array([d.angle_rad for d in detectors])
+    with corrct.projectors.ProjectorAttenuationXRF(
+        (n, n), angles32, att_maps=maps, angles_detectors_rad=det_angles, use_multithreading=False, verbose=False
+    ) as p:
+        fp_att = p.fp(x)
+    np.savez_compressed(
+        os.path.join(HERE, "surface_case.npz"), n=n, angles=angles32, det_angles=det_angles,
+        det_surfaces=np.array([d.surface_mm2 for d in detectors]), det_distances=np.array([d.distance_mm for d in detectors]),
+        sub_sampling=sub, mu_in=mu_in, mu_out=mu_out, maps=maps, x=x, fp_att=fp_att,
+    )
+    print(f"surface: maps {maps.shape}")
+
+
+def make_mask_case(corrct):
+    """MLEM, SIRT, PDHG (KL, TV2D 1e-2) and FISTA with a data mask and a cross-validation mask
+    (solvers.py:333-343, 725-805, 895-984, 1115-1206, 1395-1513), and SART with the data mask
+    (solvers.py:572-629), on the n32_a16 case: 10 % of the sinogram pixels are masked out, 15 %
+    held out."""
+    g = np.load(os.path.join(HERE, "xrf_n32_a16.npz"))
+    n, angles, b = int(g["n"]), g["angles"], g["b"]
+    rng = np.random.default_rng(23)
+    b_mask = (rng.uniform(size=b.shape) >= 0.1).astype(np.float64)
+    b_test = (rng.uniform(size=b.shape) < 0.15).astype(np.float64)
+    p = corrct.projectors.ProjectorAttenuationXRF(
+        (n, n), angles, att_maps=g["maps"], angles_detectors_rad=g["det_angles"], use_multithreading=False,
+        backend="skimage", verbose=False,
+    )
+    out = dict(b_mask=b_mask, b_test_mask=b_test)
+    mlem = corrct.solvers.MLEM(tolerance=0.0, verbose=False)
+    xm, info = mlem(p, b, iterations=ITERATIONS, b_mask=b_mask, b_test_mask=b_test)
+    out.update(mlem_x=xm, mlem_res=info.residuals[:ITERATIONS], mlem_res_cv=info.residuals_cv[:ITERATIONS],
+               mlem_res0=info.residual0, mlem_res0_cv=info.residual0_cv)
+    sirt = corrct.solvers.SIRT(tolerance=0.0, verbose=False)
+    xs, info = sirt(p, b, iterations=ITERATIONS, b_mask=b_mask, b_test_mask=b_test)
+    out.update(sirt_x=xs, sirt_res=info.residuals[:ITERATIONS], sirt_res_cv=info.residuals_cv[:ITERATIONS],
+               sirt_res0=info.residual0, sirt_res0_cv=info.residual0_cv)
+    pdhg = corrct.solvers.PDHG(data_term="kl", regularizer=corrct.regularizers.Regularizer_TV2D(1e-2), tolerance=0.0, verbose=False)
+    xp, info = pdhg(p, b, iterations=ITERATIONS, b_mask=b_mask, b_test_mask=b_test)
+    out.update(pdhg_x=xp, pdhg_res=info.residuals[:ITERATIONS], pdhg_res_cv=info.residuals_cv[:ITERATIONS],
+               pdhg_res0=info.residual0, pdhg_res0_cv=info.residual0_cv)
+    fista = corrct.solvers.FISTA(tolerance=0.0, verbose=False)
+    xf, info = fista(p, b, iterations=ITERATIONS, b_mask=b_mask, b_test_mask=b_test)
+    out.update(fista_x=xf, fista_res=info.residuals[:ITERATIONS], fista_res_cv=info.residuals_cv[:ITERATIONS],
+               fista_res0=info.residual0, fista_res0_cv=info.residual0_cv)
+    # SART draws its angle order from np.random (solvers.py:603); its tolerance path cannot run
+    # here (compute_residual, solvers.py:503-505, subtracts (A, n) data from an (n, A) stack)
+    np.random.seed(5)
+    out["sart_x"] = corrct.solvers.SART(verbose=False)(p, b, iterations=3, b_mask=b_mask)[0]
+    np.savez_compressed(os.path.join(HERE, "mask_case.npz"), **out)
+    print(f"masks: maps {g['maps'].shape}")
+
+
 NOISE_CASES = [
     # name, photons, efficiency, poisson, readout std, background avg, background std, seed
     ("poisson", 1e3, 0.5, True, None, None, None, 101),
@@ -144,6 +210,8 @@ def main():
         for case in CASES:
             make_case(corrct, *case)
         make_noise_golden(corrct)
+        make_surface_case(corrct)
+        make_mask_case(corrct)
     print("\n".join(line for line in log.getvalue().splitlines() if ":" in line and ("maps" in line or "noise" in line)))
 
 

@@ -119,6 +119,48 @@ def test_solvers_match_reference(golden_cases, case, cuda):
     assert rel_l2(xp, g["pdhg_x"]) < TOL_RECON
 
 
+def test_masked_solvers_match_reference(golden_cases, cuda):
+    """MLEM, SIRT, PDHG and FISTA with b_mask and b_test_mask, and SART with b_mask, through the
+    drop-in solvers: reconstruction, residuals and cross-validation residuals against the
+    reference's own run."""
+    import os
+
+    from conftest import GOLDEN
+    from pycorrectedemissionct_b200 import projectors, solvers
+
+    g = golden_cases["n32_a16"]
+    m = dict(np.load(os.path.join(GOLDEN, "mask_case.npz")))
+    n = int(g["n"])
+    p = projectors.ProjectorAttenuationXRF((n, n), g["angles"], att_maps=g["maps"], angles_detectors_rad=g["det_angles"])
+    kw = dict(b_mask=m["b_mask"], b_test_mask=m["b_test_mask"])
+    xm, info = solvers.MLEM(tolerance=0.0)(p, g["b"], iterations=10, **kw)
+    assert rel_l2(xm, m["mlem_x"]) < TOL_RECON
+    np.testing.assert_allclose(info.residuals[:10], m["mlem_res"], rtol=TOL_RECON)
+    np.testing.assert_allclose(info.residuals_cv[:10], m["mlem_res_cv"], rtol=TOL_RECON)
+    np.testing.assert_allclose([info.residual0, info.residual0_cv], [m["mlem_res0"], m["mlem_res0_cv"]], rtol=TOL_RECON)
+    xs, info = solvers.SIRT(tolerance=0.0)(p, g["b"], iterations=10, **kw)
+    assert rel_l2(xs, m["sirt_x"]) < TOL_RECON
+    np.testing.assert_allclose(info.residuals[:10], m["sirt_res"], rtol=TOL_RECON)
+    np.testing.assert_allclose(info.residuals_cv[:10], m["sirt_res_cv"], rtol=TOL_RECON)
+    np.testing.assert_allclose([info.residual0, info.residual0_cv], [m["sirt_res0"], m["sirt_res0_cv"]], rtol=TOL_RECON)
+    xp, info = solvers.PDHG(data_term="kl", regularizer=1e-2, tolerance=0.0)(p, g["b"], iterations=10, **kw)
+    assert rel_l2(xp, m["pdhg_x"]) < TOL_RECON
+    np.testing.assert_allclose(info.residuals[:10], m["pdhg_res"], rtol=TOL_RECON)
+    np.testing.assert_allclose(info.residuals_cv[:10], m["pdhg_res_cv"], rtol=TOL_RECON)
+    np.testing.assert_allclose([info.residual0, info.residual0_cv], [m["pdhg_res0"], m["pdhg_res0_cv"]], rtol=TOL_RECON)
+    xf, info = solvers.FISTA(tolerance=0.0)(p, g["b"], iterations=10, **kw)
+    assert rel_l2(xf, m["fista_x"]) < TOL_RECON
+    np.testing.assert_allclose(info.residuals[:10], m["fista_res"], rtol=TOL_RECON)
+    np.testing.assert_allclose(info.residuals_cv[:10], m["fista_res_cv"], rtol=TOL_RECON)
+    np.random.seed(5)  # the angle order of SART, as drawn by the reference run
+    xa, _ = solvers.SART()(p, g["b"], iterations=3, b_mask=m["b_mask"])
+    assert rel_l2(xa, m["sart_x"]) < TOL_RECON
+    # a test mask alone holds its pixels out of the reconstruction: equal to b_mask = 1 - test
+    xt, _ = solvers.SIRT()(p, g["b"], iterations=10, b_test_mask=m["b_test_mask"])
+    xo, _ = solvers.SIRT()(p, g["b"], iterations=10, b_mask=1 - m["b_test_mask"])
+    np.testing.assert_array_equal(xt, xo)
+
+
 @pytest.mark.parametrize("n,n_ang", [(66, 20), (130, 45), (128, 90), (256, 360)])
 def test_against_oracle_port_medium(n, n_ang, cuda):
     from oracle import port
@@ -278,3 +320,28 @@ def test_fp_variants_bit_identical(n, n_ang, dtype, cuda, tmp_path, monkeypatch)
     v = autotune.tune(c, x, maps)
     assert v in autotune.VARIANTS and (tmp_path / "tune.json").exists()
     assert torch.equal(c.fp(x, maps), ref)
+
+
+def test_finite_surface_detectors_match_reference(cuda):
+    """A 10 mm^2 detector (3 emitted sub-angles) next to a point detector, against the reference's
+    own AttenuationVolume: through the core and through AttenuationVolume with DetectorXRF."""
+    import os
+
+    from conftest import GOLDEN
+    from pycorrectedemissionct_b200 import attenuation, core
+
+    g = dict(np.load(os.path.join(GOLDEN, "surface_case.npz")))
+    rad32 = np.array(g["angles"], dtype=np.float32)
+    maps = core.compute_maps(_t(g["mu_in"], cuda)[None], _t(g["mu_out"], cuda)[None], rad32, g["det_angles"],
+                             surfaces_mm2=g["det_surfaces"], distances_mm=g["det_distances"],
+                             sub_sampling=int(g["sub_sampling"]))
+    assert rel_l2(maps[0].cpu().numpy(), g["maps"]) < TOL
+    dets = [attenuation.DetectorXRF(surface_mm2=float(s_), distance_mm=float(d_), angle_rad=float(a_))
+            for s_, d_, a_ in zip(g["det_surfaces"], g["det_distances"], g["det_angles"])]
+    av = attenuation.AttenuationVolume(g["mu_in"], g["mu_out"], rad32, dets, emitted_sub_sampling=int(g["sub_sampling"]),
+                                       device=cuda)
+    av.compute_maps(verbose=False)
+    assert rel_l2(av.maps, g["maps"]) < TOL
+    c = core.XrfCore(int(g["n"]), g["angles"], n_det=2, device=cuda)
+    fp = c.fp(_t(g["x"], cuda)[None], maps)[0].cpu().numpy()
+    assert rel_l2(fp, g["fp_att"]) < TOL

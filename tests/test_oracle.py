@@ -1,10 +1,12 @@
 """CPU: the oracle port against the reference-generated golden fixtures, and known-answer tests
 of the restated scikit-image primitives (analytic, independent of scikit-image)."""
 
+import os
+
 import numpy as np
 import pytest
 
-from conftest import rel_l2
+from conftest import GOLDEN, rel_l2
 from oracle import port
 from oracle import skimage_restated as skr
 
@@ -48,6 +50,38 @@ def test_port_solvers_match_reference_golden(golden_cases, case):
     np.testing.assert_allclose(res, g["mlem_res"], rtol=1e-12)
     assert rel_l2(port.sirt(fp, bp, g["b"], 10, (n, n)), g["sirt_x"]) < 1e-13
     assert rel_l2(port.pdhg_kl_tv(fp, bp, g["b"], 10, (n, n), 1e-2), g["pdhg_x"]) < 1e-13
+
+
+def test_port_masked_solvers_match_reference_golden(golden_cases):
+    """MLEM / SIRT / PDHG / FISTA with b_mask and b_test_mask, residuals and cross-validation
+    residuals included."""
+    g = golden_cases["n32_a16"]
+    m = np.load(os.path.join(GOLDEN, "mask_case.npz"))
+    n = int(g["n"])
+    _, deg32 = port.backend_angles(g["angles"])
+    fp = lambda v: port.fp_xrf(v, g["maps"], deg32)  # noqa: E731
+    bp = lambda s: port.bp_xrf(s, g["maps"], deg32)  # noqa: E731
+    cv = []
+    xm, res = port.mlem(fp, bp, g["b"], 10, tolerance=0.0, b_mask=m["b_mask"], b_test_mask=m["b_test_mask"], residuals_cv=cv)
+    assert rel_l2(xm, m["mlem_x"]) < 1e-13
+    np.testing.assert_allclose(res, m["mlem_res"], rtol=1e-12)
+    np.testing.assert_allclose(cv, m["mlem_res_cv"], rtol=1e-12)
+    cv = []
+    xs = port.sirt(fp, bp, g["b"], 10, (n, n), b_mask=m["b_mask"], b_test_mask=m["b_test_mask"], residuals_cv=cv)
+    assert rel_l2(xs, m["sirt_x"]) < 1e-13
+    np.testing.assert_allclose(cv, m["sirt_res_cv"], rtol=1e-12)
+    res, cv = [], []
+    xp = port.pdhg_kl_tv(fp, bp, g["b"], 10, (n, n), 1e-2, b_mask=m["b_mask"], b_test_mask=m["b_test_mask"], tolerance=0.0,
+                         residuals=res, residuals_cv=cv)
+    assert rel_l2(xp, m["pdhg_x"]) < 1e-13
+    np.testing.assert_allclose(res, m["pdhg_res"], rtol=1e-12)
+    np.testing.assert_allclose(cv, m["pdhg_res_cv"], rtol=1e-12)
+    res, cv = [], []
+    xf = port.fista(fp, bp, g["b"], 10, (n, n), b_mask=m["b_mask"], b_test_mask=m["b_test_mask"], tolerance=0.0,
+                    residuals=res, residuals_cv=cv)
+    assert rel_l2(xf, m["fista_x"]) < 1e-13
+    np.testing.assert_allclose(res, m["fista_res"], rtol=1e-12)
+    np.testing.assert_allclose(cv, m["fista_res_cv"], rtol=1e-12)
 
 
 def test_reference_float32_maps_close_to_fp64(golden_cases):
@@ -183,3 +217,17 @@ def test_port_add_noise_matches_reference_golden(case):
     np.testing.assert_array_equal(scaled, g[f"{name}_scaled"])
     np.testing.assert_array_equal(noisy, g[f"{name}_noisy"])
     assert background == float(g[f"{name}_background"])
+
+
+def test_port_finite_surface_detectors_match_reference_golden():
+    """Emitted sub-sampling of a finite detector next to a point detector (attenuation.py:105-120)."""
+    import os
+
+    from conftest import GOLDEN
+
+    g = dict(np.load(os.path.join(GOLDEN, "surface_case.npz")))
+    rad32, deg32 = port.backend_angles(g["angles"])
+    maps = port.compute_maps(g["mu_in"], g["mu_out"], rad32, g["det_angles"], detector_surfaces_mm2=g["det_surfaces"],
+                             detector_distances_mm=g["det_distances"], emitted_sub_sampling=int(g["sub_sampling"]))
+    assert rel_l2(maps, g["maps"]) < 1e-13
+    assert rel_l2(port.fp_xrf(g["x"], g["maps"], deg32), g["fp_att"]) < 1e-13
