@@ -11,7 +11,8 @@
 //
 // Phase 1 (maps_scan_kernel): one thread per rotated-frame column c' of one rotation job
 // walks r' = 0..P-1, sampling U only where the column crosses the image (elsewhere U is
-// exactly 0), keeping the running sum in FP64, and writes W (FP32) to the workspace.
+// exactly 0; where all four taps are inside the image, without per-tap tests), keeping the
+// running sum in FP64, and writes W (FP32) to the workspace.
 // Phase 2 (maps_resample_kernel): one thread per map pixel samples W of the incident job
 // and of every emitted (detector, sub-angle) job at the rotated-back position, and writes
 // exp(-L_in) * mean_k exp(-L_out,k) as FP32 or BF16.  Angles are processed in passes sized
@@ -61,6 +62,57 @@ __device__ __forceinline__ float bilin_zero(const float* img, int h, int w, floa
   return fmaf(fy.f, bot - top, top);
 }
 
+// Bilinear sample whose four taps are known to lie inside the (w x hgt) image.  The clamps are
+// no-ops for such coordinates; they only keep every access in bounds.  Same arithmetic as
+// bilin_zero.
+__device__ __forceinline__ float bilin_inside(const float* img, int w, int hgt, float x, float y) {
+  const FloorSplit fx = floor_split(x), fy = floor_split(y);
+  const int x0 = min(max(fx.i, 0), w - 2), y0 = min(max(fy.i, 0), hgt - 2);
+  const float* q = img + (int64_t)y0 * w + x0;
+  const float v00 = __ldg(q), v01 = __ldg(q + 1), v10 = __ldg(q + w), v11 = __ldg(q + w + 1);
+  const float top = fmaf(fx.f, v01 - v00, v00);
+  const float bot = fmaf(fx.f, v11 - v10, v10);
+  return fmaf(fy.f, bot - top, top);
+}
+
+// Bilinear sample of a (P x P) image with zero outside: one range test picks the unchecked
+// four-tap load for interior coordinates, bilin_zero otherwise.
+__device__ __forceinline__ float bilin_square(const float* img, int P, float x, float y) {
+  const FloorSplit fx = floor_split(x), fy = floor_split(y);
+  if ((unsigned)fx.i < (unsigned)(P - 1) && (unsigned)fy.i < (unsigned)(P - 1)) {
+    const float* q = img + (int64_t)fy.i * P + fx.i;
+    const float v00 = __ldg(q), v01 = __ldg(q + 1), v10 = __ldg(q + P), v11 = __ldg(q + P + 1);
+    const float top = fmaf(fx.f, v01 - v00, v00);
+    const float bot = fmaf(fx.f, v11 - v10, v10);
+    return fmaf(fy.f, bot - top, top);
+  }
+  return bilin_zero(img, P, P, x, y);
+}
+
+// Integer r in [*lo, *hi] with x(r) = ax + r bx and y(r) = ay + r by both in [lim0, lim1]
+// (exact arithmetic), clipped to [0, P - 1]; *lo > *hi when there is none.
+__device__ __forceinline__ void column_inside(double ax, double bx, double ay, double by, double lim0, double lim1,
+                                              int P, int* lo, int* hi) {
+  double tlo = -1e300, thi = 1e300;
+  if (fabs(bx) < 1e-12) {
+    if (!(ax >= lim0 && ax <= lim1)) { *lo = 1; *hi = 0; return; }
+  } else {
+    double t0 = (lim0 - ax) / bx, t1 = (lim1 - ax) / bx;
+    if (t0 > t1) { double t = t0; t0 = t1; t1 = t; }
+    tlo = fmax(tlo, t0); thi = fmin(thi, t1);
+  }
+  if (fabs(by) < 1e-12) {
+    if (!(ay >= lim0 && ay <= lim1)) { *lo = 1; *hi = 0; return; }
+  } else {
+    double t0 = (lim0 - ay) / by, t1 = (lim1 - ay) / by;
+    if (t0 > t1) { double t = t0; t0 = t1; t1 = t; }
+    tlo = fmax(tlo, t0); thi = fmin(thi, t1);
+  }
+  if (tlo > thi) { *lo = 1; *hi = 0; return; }
+  *lo = (int)fmax(0.0, ceil(tlo));
+  *hi = (int)fmin((double)(P - 1), floor(thi));
+}
+
 // Range of r' (inclusive) where the column c' samples inside (-1, n) x (-1, n) of mu, widened
 // by one row each side; outside it every bilinear tap is zero padding.
 __device__ __forceinline__ void column_support(double ax, double bx, double ay, double by, int n, int P,
@@ -87,12 +139,16 @@ __device__ __forceinline__ void column_support(double ax, double bx, double ay, 
   *hi = min(P - 1, (int)ceil(thi) + 1);
 }
 
+// One thread per column; the 32 columns of a warp walk the rows in lockstep (coalesced W
+// stores), with warp-uniform row ranges: no lane samples before the warp's first support row or
+// after its last, and rows where every lane's four taps are inside mu skip the per-tap tests.
 __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
   const int P = p.P, n = p.n;
-  const int cpr = blockIdx.x * blockDim.x + threadIdx.x;  // rotated-frame column c'
-  const int job_lin = blockIdx.y;                          // (angle in pass, job)
+  const int cpr_raw = blockIdx.x * blockDim.x + threadIdx.x;  // rotated-frame column c'
+  const bool valid = cpr_raw < P;
+  const int cpr = valid ? cpr_raw : P - 1;  // lanes past the frame shadow the last column, store nothing
+  const int job_lin = blockIdx.y;           // (angle in pass, job)
   const int s = blockIdx.z;
-  if (cpr >= P) return;
   const int ai = job_lin / p.jobs_per_angle;
   const int job = job_lin - ai * p.jobs_per_angle;
   const int a = p.a0 + ai;
@@ -102,8 +158,26 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
   // mu coordinates = padded coordinates - e
   const float m00 = (float)Md[0], m01 = (float)Md[1], m02 = (float)(Md[2] - p.e);
   const float m10 = (float)Md[3], m11 = (float)Md[4], m12 = (float)(Md[5] - p.e);
+  const double ax = Md[0] * cpr + Md[2] - p.e, ay = Md[3] * cpr + Md[5] - p.e;
   int lo, hi;
-  column_support(Md[0] * cpr + Md[2] - p.e, Md[1], Md[3] * cpr + Md[5] - p.e, Md[4], n, P, &lo, &hi);
+  column_support(ax, Md[1], ay, Md[4], n, P, &lo, &hi);
+  if (lo > hi) { lo = P; hi = -1; }
+  // rows whose four taps all lie inside mu, with a 0.01-pixel margin against the FP32
+  // evaluation of the coordinates below
+  int ilo = P, ihi = -1;
+  if (n >= 2) column_inside(ax, Md[1], ay, Md[4], 0.01, (double)n - 1.01, P, &ilo, &ihi);
+  ilo = max(ilo, lo);
+  ihi = min(ihi, hi);
+  if (ilo > ihi) { ilo = P; ihi = -1; }
+  int wlo = lo, whi = hi, wilo = ilo, wihi = ihi;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    wlo = min(wlo, __shfl_xor_sync(0xffffffffu, wlo, o));
+    whi = max(whi, __shfl_xor_sync(0xffffffffu, whi, o));
+    wilo = max(wilo, __shfl_xor_sync(0xffffffffu, wilo, o));
+    wihi = min(wihi, __shfl_xor_sync(0xffffffffu, wihi, o));
+  }
+  if (wilo > wihi) { wilo = whi + 1; wihi = whi; }  // no row is inside for every lane
   const float fc = (float)cpr;
   const float xc = fmaf(m00, fc, m02), yc = fmaf(m10, fc, m12);
   float* W = p.work + (((int64_t)s * p.na + ai) * p.jobs_per_angle + job) * (int64_t)P * P + cpr;
@@ -114,63 +188,158 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
     const float fr = (float)(P - 1);
     wrap = 0.5 * (double)bilin_zero(mu, n, n, fmaf(m01, fr, xc), fmaf(m11, fr, yc));
   }
+  // W[r] = acc + U[r]/2 + wrap with acc = sum_{k<r} U[k] (FP64); U = 0 outside [lo, hi]
   double acc = 0.0;
-  for (int r = 0; r < P; ++r) {
-    float u = 0.f;
-    if (r >= lo && r <= hi) {
-      const float fr = (float)r;
-      u = bilin_zero(mu, n, n, fmaf(m01, fr, xc), fmaf(m11, fr, yc));
-    }
-    W[(int64_t)r * P] = (float)(acc + 0.5 * (double)u + wrap);
+  int r = 0;
+  const float w_before = (float)wrap;
+  for (; r < wlo; ++r)
+    if (valid) W[(int64_t)r * P] = w_before;
+  for (; r < wilo; ++r) {
+    const float fr = (float)r;
+    const float u = (r >= lo && r <= hi) ? bilin_zero(mu, n, n, fmaf(m01, fr, xc), fmaf(m11, fr, yc)) : 0.f;
+    if (valid) W[(int64_t)r * P] = (float)(acc + 0.5 * (double)u + wrap);
     acc += (double)u;
   }
+  for (; r + 3 <= wihi; r += 4) {
+    float u[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float fr = (float)(r + k);
+      u[k] = bilin_inside(mu, n, n, fmaf(m01, fr, xc), fmaf(m11, fr, yc));
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (valid) W[(int64_t)(r + k) * P] = (float)(acc + 0.5 * (double)u[k] + wrap);
+      acc += (double)u[k];
+    }
+  }
+  for (; r <= wihi; ++r) {
+    const float fr = (float)r;
+    const float u = bilin_inside(mu, n, n, fmaf(m01, fr, xc), fmaf(m11, fr, yc));
+    if (valid) W[(int64_t)r * P] = (float)(acc + 0.5 * (double)u + wrap);
+    acc += (double)u;
+  }
+  for (; r <= whi; ++r) {
+    const float fr = (float)r;
+    const float u = (r >= lo && r <= hi) ? bilin_zero(mu, n, n, fmaf(m01, fr, xc), fmaf(m11, fr, yc)) : 0.f;
+    if (valid) W[(int64_t)r * P] = (float)(acc + 0.5 * (double)u + wrap);
+    acc += (double)u;
+  }
+  const float w_after = (float)(acc + wrap);
+  for (; r < P; ++r)
+    if (valid) W[(int64_t)r * P] = w_after;
 }
 
+// One CTA = a 32 x 32 pixel tile of one (slice, angle); thread t owns the four pixels
+// (x, y + 8k), k < 4, so that each warp instruction covers an 8-wide, 4-tall block whose taps
+// fall in a compact patch of the rotated frame.  The rotate(+phi) matrices of the angle's jobs
+// are converted to FP32 once per CTA into shared memory.
+constexpr int RS_TILE = 32;
+constexpr int RS_PIX = 4;
+
 __global__ void __launch_bounds__(256) maps_resample_kernel(MapsPass p) {
+  extern __shared__ float rs_mats[];  // [jobs_per_angle][6]
   const int n = p.n, P = p.P;
-  const int64_t pix = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int ai = blockIdx.y;
   const int s = blockIdx.z;
-  if (pix >= (int64_t)n * n) return;
-  const int i = (int)(pix / n), j = (int)(pix - (int64_t)i * n);
   const int a = p.a0 + ai;
-  const float X = (float)(j + p.e), Y = (float)(i + p.e);  // padded coordinates of the pixel
-  const float* wbase = p.work + ((int64_t)s * p.na + ai) * p.jobs_per_angle * (int64_t)P * P;
+  const int J = p.jobs_per_angle;
+  for (int t = threadIdx.x; t < 6 * J; t += blockDim.x) {
+    const int job = t / 6;
+    rs_mats[t] = (float)job_matrix(p, a, job, 1)[t - job * 6];
+  }
+  __syncthreads();
+  const int tiles_x = (n + RS_TILE - 1) / RS_TILE;
+  const int ty = blockIdx.x / tiles_x, tx = blockIdx.x - ty * tiles_x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = tx * RS_TILE + (warp & 3) * 8 + (lane & 7);
+  const int i0 = ty * RS_TILE + (warp >> 2) * 4 + (lane >> 3);
+  if (j >= n || i0 >= n) return;
+  const float X = (float)(j + p.e);  // padded coordinates of the pixels
+  const float* wbase = p.work + ((int64_t)s * p.na + ai) * J * (int64_t)P * P;
+  const int64_t n2 = (int64_t)n * n;
 
-  auto sample_job = [&](int job) -> float {
-    const double* Mb = job_matrix(p, a, job, 1);  // rotate(+phi)
-    const float x = fmaf((float)Mb[1], Y, fmaf((float)Mb[0], X, (float)Mb[2]));
-    const float y = fmaf((float)Mb[4], Y, fmaf((float)Mb[3], X, (float)Mb[5]));
-    return bilin_zero(wbase + (int64_t)job * P * P, P, P, x, y);
+  // L of job `job` at the four pixels (pixels past the image edge are sampled, in bounds, and
+  // not stored)
+  auto sample4 = [&](int job, float* L) {
+    const float* m = rs_mats + job * 6;
+    const float* w = wbase + (int64_t)job * P * P;
+#pragma unroll
+    for (int k = 0; k < RS_PIX; ++k) {
+      const float Y = (float)(i0 + 8 * k + p.e);
+      const float x = fmaf(m[1], Y, fmaf(m[0], X, m[2]));
+      const float y = fmaf(m[4], Y, fmaf(m[3], X, m[5]));
+      L[k] = bilin_square(w, P, x, y);
+    }
+  };
+  auto store4 = [&](int64_t plane, const float* v) {
+#pragma unroll
+    for (int k = 0; k < RS_PIX; ++k) {
+      const int i = i0 + 8 * k;
+      if (i >= n) break;
+      const int64_t off = plane * n2 + (int64_t)i * n + j;
+      if (p.maps_dtype == CCT_DTYPE_BF16) {
+        reinterpret_cast<__nv_bfloat16*>(p.maps)[off] = __float2bfloat16_rn(v[k]);
+      } else {
+        reinterpret_cast<float*>(p.maps)[off] = v[k];
+      }
+    }
   };
 
+  float L[RS_PIX];
   if (p.maps_dtype == CCT_DTYPE_FIELDS_F32) {
     // line-integral fields: plane 0 = L_in, plane 1 + d = L_out of detector d (n_sub == 1)
-    float* fo = reinterpret_cast<float*>(p.maps) + ((int64_t)s * p.n_angles + a) * (1 + p.n_det) * (int64_t)n * n + pix;
-    fo[0] = p.has_in ? sample_job(0) : 0.f;
-    for (int d = 0; d < p.n_det; ++d)
-      fo[(int64_t)(1 + d) * n * n] = p.has_out ? sample_job((p.has_in ? 1 : 0) + d) : 0.f;
+    const int64_t plane0 = ((int64_t)s * p.n_angles + a) * (1 + p.n_det);
+    if (p.has_in) {
+      sample4(0, L);
+    } else {
+#pragma unroll
+      for (int k = 0; k < RS_PIX; ++k) L[k] = 0.f;
+    }
+    store4(plane0, L);
+    for (int d = 0; d < p.n_det; ++d) {
+      if (p.has_out) {
+        sample4((p.has_in ? 1 : 0) + d, L);
+      } else {
+#pragma unroll
+        for (int k = 0; k < RS_PIX; ++k) L[k] = 0.f;
+      }
+      store4(plane0 + 1 + d, L);
+    }
     return;
   }
-  float f_in = 1.f;
+  float f_in[RS_PIX];
   int job = 0;
   if (p.has_in) {
-    f_in = expf(-sample_job(0));
+    sample4(0, L);
+#pragma unroll
+    for (int k = 0; k < RS_PIX; ++k) f_in[k] = expf(-L[k]);
     job = 1;
+  } else {
+#pragma unroll
+    for (int k = 0; k < RS_PIX; ++k) f_in[k] = 1.f;
   }
   for (int d = 0; d < p.n_det; ++d) {
-    float f = f_in;
+    float f[RS_PIX];
+#pragma unroll
+    for (int k = 0; k < RS_PIX; ++k) f[k] = f_in[k];
     if (p.has_out) {
-      float sum = 0.f;
-      for (int k = 0; k < p.n_sub; ++k) sum += expf(-sample_job(job + d * p.n_sub + k));
-      f *= sum / (float)p.n_sub;
+      float sum[RS_PIX] = {0.f, 0.f, 0.f, 0.f};
+      for (int q = 0; q < p.n_sub; ++q) {
+        sample4(job + d * p.n_sub + q, L);
+#pragma unroll
+        for (int k = 0; k < RS_PIX; ++k) sum[k] += expf(-L[k]);
+      }
+      if (p.n_sub == 1) {
+#pragma unroll
+        for (int k = 0; k < RS_PIX; ++k) f[k] *= sum[k];
+      } else {
+        const float ns = (float)p.n_sub;
+#pragma unroll
+        for (int k = 0; k < RS_PIX; ++k) f[k] *= sum[k] / ns;
+      }
     }
-    const int64_t off = (((int64_t)s * p.n_angles + a) * p.n_det + d) * (int64_t)n * n + pix;
-    if (p.maps_dtype == CCT_DTYPE_BF16) {
-      reinterpret_cast<__nv_bfloat16*>(p.maps)[off] = __float2bfloat16_rn(f);
-    } else {
-      reinterpret_cast<float*>(p.maps)[off] = f;
-    }
+    store4(((int64_t)s * p.n_angles + a) * p.n_det + d, f);
   }
 }
 
@@ -205,8 +374,9 @@ int launch_maps(const cct_maps_desc* d, const float* mu_in, const float* mu_out,
     p.na = std::min(per_pass, d->n_angles - a0);
     const dim3 g1((P + 127) / 128, p.na * p.jobs_per_angle, d->n_slices);
     maps_scan_kernel<<<g1, 128, 0, st>>>(p);
-    const dim3 g2((unsigned)(((int64_t)d->n * d->n + 255) / 256), p.na, d->n_slices);
-    maps_resample_kernel<<<g2, 256, 0, st>>>(p);
+    const int tiles = (d->n + RS_TILE - 1) / RS_TILE;
+    const dim3 g2((unsigned)(tiles * tiles), p.na, d->n_slices);
+    maps_resample_kernel<<<g2, 256, 6 * p.jobs_per_angle * sizeof(float), st>>>(p);
   }
   return CCT_OK;
 }
