@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define CCT_ABI_VERSION 4
+#define CCT_ABI_VERSION 5
 
 /* Status codes. */
 #define CCT_OK 0
@@ -128,9 +128,18 @@ typedef struct cct_maps_desc {
   const double* rot_in;  /* device [A][2][6]: scikit-image rotate inverse maps of the padded image,
                             [0] = rotate(-phi), [1] = rotate(+phi), same entry order as fp_matrix */
   const double* rot_out; /* device [A][D][n_sub][2][6], emitted directions (phi includes + pi) */
+  const int32_t* pairs;  /* device [n_entries][2] (angle, partner), or NULL (every angle on its own).
+                            Each entry computes the maps of `angle` and, when partner >= 0, of the
+                            angle `partner` = angle + pi (to float32 rounding) from the same
+                            rotations: the half turn of the rotated frame is a permutation of its
+                            lattice and the partner's scans are the reverse scans, so one rotation
+                            per direction serves both angles.  Every angle must appear once; out of
+                            range indices are skipped. */
+  int32_t n_entries;     /* entries of `pairs` (ignored when pairs is NULL) */
+  int32_t reserved;
 } cct_maps_desc;
 
-/* Workspace bytes needed to process `angles_per_pass` angles per pass (>= 1). */
+/* Workspace bytes needed to process `angles_per_pass` angles (entries, with pairs) per pass (>= 1). */
 int cct_maps_workspace_size(const cct_maps_desc* desc, int32_t angles_per_pass, size_t* bytes);
 
 /* Compute maps.  mu_in / mu_out: device [S][n][n] float32 (NULL when absent).  The number of

@@ -13,7 +13,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcorrct_b200.so")
 
-ABI_VERSION = 4  # CCT_ABI_VERSION of include/corrct_b200.h
+ABI_VERSION = 5  # CCT_ABI_VERSION of include/corrct_b200.h
 
 CCT_OK = 0
 CCT_ERR_VALUE = 1
@@ -68,6 +68,9 @@ class MapsDesc(ctypes.Structure):
         ("has_out", ctypes.c_int32),
         ("rot_in", ctypes.c_void_p),
         ("rot_out", ctypes.c_void_p),
+        ("pairs", ctypes.c_void_p),
+        ("n_entries", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

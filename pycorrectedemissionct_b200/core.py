@@ -299,8 +299,13 @@ def compute_maps(
     workspace: torch.Tensor | None = None,
     workspace_bytes: int = DEFAULT_MAPS_WORKSPACE,
     out: torch.Tensor | None = None,
+    half_turns: bool = True,
 ) -> torch.Tensor:
-    """Attenuation maps (S, A, D, n, n) on the device from mu_in / mu_out (S, n, n) float32."""
+    """Attenuation maps (S, A, D, n, n) on the device from mu_in / mu_out (S, n, n) float32.
+
+    ``half_turns``: angles whose half-turn partner (angle + pi) is also in the set share one
+    rotation per direction (``geometry.half_turn_pairs``); False computes every angle on its own.
+    """
     ref = mu_in if mu_in is not None else mu_out
     if ref is None:
         raise ValueError("No attenuation volumes were given.")
@@ -323,11 +328,18 @@ def compute_maps(
     desc.n_sub, desc.maps_dtype = n_sub, cdt
     desc.has_in, desc.has_out = int(mu_in is not None), int(mu_out is not None)
     desc.rot_in, desc.rot_out = rot_in_d.data_ptr(), rot_out_d.data_ptr()
+    pairs = geometry.half_turn_pairs(angles_rad32) if half_turns else None
+    pairs_d = None
+    entries = n_ang
+    if pairs is not None:
+        pairs_d = torch.from_numpy(pairs).to(device)
+        desc.pairs, desc.n_entries = pairs_d.data_ptr(), len(pairs)
+        entries = len(pairs)
     need = ctypes.c_size_t(0)
     _lib.call("cct_maps_workspace_size", ctypes.byref(desc), 1, ctypes.byref(need))
     if workspace is None:
         # at least 8 angles (of the whole batch) per pass, at most all of them
-        nbytes = min(max(int(workspace_bytes), 8 * int(need.value)), int(need.value) * n_ang)
+        nbytes = min(max(int(workspace_bytes), 8 * int(need.value)), int(need.value) * entries)
         workspace = torch.empty(nbytes, dtype=torch.uint8, device=device)
     planes = n_det + 1 if cdt == _lib.CCT_DTYPE_FIELDS_F32 else n_det
     if out is None:
@@ -335,7 +347,7 @@ def compute_maps(
     else:
         _check_tensor(out, (s, n_ang, planes, n, n), tdt, device, "out")
         maps = out
-    compute_maps.last_passes = -(-n_ang // max(1, (workspace.numel() * workspace.element_size()) // int(need.value)))
+    compute_maps.last_passes = -(-entries // max(1, (workspace.numel() * workspace.element_size()) // int(need.value)))
     _lib.call(
         "cct_compute_maps", ctypes.byref(desc), _ptr(mu_in), _ptr(mu_out), maps.data_ptr(), workspace.data_ptr(),
         workspace.numel() * workspace.element_size(), stream_handle(device),

@@ -130,6 +130,8 @@ int cct_maps_workspace_size(const cct_maps_desc* desc, int32_t angles_per_pass, 
               "n_angles, n_det, n_slices and n_sub must be >= 1");
   CCT_REQUIRE(angles_per_pass >= 1, "angles_per_pass must be >= 1");
   CCT_REQUIRE(desc->has_in || desc->has_out, "No attenuation volumes were given.");
+  CCT_REQUIRE(desc->pairs == nullptr || (desc->n_entries >= 1 && desc->n_entries <= desc->n_angles),
+              "n_entries must be in [1, n_angles] when pairs are given");
   *bytes = (size_t)cct::maps_bytes_per_angle(desc) * (size_t)angles_per_pass;
   return CCT_OK;
 }

@@ -17,6 +17,11 @@
 // and of every emitted (detector, sub-angle) job at the rotated-back position, and writes
 // exp(-L_in) * mean_k exp(-L_out,k) as FP32 or BF16.  Angles are processed in passes sized
 // to the caller's workspace.
+// Half-turn pairs: for angles phi and phi + pi every rotation of the second is the first's turned
+// by 180 degrees about the frame centre, a permutation of the lattice.  Its W at the first's
+// (r', c') is then K[c'] - W[r'][c'] with the per-column constant K = sum U + U[0]/2 + U[P-1]/2,
+// and its rotate-back samples sit at the same positions; one scan and one resample per direction
+// give both angles' maps.
 
 #include <algorithm>
 #include <cmath>
@@ -28,15 +33,29 @@ namespace cct {
 
 struct MapsPass {
   int n, P, e, n_det, n_sub, has_in, has_out, maps_dtype, n_angles;
-  int a0, na;                 // angles of this pass
+  int a0, na;                 // entries of this pass (angles, or (angle, partner) pairs)
   int jobs_per_angle;         // has_in + has_out * n_det * n_sub
   const double* rot_in;       // [A][2][6]
   const double* rot_out;      // [A][D][n_sub][2][6]
+  const int* pairs;           // [entries][2] (angle, partner) or NULL
   const float* mu_in;         // [S][n][n]
   const float* mu_out;
   float* work;                // [S][na][jobs_per_angle][P][P]
+  float* kcol;                // [S][na][jobs_per_angle][P] per-column constants of the partner scans
   void* maps;                 // [S][A][D][n][n]
 };
+
+// Angle of entry e and its half-turn partner (-1: none); a = -1 for an out-of-range entry.
+__device__ __forceinline__ void entry_angles(const MapsPass& p, int e, int* a, int* b) {
+  if (p.pairs == nullptr) {
+    *a = e;
+    *b = -1;
+    return;
+  }
+  const int aa = p.pairs[2 * e], bb = p.pairs[2 * e + 1];
+  *a = (aa >= 0 && aa < p.n_angles) ? aa : -1;
+  *b = (bb >= 0 && bb < p.n_angles && bb != aa) ? bb : -1;
+}
 
 __device__ __forceinline__ const double* job_matrix(const MapsPass& p, int a, int job, int which) {
   // job 0 = incident (if has_in); then emitted jobs d * n_sub + k
@@ -87,6 +106,39 @@ __device__ __forceinline__ float bilin_square(const float* img, int P, float x, 
     return fmaf(fy.f, bot - top, top);
   }
   return bilin_zero(img, P, P, x, y);
+}
+
+// Bilinear samples at (x, y) of a (P x P) image W and of the partner field K[c] - W[r][c]
+// (zero outside the frame for both).  *La is bilin_square(W) exactly.
+__device__ __forceinline__ void bilin_square_pair(const float* img, const float* K, int P, float x, float y,
+                                                  float* La, float* Lb) {
+  const FloorSplit fx = floor_split(x), fy = floor_split(y);
+  const int x0 = fx.i, y0 = fy.i;
+  float v00, v01, v10, v11, u00, u01, u10, u11;
+  if ((unsigned)x0 < (unsigned)(P - 1) && (unsigned)y0 < (unsigned)(P - 1)) {
+    const float* q = img + (int64_t)y0 * P + x0;
+    v00 = __ldg(q); v01 = __ldg(q + 1); v10 = __ldg(q + P); v11 = __ldg(q + P + 1);
+    const float k0 = __ldg(K + x0), k1 = __ldg(K + x0 + 1);
+    u00 = k0 - v00; u01 = k1 - v01; u10 = k0 - v10; u11 = k1 - v11;
+  } else {
+    const bool xin0 = x0 >= 0 && x0 < P, xin1 = x0 + 1 >= 0 && x0 + 1 < P;
+    const bool yin0 = y0 >= 0 && y0 < P, yin1 = y0 + 1 >= 0 && y0 + 1 < P;
+    const float k0 = xin0 ? __ldg(K + x0) : 0.f, k1 = xin1 ? __ldg(K + x0 + 1) : 0.f;
+    v00 = (yin0 && xin0) ? __ldg(img + (int64_t)y0 * P + x0) : 0.f;
+    v01 = (yin0 && xin1) ? __ldg(img + (int64_t)y0 * P + x0 + 1) : 0.f;
+    v10 = (yin1 && xin0) ? __ldg(img + (int64_t)(y0 + 1) * P + x0) : 0.f;
+    v11 = (yin1 && xin1) ? __ldg(img + (int64_t)(y0 + 1) * P + x0 + 1) : 0.f;
+    u00 = (yin0 && xin0) ? k0 - v00 : 0.f;
+    u01 = (yin0 && xin1) ? k1 - v01 : 0.f;
+    u10 = (yin1 && xin0) ? k0 - v10 : 0.f;
+    u11 = (yin1 && xin1) ? k1 - v11 : 0.f;
+  }
+  const float top = fmaf(fx.f, v01 - v00, v00);
+  const float bot = fmaf(fx.f, v11 - v10, v10);
+  *La = fmaf(fy.f, bot - top, top);
+  const float topb = fmaf(fx.f, u01 - u00, u00);
+  const float botb = fmaf(fx.f, u11 - u10, u10);
+  *Lb = fmaf(fy.f, botb - topb, topb);
 }
 
 // Integer r in [*lo, *hi] with x(r) = ax + r bx and y(r) = ay + r by both in [lim0, lim1]
@@ -142,6 +194,7 @@ __device__ __forceinline__ void column_support(double ax, double bx, double ay, 
 // One thread per column; the 32 columns of a warp walk the rows in lockstep (coalesced W
 // stores), with warp-uniform row ranges: no lane samples before the warp's first support row or
 // after its last, and rows where every lane's four taps are inside mu skip the per-tap tests.
+template <bool PAIRS>
 __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
   const int P = p.P, n = p.n;
   const int cpr_raw = blockIdx.x * blockDim.x + threadIdx.x;  // rotated-frame column c'
@@ -151,7 +204,9 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
   const int s = blockIdx.z;
   const int ai = job_lin / p.jobs_per_angle;
   const int job = job_lin - ai * p.jobs_per_angle;
-  const int a = p.a0 + ai;
+  int a, b;
+  entry_angles(p, p.a0 + ai, &a, &b);
+  if (a < 0) return;  // the whole CTA
   const double* Md = job_matrix(p, a, job, 0);  // rotate(-phi)
   const bool incident = p.has_in && job == 0;
   const float* mu = (incident ? p.mu_in : p.mu_out) + (int64_t)s * n * n;
@@ -228,6 +283,14 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
   const float w_after = (float)(acc + wrap);
   for (; r < P; ++r)
     if (valid) W[(int64_t)r * P] = w_after;
+  if (PAIRS && b >= 0 && valid) {
+    // the partner angle (phi + pi) rotates by a half turn more: its frame is this one turned
+    // about the centre, and its W at this frame's (r', c') is K[c'] - W[r'][c'] with
+    // K = sum_k U[k] + U[0]/2 + U[P-1]/2 (the reverse roll + cumsum of the same column)
+    double first = 0.0;
+    if (0 >= lo && 0 <= hi) first = 0.5 * (double)bilin_zero(mu, n, n, xc, yc);
+    p.kcol[(((int64_t)s * p.na + ai) * p.jobs_per_angle + job) * P + cpr] = (float)(acc + first + wrap);
+  }
 }
 
 // One CTA = a 32 x 32 pixel tile of one (slice, angle); thread t owns the four pixels
@@ -237,12 +300,16 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
 constexpr int RS_TILE = 32;
 constexpr int RS_PIX = 4;
 
-__global__ void __launch_bounds__(256) maps_resample_kernel(MapsPass p) {
+template <bool PAIRS>
+__global__ void __launch_bounds__(256, PAIRS ? 5 : 1) maps_resample_kernel(MapsPass p) {
   extern __shared__ float rs_mats[];  // [jobs_per_angle][6]
   const int n = p.n, P = p.P;
   const int ai = blockIdx.y;
   const int s = blockIdx.z;
-  const int a = p.a0 + ai;
+  int a, b;
+  entry_angles(p, p.a0 + ai, &a, &b);
+  if (a < 0) return;  // the whole CTA
+  const bool paired = PAIRS && b >= 0;
   const int J = p.jobs_per_angle;
   for (int t = threadIdx.x; t < 6 * J; t += blockDim.x) {
     const int job = t / 6;
@@ -259,17 +326,24 @@ __global__ void __launch_bounds__(256) maps_resample_kernel(MapsPass p) {
   const float* wbase = p.work + ((int64_t)s * p.na + ai) * J * (int64_t)P * P;
   const int64_t n2 = (int64_t)n * n;
 
-  // L of job `job` at the four pixels (pixels past the image edge are sampled, in bounds, and
-  // not stored)
-  auto sample4 = [&](int job, float* L) {
+  const float* kbase = p.kcol + ((int64_t)s * p.na + ai) * J * (int64_t)P;
+
+  // L of job `job` at the four pixels, and with a partner its L at the same pixels (pixels
+  // past the image edge are sampled, in bounds, and not stored)
+  auto sample4 = [&](int job, float* L, float* Lb) {
     const float* m = rs_mats + job * 6;
     const float* w = wbase + (int64_t)job * P * P;
+    const float* kc = kbase + (int64_t)job * P;
 #pragma unroll
     for (int k = 0; k < RS_PIX; ++k) {
       const float Y = (float)(i0 + 8 * k + p.e);
       const float x = fmaf(m[1], Y, fmaf(m[0], X, m[2]));
       const float y = fmaf(m[4], Y, fmaf(m[3], X, m[5]));
-      L[k] = bilin_square(w, P, x, y);
+      if (PAIRS && paired) {
+        bilin_square_pair(w, kc, P, x, y, &L[k], &Lb[k]);
+      } else {
+        L[k] = bilin_square(w, P, x, y);
+      }
     }
   };
   auto store4 = [&](int64_t plane, const float* v) {
@@ -286,60 +360,79 @@ __global__ void __launch_bounds__(256) maps_resample_kernel(MapsPass p) {
     }
   };
 
-  float L[RS_PIX];
+  float L[RS_PIX], Lb[RS_PIX];
   if (p.maps_dtype == CCT_DTYPE_FIELDS_F32) {
     // line-integral fields: plane 0 = L_in, plane 1 + d = L_out of detector d (n_sub == 1)
     const int64_t plane0 = ((int64_t)s * p.n_angles + a) * (1 + p.n_det);
+    const int64_t plane0b = ((int64_t)s * p.n_angles + b) * (1 + p.n_det);
     if (p.has_in) {
-      sample4(0, L);
+      sample4(0, L, Lb);
     } else {
 #pragma unroll
-      for (int k = 0; k < RS_PIX; ++k) L[k] = 0.f;
+      for (int k = 0; k < RS_PIX; ++k) L[k] = Lb[k] = 0.f;
     }
     store4(plane0, L);
+    if (paired) store4(plane0b, Lb);
     for (int d = 0; d < p.n_det; ++d) {
       if (p.has_out) {
-        sample4((p.has_in ? 1 : 0) + d, L);
+        sample4((p.has_in ? 1 : 0) + d, L, Lb);
       } else {
 #pragma unroll
-        for (int k = 0; k < RS_PIX; ++k) L[k] = 0.f;
+        for (int k = 0; k < RS_PIX; ++k) L[k] = Lb[k] = 0.f;
       }
       store4(plane0 + 1 + d, L);
+      if (paired) store4(plane0b + 1 + d, Lb);
     }
     return;
   }
-  float f_in[RS_PIX];
+  float f_in[RS_PIX], f_inb[RS_PIX];
   int job = 0;
   if (p.has_in) {
-    sample4(0, L);
+    sample4(0, L, Lb);
 #pragma unroll
-    for (int k = 0; k < RS_PIX; ++k) f_in[k] = expf(-L[k]);
+    for (int k = 0; k < RS_PIX; ++k) {
+      f_in[k] = expf(-L[k]);
+      f_inb[k] = paired ? expf(-Lb[k]) : 1.f;
+    }
     job = 1;
   } else {
 #pragma unroll
-    for (int k = 0; k < RS_PIX; ++k) f_in[k] = 1.f;
+    for (int k = 0; k < RS_PIX; ++k) f_in[k] = f_inb[k] = 1.f;
   }
   for (int d = 0; d < p.n_det; ++d) {
-    float f[RS_PIX];
+    float f[RS_PIX], fb[RS_PIX];
 #pragma unroll
-    for (int k = 0; k < RS_PIX; ++k) f[k] = f_in[k];
+    for (int k = 0; k < RS_PIX; ++k) {
+      f[k] = f_in[k];
+      fb[k] = f_inb[k];
+    }
     if (p.has_out) {
-      float sum[RS_PIX] = {0.f, 0.f, 0.f, 0.f};
+      float sum[RS_PIX] = {0.f, 0.f, 0.f, 0.f}, sumb[RS_PIX] = {0.f, 0.f, 0.f, 0.f};
       for (int q = 0; q < p.n_sub; ++q) {
-        sample4(job + d * p.n_sub + q, L);
+        sample4(job + d * p.n_sub + q, L, Lb);
 #pragma unroll
-        for (int k = 0; k < RS_PIX; ++k) sum[k] += expf(-L[k]);
+        for (int k = 0; k < RS_PIX; ++k) {
+          sum[k] += expf(-L[k]);
+          if (paired) sumb[k] += expf(-Lb[k]);
+        }
       }
       if (p.n_sub == 1) {
 #pragma unroll
-        for (int k = 0; k < RS_PIX; ++k) f[k] *= sum[k];
+        for (int k = 0; k < RS_PIX; ++k) {
+          f[k] *= sum[k];
+          fb[k] *= sumb[k];
+        }
       } else {
         const float ns = (float)p.n_sub;
 #pragma unroll
-        for (int k = 0; k < RS_PIX; ++k) f[k] *= sum[k] / ns;
+        for (int k = 0; k < RS_PIX; ++k) {
+          f[k] *= sum[k] / ns;
+          fb[k] *= sumb[k] / ns;
+        }
       }
     }
     store4(((int64_t)s * p.n_angles + a) * p.n_det + d, f);
+    if (paired) store4(((int64_t)s * p.n_angles + b) * p.n_det + d, fb);
   }
 }
 
@@ -353,7 +446,7 @@ int64_t maps_bytes_per_angle(const cct_maps_desc* d) {
   const int e = padded_edge(d->n);
   const int64_t P = d->n + 2 * e;
   const int64_t jobs = (d->has_in ? 1 : 0) + (d->has_out ? (int64_t)d->n_det * d->n_sub : 0);
-  return jobs * P * P * (int64_t)sizeof(float) * d->n_slices;
+  return jobs * (P * P + P) * (int64_t)sizeof(float) * d->n_slices;  // W planes + partner constants
 }
 
 int launch_maps(const cct_maps_desc* d, const float* mu_in, const float* mu_out, void* maps, void* work,
@@ -361,22 +454,34 @@ int launch_maps(const cct_maps_desc* d, const float* mu_in, const float* mu_out,
   const int e = padded_edge(d->n);
   const int P = d->n + 2 * e;
   const int64_t per_angle = maps_bytes_per_angle(d);
-  int per_pass = (int)std::min<int64_t>((int64_t)work_bytes / per_angle, (int64_t)d->n_angles);
+  const int entries = d->pairs != nullptr ? d->n_entries : d->n_angles;
+  if (entries < 1 || entries > d->n_angles) return CCT_ERR_VALUE;
+  int per_pass = (int)std::min<int64_t>((int64_t)work_bytes / per_angle, (int64_t)entries);
   if (per_pass < 1) return CCT_ERR_VALUE;
   MapsPass p;
   p.n = d->n; p.P = P; p.e = e; p.n_det = d->n_det; p.n_sub = d->n_sub;
   p.has_in = d->has_in; p.has_out = d->has_out; p.maps_dtype = d->maps_dtype; p.n_angles = d->n_angles;
   p.jobs_per_angle = (d->has_in ? 1 : 0) + (d->has_out ? d->n_det * d->n_sub : 0);
-  p.rot_in = d->rot_in; p.rot_out = d->rot_out; p.mu_in = mu_in; p.mu_out = mu_out;
+  p.rot_in = d->rot_in; p.rot_out = d->rot_out; p.pairs = d->pairs; p.mu_in = mu_in; p.mu_out = mu_out;
   p.work = reinterpret_cast<float*>(work); p.maps = maps;
-  for (int a0 = 0; a0 < d->n_angles; a0 += per_pass) {
+  p.kcol = p.work + (int64_t)per_pass * p.jobs_per_angle * (int64_t)P * P * d->n_slices;
+  for (int a0 = 0; a0 < entries; a0 += per_pass) {
     p.a0 = a0;
-    p.na = std::min(per_pass, d->n_angles - a0);
+    p.na = std::min(per_pass, entries - a0);
     const dim3 g1((P + 127) / 128, p.na * p.jobs_per_angle, d->n_slices);
-    maps_scan_kernel<<<g1, 128, 0, st>>>(p);
+    if (p.pairs != nullptr) {
+      maps_scan_kernel<true><<<g1, 128, 0, st>>>(p);
+    } else {
+      maps_scan_kernel<false><<<g1, 128, 0, st>>>(p);
+    }
     const int tiles = (d->n + RS_TILE - 1) / RS_TILE;
     const dim3 g2((unsigned)(tiles * tiles), p.na, d->n_slices);
-    maps_resample_kernel<<<g2, 256, 6 * p.jobs_per_angle * sizeof(float), st>>>(p);
+    const size_t smem = 6 * p.jobs_per_angle * sizeof(float);
+    if (p.pairs != nullptr) {
+      maps_resample_kernel<true><<<g2, 256, smem, st>>>(p);
+    } else {
+      maps_resample_kernel<false><<<g2, 256, smem, st>>>(p);
+    }
   }
   return CCT_OK;
 }

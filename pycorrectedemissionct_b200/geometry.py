@@ -118,3 +118,41 @@ def attenuation_rotations(
             for kk, a_s in enumerate(subs[dd]):
                 rot_out[ii, dd, kk] = _attenuation_pair(ad + a_s, True, size)
     return rot_in, rot_out, n_sub
+
+
+def half_turn_pairs(angles_rot_rad32: NDArray, tol: float = 1e-6) -> NDArray | None:
+    """(angle, partner) entries for the maps: partner = the angle that is ``angle + pi`` (within
+    ``tol`` radians, which covers the float32 rounding of the two angles), -1 when there is none.
+
+    Every angle appears once, as an entry's angle or as its partner.  None when no angle has a
+    partner.  The maps of a partner come from its angle's rotations turned by a half turn (an
+    exact permutation of the rotated lattice); the rotation angle then differs from the
+    partner's own float32 angle by at most ``tol``.
+    """
+    a = np.mod(np.array(angles_rot_rad32, ndmin=1, dtype=np.float64), 2 * np.pi)
+    order = np.argsort(a, kind="stable")
+    srt = a[order]
+    used = np.zeros(len(a), dtype=bool)
+    entries = []
+    for i in range(len(a)):
+        if used[i]:
+            continue
+        used[i] = True
+        partner = -1
+        target = np.mod(a[i] + np.pi, 2 * np.pi)
+        for t in (target, target - 2 * np.pi, target + 2 * np.pi):
+            k = int(np.searchsorted(srt, t - tol))
+            while k < len(srt) and srt[k] <= t + tol:
+                j = int(order[k])
+                if not used[j]:
+                    partner = j
+                    break
+                k += 1
+            if partner >= 0:
+                break
+        if partner >= 0:
+            used[partner] = True
+        entries.append((i, partner))
+    if all(p < 0 for _, p in entries):
+        return None
+    return np.array(entries, dtype=np.int32)

@@ -119,6 +119,33 @@ def test_solvers_match_reference(golden_cases, case, cuda):
     assert rel_l2(xp, g["pdhg_x"]) < TOL_RECON
 
 
+@pytest.mark.parametrize("maps_dtype", ["float32", "bfloat16", "fields-float32"])
+def test_half_turn_pairs_match_single_angles(maps_dtype, cuda):
+    """Maps from half-turn pairs (one rotation per direction for angles phi and phi + pi) against
+    every angle on its own: the entries' own angles are bit-identical, the partners within the
+    float32 rounding of the angles; with a permuted angle order and two detectors, one of them
+    finite (3 emitted sub-angles) where the maps dtype allows it."""
+    from pycorrectedemissionct_b200 import core, geometry, phantoms
+
+    n, n_ang = 72, 40
+    rad32 = np.array(phantoms.angles(n_ang), dtype=np.float32)[np.random.default_rng(3).permutation(n_ang)]
+    fields = maps_dtype == "fields-float32"
+    kw = dict(det_angles=[np.pi / 2, np.pi / 3])
+    if not fields:
+        kw.update(surfaces_mm2=[0.0, 10.0], distances_mm=[1.0, 50.0], sub_sampling=3)
+    mus = np.stack([phantoms.disk_attenuation(n, phantoms.slice_rng(77, k), 0.04) for k in range(2)])
+    mu = torch.from_numpy(mus).to(cuda)
+    paired = core.compute_maps(mu, 0.8 * mu, rad32, maps_dtype=maps_dtype, **kw)
+    single = core.compute_maps(mu, 0.8 * mu, rad32, maps_dtype=maps_dtype, half_turns=False, **kw)
+    pairs = geometry.half_turn_pairs(rad32)
+    assert pairs is not None and (pairs[:, 1] >= 0).all()
+    own, partner = pairs[:, 0], pairs[:, 1]
+    assert torch.equal(paired[:, own], single[:, own])
+    tol = 4e-3 if maps_dtype == "bfloat16" else 2e-6
+    got, want = paired[:, partner].double().cpu().numpy(), single[:, partner].double().cpu().numpy()
+    assert rel_l2(got, want) < tol
+
+
 def test_masked_solvers_match_reference(golden_cases, cuda):
     """MLEM, SIRT, PDHG and FISTA with b_mask and b_test_mask, and SART with b_mask, through the
     drop-in solvers: reconstruction, residuals and cross-validation residuals against the

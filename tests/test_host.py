@@ -147,3 +147,27 @@ def test_subset_ranges_for_any_angle_count():
             assert sum(sizes) == n_ang and max(sizes) - min(sizes) <= 1
             for r in ranges:
                 assert len(set((p[r] % k).tolist())) == 1
+
+
+def test_half_turn_pairs():
+    from pycorrectedemissionct_b200 import geometry, phantoms
+
+    a = np.array(phantoms.angles(720), dtype=np.float32)
+    p = geometry.half_turn_pairs(a)
+    assert p.shape == (360, 2) and (p[:, 1] == p[:, 0] + 360).all()
+    perm = np.random.default_rng(1).permutation(720)
+    q = geometry.half_turn_pairs(a[perm])
+    covered = np.concatenate([q[:, 0], q[q[:, 1] >= 0, 1]])
+    assert sorted(covered.tolist()) == list(range(720)) and (q[:, 1] >= 0).all()
+    for i, j in q:
+        d = np.mod(float(a[perm][j]) - float(a[perm][i]) - np.pi + np.pi, 2 * np.pi) - np.pi
+        assert abs(d) < 1e-6
+    # no partners: half-turn sets, odd counts
+    assert geometry.half_turn_pairs(np.array(phantoms.angles(10, 0, np.pi), dtype=np.float32)) is None
+    assert geometry.half_turn_pairs(np.array(phantoms.angles(9), dtype=np.float32)) is None
+    # some partners: angles 0, 90, 180 degrees -> (0, 180) paired, 90 alone
+    r = geometry.half_turn_pairs(np.array([0.0, np.pi / 2, np.pi], dtype=np.float32))
+    assert r.tolist() == [[0, 2], [1, -1]]
+    # a repeated angle pairs once
+    r = geometry.half_turn_pairs(np.array([0.0, 0.0, np.pi], dtype=np.float32))
+    assert r.tolist() == [[0, 2], [1, -1]]
