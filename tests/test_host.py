@@ -104,7 +104,7 @@ def test_validation_errors_map_to_value_error():
     md.has_in = 1
     assert lib.cct_maps_workspace_size(ctypes.byref(md), 2, ctypes.byref(out)) == _lib.CCT_OK
     p = geometry.padded_size(16)[1]
-    assert out.value == 2 * p * p * 4
+    assert out.value == 2 * (p * p + p) * 4  # W planes and the per-column constants of half-turn partners
 
 
 def test_compute_paths_need_cuda():
