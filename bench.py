@@ -9,7 +9,7 @@ reaches after 200 iterations (calibrated once, untimed).  Three paths are timed:
 * plain: MLEM from the default start;
 * learned: 10 MLEM iterations, the encoder-decoder on them (tensor-core kernels), MLEM to the
   residual (when trained weights are present);
-* subsets: ordered-subsets EM passes (60 subsets x 3 passes, then 30 x 2; each pass costs one
+* subsets: ordered-subsets EM passes (90 subsets x 2 passes, then 18 x 1; each pass costs one
   MLEM iteration), then MLEM to the residual, which judges every slice.
 
 ``value`` = slices converged per second over the timed steps of the headline path (``--method``,
@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=20240)
     ap.add_argument("--method", default="auto", choices=["auto", "plain", "learned", "subsets"],
                     help="headline path (auto: ordered subsets); the others are timed beside it")
-    ap.add_argument("--subsets", default="60:3,30:2", help="ordered-subsets schedule subsets:passes,...")
+    ap.add_argument("--subsets", default="90:2,18:1", help="ordered-subsets schedule subsets:passes,...")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fp-variant", default="auto", choices=["auto", "ldg", "tma"],
                     help="fp staging variant: the autotuner's choice (auto) or a fixed one")
@@ -223,8 +223,7 @@ def run_ours(a):
     maps = torch.empty((S, a.angles, 1, n, n), dtype=tdt, device=dev)  # recomputed by every step, in its order
     _, P = core.geometry.padded_size(n)
     # maps workspace: ~16 angles of the whole batch per pass (incident + emitted W of P^2 floats)
-    ws = torch.empty(max(core.DEFAULT_MAPS_WORKSPACE, 16 * 2 * P * P * 4 * S), dtype=torch.uint8, device=dev)
-    passes = -(-a.angles // max(1, ws.numel() // (2 * P * P * 4 * S)))
+    ws = torch.empty(max(core.DEFAULT_MAPS_WORKSPACE, 16 * 2 * (P * P + P) * 4 * S), dtype=torch.uint8, device=dev)
 
     def maps_natural():
         core.compute_maps(mu_in, mu_out, c.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
@@ -233,6 +232,7 @@ def run_ours(a):
         core.compute_maps(mu_in, mu_out, c_os.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
 
     maps_natural()
+    passes = core.compute_maps.last_passes  # two kernels per pass
     if a.fp_variant == "auto":
         variant = autotune.tune(c, x_true, maps)
     else:

@@ -8,6 +8,7 @@ there is no CPU path.
 from __future__ import annotations
 
 import ctypes
+from collections import OrderedDict
 
 import numpy as np
 import torch
@@ -287,6 +288,35 @@ class XrfCore:
         return int(c.value)
 
 
+_MAPS_TABLES: OrderedDict = OrderedDict()
+_MAPS_TABLES_MAX = 16
+
+
+def _maps_tables(device, n, angles_rad32, det_angles, surfaces_mm2, distances_mm, sub_sampling, half_turns):
+    """Device rotation tables (and half-turn pairs) of one geometry, built on the host once and
+    kept for the next calls with the same geometry (least recently used of 16 dropped)."""
+    a32 = np.ascontiguousarray(np.array(angles_rad32, ndmin=1, dtype=np.float32))
+
+    def key_of(v):
+        return None if v is None else tuple(np.array(v, ndmin=1, dtype=np.float64).tolist())
+
+    key = (str(device), int(n), a32.tobytes(), key_of(det_angles), key_of(surfaces_mm2), key_of(distances_mm),
+           int(sub_sampling), bool(half_turns))
+    hit = _MAPS_TABLES.get(key)
+    if hit is not None:
+        _MAPS_TABLES.move_to_end(key)
+        return hit
+    rot_in, rot_out, n_sub = geometry.attenuation_rotations(a32, det_angles, n, surfaces_mm2, distances_mm, sub_sampling)
+    rot_in_d = torch.from_numpy(np.ascontiguousarray(rot_in)).to(device)
+    rot_out_d = torch.from_numpy(np.ascontiguousarray(rot_out)).to(device)
+    pairs = geometry.half_turn_pairs(a32) if half_turns else None
+    pairs_d = None if pairs is None else torch.from_numpy(pairs).to(device)
+    _MAPS_TABLES[key] = (rot_in_d, rot_out_d, n_sub, pairs_d)
+    while len(_MAPS_TABLES) > _MAPS_TABLES_MAX:
+        _MAPS_TABLES.popitem(last=False)
+    return _MAPS_TABLES[key]
+
+
 def compute_maps(
     mu_in: torch.Tensor | None,
     mu_out: torch.Tensor | None,
@@ -317,24 +347,19 @@ def compute_maps(
     if maps_dtype not in MAPS_DTYPES:
         raise ValueError(f"maps_dtype must be one of {sorted(MAPS_DTYPES)}")
     tdt, cdt = MAPS_DTYPES[maps_dtype]
-    rot_in, rot_out, n_sub = geometry.attenuation_rotations(
-        angles_rad32, det_angles, n, surfaces_mm2, distances_mm, sub_sampling
+    rot_in_d, rot_out_d, n_sub, pairs_d = _maps_tables(
+        device, n, angles_rad32, det_angles, surfaces_mm2, distances_mm, sub_sampling, half_turns
     )
-    n_ang, n_det = rot_out.shape[0], rot_out.shape[1]
-    rot_in_d = torch.from_numpy(np.ascontiguousarray(rot_in)).to(device)
-    rot_out_d = torch.from_numpy(np.ascontiguousarray(rot_out)).to(device)
+    n_ang, n_det = rot_out_d.shape[0], rot_out_d.shape[1]
     desc = _lib.MapsDesc()
     desc.n, desc.n_angles, desc.n_det, desc.n_slices = n, n_ang, n_det, s
     desc.n_sub, desc.maps_dtype = n_sub, cdt
     desc.has_in, desc.has_out = int(mu_in is not None), int(mu_out is not None)
     desc.rot_in, desc.rot_out = rot_in_d.data_ptr(), rot_out_d.data_ptr()
-    pairs = geometry.half_turn_pairs(angles_rad32) if half_turns else None
-    pairs_d = None
     entries = n_ang
-    if pairs is not None:
-        pairs_d = torch.from_numpy(pairs).to(device)
-        desc.pairs, desc.n_entries = pairs_d.data_ptr(), len(pairs)
-        entries = len(pairs)
+    if pairs_d is not None:
+        desc.pairs, desc.n_entries = pairs_d.data_ptr(), pairs_d.shape[0]
+        entries = pairs_d.shape[0]
     need = ctypes.c_size_t(0)
     _lib.call("cct_maps_workspace_size", ctypes.byref(desc), 1, ctypes.byref(need))
     if workspace is None:
@@ -352,8 +377,8 @@ def compute_maps(
         "cct_compute_maps", ctypes.byref(desc), _ptr(mu_in), _ptr(mu_out), maps.data_ptr(), workspace.data_ptr(),
         workspace.numel() * workspace.element_size(), stream_handle(device),
     )
-    # torch's caching allocator reuses the freed matrices / workspace only for work queued
-    # later on the same stream, so dropping them here is safe
+    # torch's caching allocator reuses a workspace allocated here only for work queued later on
+    # the same stream, so dropping it here is safe
     return maps
 
 
