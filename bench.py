@@ -308,13 +308,22 @@ def run_ours(a):
         solve_to_tol(learned, False, max_iters)
         return float((learned.iterations.float() + N_ITERATES).mean().item())
 
+    phase_ms = []  # (maps, passes, judge) of timed ordered-subsets steps
+
     def step_subsets(timed: bool) -> float:
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record()
         maps_subsets()
+        ev[1].record()
         launches[0] += 2 * passes + launches_os_pass
         subsets.reset()
         subsets.run()
+        ev[2].record()
         judge.reset(subsets.x)
         solve_to_tol(judge, False, max_iters, block=2)
+        ev[3].record()
+        if timed:
+            phase_ms.append(ev)
         return float((judge.iterations.float() + subsets.passes).mean().item())
 
     def timed_steps(fn, k: int) -> tuple[float, float]:
@@ -420,9 +429,11 @@ def run_ours(a):
         },
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            # DRAM bytes per launch from one ncu capture of this kernel on 2 slices (1.4366 GB), scaled
-            # by the slices per launch; only for the capture's own configuration
-            "traffic": (1.4366e9 / 2 * S) if (n == 512 and a.angles == 720 and a.maps_dtype == "float32") else None,
+            # DRAM read + write bytes per launch from one ncu capture of each variant on 2 slices
+            # (fp_tma_kernel 1.4616 GB, fp_kernel 1.4749 GB), scaled by the slices per launch;
+            # only for the captures' own configuration
+            "traffic": ((1.4616e9 if variant else 1.4749e9) / 2 * S)
+            if (n == 512 and a.angles == 720 and a.maps_dtype == "float32") else None,
             "kernel": ("fp_tma_kernel" if variant else "fp_kernel") + "<MLEM> (attenuated fp + ratio + KL residual)",
             "peak_source": peak_src, "fp_launch_us": fp_avg_s * 1e6, "bp_launch_us": bp_avg_s * 1e6,
             "algorithmic_bytes_per_launch": fp_bytes,
@@ -431,6 +442,10 @@ def run_ours(a):
         "gpu_launches": head_launches,
         "clocks": clk,
     }
+    if headline == "subsets" and phase_ms:
+        torch.cuda.synchronize(dev)
+        ph = np.array([[e[i].elapsed_time(e[i + 1]) for i in range(3)] for e in phase_ms])
+        line["phases_ms_per_step"] = dict(zip(("compute_maps", "subset_passes", "judge_mlem"), ph.mean(axis=0).tolist()))
     for name, r in results.items():
         line[name] = dict(r, solver=solver_desc[name])
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
