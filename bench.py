@@ -261,8 +261,19 @@ def run_ours(a):
         net.load(WEIGHTS)
     elif a.method == "learned":
         raise FileNotFoundError(f"no trained warm-start weights at {WEIGHTS}")
-    learned = engine.BatchedSolver(c, maps, b, "mlem", tolerance=tol_np) if net is not None else None
-    first = engine.BatchedSolver(c, maps, b, "mlem") if net is not None else None
+    learned = first = None
+    k_l = net.pass_subsets(a.angles) if net is not None else 0
+    c_l, b_l, os_l = c, b, None
+    if k_l > 0:
+        # the network's inputs are snapshots of one ordered-subsets pass: its own angle order
+        perm_l_t = torch.from_numpy(engine.subset_permutation(a.angles, [k_l])).to(dev)
+        c_l = core.XrfCore(n, angles[perm_l_t.cpu().numpy()], device=dev)
+        c_l.variant = variant
+        b_l = b[:, :, perm_l_t].contiguous()
+        os_l = engine.OrderedSubsets(c_l, maps, b_l, [(k_l, 1)])
+    if net is not None:
+        learned = engine.BatchedSolver(c_l, maps, b_l, "mlem", tolerance=tol_np)
+        first = engine.BatchedSolver(c_l, maps, b_l, "mlem")
     subsets = engine.OrderedSubsets(c_os, maps, b_os, schedule)
     judge = engine.BatchedSolver(c_os, maps, b_os, "mlem", tolerance=tol_np, x_shared=subsets.x)
     launches_os_pass = sum(k * 3 * p for k, p in schedule)
@@ -296,17 +307,27 @@ def run_ours(a):
         return float(plain.iterations.float().mean().item())
 
     def step_learned(timed: bool) -> float:
-        maps_natural()
-        launches[0] += 2 * passes
-        first.reset()
-        its = tw.first_iterates(first)
-        bpn = tw.normalized_backprojection(c, b, first.tau)
+        if os_l is not None:
+            core.compute_maps(mu_in, mu_out, c_l.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
+            launches[0] += 2 * passes
+            os_l.reset()
+            its = tw.pass_snapshots(os_l)
+            launches[0] += 3 * k_l  # one pass: fp, residual and bp per subset
+            first_passes = 1
+        else:
+            maps_natural()
+            launches[0] += 2 * passes
+            first.reset()
+            its = tw.first_iterates(first)
+            launches[0] += 3 * N_ITERATES
+            first_passes = N_ITERATES
+        bpn = tw.normalized_backprojection(c_l, b_l, first.tau)
         scale = tw.slice_means(its[-1])
         x0 = net.predict(its + [bpn], base=its[-1], slice_scale=scale)
-        launches[0] += 3 * N_ITERATES + 2 + 90  # 10 iterations, bp + ratio, network (~90 kernels)
+        launches[0] += 2 + 90  # bp + ratio, network (~90 kernels)
         learned.reset(x0)
         solve_to_tol(learned, False, max_iters)
-        return float((learned.iterations.float() + N_ITERATES).mean().item())
+        return float((learned.iterations.float() + first_passes).mean().item())
 
     phase_ms = []  # (maps, passes, judge) of timed ordered-subsets steps
 
@@ -386,6 +407,9 @@ def run_ours(a):
         if headline == "subsets":
             torch.index_select(b, 2, perm_t, out=b_os)
             subsets.set_data(b_os)
+        if headline == "learned" and os_l is not None:
+            torch.index_select(b, 2, perm_l_t, out=b_l)
+            os_l.set_data(b_l)
         its = paths[headline](False)
         x_h.copy_(result.x, non_blocking=True)
         return its
@@ -411,7 +435,9 @@ def run_ours(a):
     achieved = fp_bytes / fp_avg_s / 1e9
     solver_desc = {
         "plain": "plain MLEM (cold start)",
-        "learned": "MLEM warm-started by the learned encoder-decoder (10 MLEM iterations, network, MLEM to the residual)",
+        "learned": ("MLEM warm-started by the learned encoder-decoder ("
+                    + (f"10 snapshots of one ordered-subsets pass over {k_l} subsets" if k_l else "10 MLEM iterations")
+                    + ", network, MLEM to the residual)"),
         "subsets": f"MLEM warm-started by ordered-subsets EM passes {schedule} (subsets, passes), then MLEM to the residual",
     }
     line = {

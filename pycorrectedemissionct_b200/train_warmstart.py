@@ -60,11 +60,18 @@ def first_iterates(solver: BatchedSolver, count: int = N_ITERATES) -> list[torch
     return its
 
 
-def subsets_iterates(os_: OrderedSubsets, count: int = N_ITERATES) -> list[torch.Tensor]:
-    """Run `count` passes of a one-level ordered-subsets schedule, keeping the iterate after each."""
+def pass_snapshots(os_: OrderedSubsets, count: int = N_ITERATES) -> list[torch.Tensor]:
+    """One pass of a one-level ordered-subsets schedule of k subsets, keeping a copy of the
+    iterate after every (k // count)-th subset step (the last one after the whole pass)."""
+    subsets = os_.levels[0]
+    k = len(subsets)
+    stride = max(1, k // count)
     its = []
-    for _ in range(count):
-        os_.run()
+    for t, sm in enumerate(subsets):
+        sm.step()
+        if t + 1 == k or ((t + 1) % stride == 0 and len(its) < count - 1):
+            its.append(os_.x.clone())
+    while len(its) < count:
         its.append(os_.x.clone())
     return its
 
@@ -98,13 +105,13 @@ def generate_pairs(n_slices: int, n: int = 256, n_angles: int = 360, seed: int =
     device = core.require_cuda(device)
     helper = net if net is not None else WarmStartNet(device=device)
     inputs, targets = [], []
-    n_sub = helper.first_subsets
+    n_sub = helper.pass_subsets(n_angles)
     for s0 in range(0, n_slices, batch):
         seeds = [seed + k for k in range(s0, min(n_slices, s0 + batch))]
         c, maps, b, _ = synth_batch(n, n_angles, seeds, mu_max, peak, device, subsets=n_sub)
         solver = BatchedSolver(c, maps, b, "mlem")
         if n_sub > 0:
-            its = subsets_iterates(OrderedSubsets(c, maps, b, [(n_sub, 1)]))
+            its = pass_snapshots(OrderedSubsets(c, maps, b, [(n_sub, 1)]))
             bpn = normalized_backprojection(c, b, solver.tau)
             solver.run(target_iterations, check_every=target_iterations, use_graph=False)
         else:
@@ -152,14 +159,16 @@ def train(net: WarmStartNet, inputs: torch.Tensor, targets: torch.Tensor, steps:
 
 def warm_started_solve(net: WarmStartNet, c: core.XrfCore, maps: torch.Tensor, b: torch.Tensor, tolerance,
                        max_iterations: int = 400, check_every: int = 5, history_len: int = 0):
-    """10 plain MLEM iterations (or ordered-subsets passes, by the network's inputs) -> network ->
-    MLEM from the prediction until `tolerance`.  With ordered-subsets inputs, ``c``, ``maps`` and
-    ``b`` must be in ``subset_permutation(A, [net.first_subsets])`` angle order.
+    """10 plain MLEM iterations (or 10 snapshots of one ordered-subsets pass, by the network's
+    inputs) -> network -> MLEM from the prediction until `tolerance`.  With ordered-subsets inputs,
+    ``c``, ``maps`` and ``b`` must be in ``subset_permutation(A, [net.pass_subsets(A)])`` angle
+    order.
 
     Returns (solver, total full-data passes per slice as a numpy array)."""
     first = BatchedSolver(c, maps, b, "mlem")
-    if net.first_subsets > 0:
-        its = subsets_iterates(OrderedSubsets(c, maps, b, [(net.first_subsets, 1)]))
+    n_sub = net.pass_subsets(c.n_angles)
+    if n_sub > 0:
+        its = pass_snapshots(OrderedSubsets(c, maps, b, [(n_sub, 1)]))
     else:
         its = first_iterates(first)
     bpn = normalized_backprojection(c, b, first.tau)
@@ -167,7 +176,7 @@ def warm_started_solve(net: WarmStartNet, c: core.XrfCore, maps: torch.Tensor, b
     x0 = net.predict(its + [bpn], base=its[-1], slice_scale=scale)
     solver = BatchedSolver(c, maps, b, "mlem", tolerance=tolerance, x0=x0, history_len=history_len)
     solver.run(max_iterations, check_every=check_every)
-    return solver, solver.iterations.cpu().numpy() + N_ITERATES
+    return solver, solver.iterations.cpu().numpy() + (1 if n_sub > 0 else N_ITERATES)
 
 
 def main():
@@ -181,8 +190,9 @@ def main():
     ap.add_argument("--target-iterations", type=int, default=500)
     ap.add_argument("--additive", action="store_true", help="additive instead of log-ratio (multiplicative) targets")
     ap.add_argument("--log-floor", type=float, default=1e-3, help="floor of the log-ratio target, in slice means")
-    ap.add_argument("--first-subsets", type=int, default=0,
-                    help="inputs from ordered-subsets passes over this many subsets (0: MLEM iterates)")
+    ap.add_argument("--pass-angles", type=int, default=0,
+                    help="inputs: 10 snapshots of one ordered-subsets pass over subsets of this many angles "
+                         "(0: the first 10 MLEM iterates)")
     ap.add_argument("--out", default="warmstart.pt")
     a = ap.parse_args()
     dev = core.require_cuda()
@@ -190,7 +200,7 @@ def main():
     net = WarmStartNet(seed=0, device=dev)
     net.multiplicative = not a.additive
     net.log_floor = a.log_floor
-    net.first_subsets = a.first_subsets
+    net.pass_angles = a.pass_angles
     inputs, targets = generate_pairs(a.slices, a.n, a.angles, target_iterations=a.target_iterations, device=dev, net=net)
     torch.cuda.synchronize()
     t1 = time.time()

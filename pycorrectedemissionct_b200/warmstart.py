@@ -87,11 +87,15 @@ class WarmStartNet:
         # log((x_target + floor * scale) / (x10 + floor * scale))
         self.multiplicative = False
         self.log_floor = 1e-2
-        # inputs: 0 = the first 10 MLEM iterates; k > 0 = the iterates after each of the first 10
-        # ordered-subsets passes over k subsets
-        self.first_subsets = 0
+        # inputs: 0 = the first 10 MLEM iterates; k > 0 = 10 snapshots of the iterate taken during
+        # one ordered-subsets pass over subsets of k angles each (A // k subsets)
+        self.pass_angles = 0
 
     # ------------------------------------------------------------------ helpers
+    def pass_subsets(self, n_angles: int) -> int:
+        """Subsets of the one ordered-subsets pass that makes the inputs (0: MLEM inputs)."""
+        return 0 if self.pass_angles <= 0 else min(n_angles, max(N_ITERATES, n_angles // self.pass_angles))
+
     def n_params(self) -> int:
         return sum(l.w.numel() + l.b.numel() for l in self.layers.values())
 
@@ -254,7 +258,7 @@ class WarmStartNet:
         """BF16 weights, FP32 biases and the target parameterisation."""
         st = {k: (l.w.to(BF16).cpu(), l.b.cpu()) for k, l in self.layers.items()}
         st.update(step=self.step_count, multiplicative=self.multiplicative, log_floor=self.log_floor,
-                  first_subsets=self.first_subsets)
+                  pass_angles=self.pass_angles)
         torch.save(st, path)
 
     def load(self, path: str) -> None:
@@ -266,4 +270,4 @@ class WarmStartNet:
         self.step_count = int(st.get("step", 0))
         self.multiplicative = bool(st.get("multiplicative", False))
         self.log_floor = float(st.get("log_floor", 1e-2))
-        self.first_subsets = int(st.get("first_subsets", 0))
+        self.pass_angles = int(st.get("pass_angles", 0))
