@@ -119,15 +119,15 @@ def test_solvers_match_reference(golden_cases, case, cuda):
     assert rel_l2(xp, g["pdhg_x"]) < TOL_RECON
 
 
-@pytest.mark.parametrize("maps_dtype", ["float32", "bfloat16", "fields-float32"])
-def test_half_turn_pairs_match_single_angles(maps_dtype, cuda):
+@pytest.mark.parametrize("n,maps_dtype", [(72, "float32"), (45, "float32"), (72, "bfloat16"), (72, "fields-float32")])
+def test_half_turn_pairs_match_single_angles(n, maps_dtype, cuda):
     """Maps from half-turn pairs (one rotation per direction for angles phi and phi + pi) against
     every angle on its own: the entries' own angles are bit-identical, the partners within the
     float32 rounding of the angles; with a permuted angle order and two detectors, one of them
     finite (3 emitted sub-angles) where the maps dtype allows it."""
     from pycorrectedemissionct_b200 import core, geometry, phantoms
 
-    n, n_ang = 72, 40
+    n_ang = 40
     rad32 = np.array(phantoms.angles(n_ang), dtype=np.float32)[np.random.default_rng(3).permutation(n_ang)]
     fields = maps_dtype == "fields-float32"
     kw = dict(det_angles=[np.pi / 2, np.pi / 3])
