@@ -1,12 +1,13 @@
 """Solvers with the reference's interface running device-resident on the B200 projectors.
 
 Mirrors ``corrct``: ``src/corrct/solvers.py`` — ``SolutionInfo`` (``:161-201``),
-``MLEM`` (``:634-805``), ``SIRT`` (``:808-984``), ``PDHG`` (``:987-1206``, KL or l2
-data term, optional isotropic TV2D), ``SART`` (``:473-631``) and ``FISTA``
-(``:1209-1513``, l2 data term, no regularizer).  ``__call__(A, b, iterations, x0,
-lower_limit, upper_limit, x_mask, ...)`` returns ``(x, SolutionInfo)`` like the
-reference.  MLEM, SIRT and PDHG run the fused ``cct_*_step`` kernels (the update
-equations of the reference); SART and FISTA drive the projector's device fp / bp.
+``MLEM`` (``:634-805``), ``SIRT`` (``:808-984``), ``PDHG`` (``:987-1206``, KL data term
+with isotropic TV2D), ``SART`` (``:473-631``) and ``FISTA`` (``:1209-1513``, l2 data term,
+no regularizer).  ``__call__(A, b, iterations, x0, lower_limit, upper_limit, x_mask, b_mask,
+b_test_mask, ...)`` returns ``(x, SolutionInfo)`` like the reference, with the data masks of
+``Solver._initialize_b_masks`` (``:333-343``) and the cross-validation residuals.  MLEM, SIRT
+and PDHG run the fused ``cct_*_step`` kernels (the update equations of the reference); SART and
+FISTA drive the projector's device fp / bp.
 ``A`` must be one of this package's projectors: the unchanged corrct solvers
 remain available for any other operator (including these projectors).
 """
