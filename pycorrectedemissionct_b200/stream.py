@@ -135,7 +135,9 @@ class RaggedStream:
         seconds from the start of the stream to the slice's completion).  Returns totals."""
         torch.cuda.synchronize(self.device)
         t0 = time.perf_counter()
-        ws = torch.empty(_core.DEFAULT_MAPS_WORKSPACE, dtype=torch.uint8, device=self.device)
+        # maps workspace: 4x the default, so that the few slices of a small group still fill the
+        # GPU with enough angles per pass (outside the wave budget)
+        ws = torch.empty(4 * _core.DEFAULT_MAPS_WORKSPACE, dtype=torch.uint8, device=self.device)
         for wave in self.waves(jobs):
             groups = {}
             for j in wave:
