@@ -29,6 +29,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -92,8 +93,10 @@ class ClockSampler:
     )
 
     def __init__(self, index: int):
-        out = os.path.join(ROOT, "gpurun_out")
-        self.path = os.path.join(out, f"clocks_rank{index}.csv") if os.path.isdir(out) else f"/tmp/cct_clocks_{os.getpid()}.csv"
+        # the raw samples go to $CCT_CLOCKS_DIR (default: the temp directory); the summary is in
+        # the JSON line
+        out = os.environ.get("CCT_CLOCKS_DIR", tempfile.gettempdir())
+        self.path = os.path.join(out, f"cct_clocks_rank{index}_{os.getpid()}.csv")
         self.index = index
         self.proc = None
 
