@@ -171,3 +171,24 @@ def test_half_turn_pairs():
     # a repeated angle pairs once
     r = geometry.half_turn_pairs(np.array([0.0, 0.0, np.pi], dtype=np.float32))
     assert r.tolist() == [[0, 2], [1, -1]]
+
+
+def test_bench_reference_arm_contract():
+    """bench.py --impl reference (the oracle port on the host cores) prints one JSON line with the
+    contract's keys, on a tiny workload."""
+    import json
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run(
+        [sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "1",
+         "--n", "16", "--angles", "8", "--slices", "1", "--cpu-sample-angles", "4"],
+        capture_output=True, text=True, timeout=600, check=True,
+    )
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "slices/s" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"] == {"value": line["value"], "unit": "slices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    for key in ("metric", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling", "dtype", "config"):
+        assert key in line
