@@ -58,6 +58,23 @@ def default_schedule(n_angles: int, angles_per_subset: int = 12) -> list[tuple[i
     return [(k, 3), (k // 2, 2)]
 
 
+def pack_waves(jobs: list[Job], memory_budget: int, maps_bytes: int = 4) -> list[list[Job]]:
+    """Jobs sorted by (method, n, angles) and cut into consecutive waves of at most
+    ``memory_budget`` bytes (``job_bytes``); a job larger than the budget is a wave of its own."""
+    order = sorted(jobs, key=lambda j: (j.method, j.n, len(j.angles)))
+    out, cur, used = [], [], 0
+    for j in order:
+        need = job_bytes(j, maps_bytes)
+        if cur and used + need > memory_budget:
+            out.append(cur)
+            cur, used = [], 0
+        cur.append(j)
+        used += need
+    if cur:
+        out.append(cur)
+    return out
+
+
 class _Group:
     def __init__(self, jobs: list[Job], device, maps_dtype: str, schedule, warm: bool, workspace: torch.Tensor):
         j0 = jobs[0]
@@ -116,19 +133,7 @@ class RaggedStream:
         self.launches = 0
 
     def waves(self, jobs: list[Job]) -> list[list[Job]]:
-        mb = 2 if self.maps_dtype == "bfloat16" else 4
-        order = sorted(jobs, key=lambda j: (j.method, j.n, len(j.angles)))
-        out, cur, used = [], [], 0
-        for j in order:
-            need = job_bytes(j, mb)
-            if cur and used + need > self.memory_budget:
-                out.append(cur)
-                cur, used = [], 0
-            cur.append(j)
-            used += need
-        if cur:
-            out.append(cur)
-        return out
+        return pack_waves(jobs, self.memory_budget, 2 if self.maps_dtype == "bfloat16" else 4)
 
     def solve(self, jobs: list[Job], max_iterations: int = 1000) -> dict:
         """Solve every job (results in ``job.x``, ``job.iterations_done``, ``job.finished_s`` =

@@ -192,3 +192,31 @@ def test_bench_reference_arm_contract():
     assert line["e2e"] == {"value": line["value"], "unit": "slices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     for key in ("metric", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling", "dtype", "config"):
         assert key in line
+
+
+def test_pack_waves_and_default_schedule():
+    from pycorrectedemissionct_b200 import engine, stream
+
+    rng = np.random.default_rng(4)
+    jobs = []
+    for k in range(40):
+        n = int(rng.choice([64, 128, 256]))
+        a = int(rng.integers(30, 200))
+        jobs.append(stream.Job(n, np.linspace(0, 2 * np.pi, a, endpoint=False), None, None, np.zeros((a, n), np.float32),
+                               method="mlem" if k % 2 else "sirt"))
+    budget = 40 << 20
+    waves = stream.pack_waves(jobs, budget)
+    assert sorted(id(j) for w in waves for j in w) == sorted(id(j) for j in jobs)
+    for w in waves:
+        assert len(w) == 1 or sum(stream.job_bytes(j) for j in w) <= budget
+    flat = [j for w in waves for j in w]
+    keys = [(j.method, j.n, len(j.angles)) for j in flat]
+    assert keys == sorted(keys)
+    # a job above the budget forms its own wave
+    assert stream.pack_waves(jobs[:3], 1) == [[j] for j in sorted(jobs[:3], key=lambda j: (j.method, j.n, len(j.angles)))]
+    # schedules: even subset counts of ~12 angles, the second level dividing the first
+    for a in (90, 360, 720, 1440, 37):
+        (k1, p1), (k2, p2) = stream.default_schedule(a)
+        assert k1 % 2 == 0 and k1 % k2 == 0 and (p1, p2) == (3, 2)
+        engine.subset_permutation(a, [k1, k2])
+    assert stream.default_schedule(720) == [(60, 3), (30, 2)]

@@ -231,3 +231,22 @@ def test_port_finite_surface_detectors_match_reference_golden():
                              detector_distances_mm=g["det_distances"], emitted_sub_sampling=int(g["sub_sampling"]))
     assert rel_l2(maps, g["maps"]) < 1e-13
     assert rel_l2(port.fp_xrf(g["x"], g["maps"], deg32), g["fp_att"]) < 1e-13
+
+
+def test_half_turn_line_integral_is_the_reverse_scan():
+    """The identity behind the maps kernels' half-turn pairs: the line integral at phi + pi is the
+    rotate-back of K - W_phi, K[c] = sum_r U[r][c] + (U[0][c] + U[P-1][c]) / 2, with W_phi the
+    roll + cumsum of halves at phi (``_projector_backends.py:68-73``)."""
+    n = 24
+    mu = np.zeros((n, n))
+    mu[5:15, 8:20] = 0.05
+    mu[12:20, 3:9] = 0.02
+    edge, _ = port.padded_size(n)
+    for phi in (0.3, 1.2, 2.9):
+        deg = np.rad2deg(phi)
+        u = skr.rotate(np.pad(mu, edge), -deg, order=1, clip=False)
+        w = np.cumsum((u + np.roll(u, 1, axis=-2)) / 2, axis=-2)
+        k = u.sum(axis=0) + (u[0] + u[-1]) / 2
+        l_pair = skr.rotate(k[None, :] - w, deg, order=1, clip=False)[edge:-edge, edge:-edge]
+        l_ref = -np.log(port.compute_attenuation(mu, phi + np.pi))
+        np.testing.assert_allclose(l_pair, l_ref, atol=1e-12)
