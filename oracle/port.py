@@ -399,6 +399,27 @@ def b_masks(b: NDArray, b_mask, b_test_mask):
     return b_mask, b_test_mask
 
 
+def power_method(fp, bp, b: NDArray, iterations: int = 5) -> float:
+    """l2 norm of the operator by power iterations from a ``np.random.rand`` start (``solvers.py:26-57``)."""
+    x = np.random.rand(*b.shape).astype(b.dtype)
+    x /= np.linalg.norm(x)
+    x = bp(x)
+    x_norm = np.linalg.norm(x)
+    L = x_norm
+    for _ in range(iterations):
+        x /= x_norm
+        x = bp(fp(x))
+        x_norm = np.linalg.norm(x)
+        L = np.sqrt(x_norm)
+    return float(L)
+
+
+def lipschitz_scaling(fp, bp, b: NDArray, reg_tau: float = 0.0, relax_tau: float = 1.0, relax_sigma: float = 1.0):
+    """``compute_Lipschitz_scaling`` (``solvers.py:120-158``): scalar (sigma, tau)."""
+    L = power_method(fp, bp, b)
+    return relax_sigma / L, relax_tau / (L + reg_tau)
+
+
 def mlem(fp, bp, b: NDArray, iterations: int, x0=None, tolerance=None, lower_limit=None, upper_limit=None, x_mask=None,
          b_mask=None, b_test_mask=None, residuals_cv=None):
     """MLEM update loop of ``solvers.py:725-805`` (KL data term, no background).
@@ -454,7 +475,7 @@ def sirt(fp, bp, b: NDArray, iterations: int, x_shape, relaxation: float = 1.95,
 
 
 def pdhg_kl_tv(fp, bp, b: NDArray, iterations: int, x_shape, lam: float, relaxation: float = 0.95, lower_limit=None, upper_limit=None, x_mask=None,
-               x0=None, b_mask=None, b_test_mask=None, tolerance=None, residuals=None, residuals_cv=None):
+               x0=None, b_mask=None, b_test_mask=None, tolerance=None, residuals=None, residuals_cv=None, precondition: bool = True):
     """PDHG with KL data term and isotropic TV2D (``solvers.py:1099-1206``).
 
     Dual KL prox ``data_terms.py:682-692``; TV via ``Regularizer_Grad``
@@ -465,12 +486,15 @@ def pdhg_kl_tv(fp, bp, b: NDArray, iterations: int, x_shape, lam: float, relaxat
     """
     b = np.array(b)
     b_mask, b_test_mask = b_masks(b, b_mask, b_test_mask)
-    sigma, tau = diagonal_scaling(fp, bp, b, x_shape, reg_tau=4.0, relax_tau=relaxation, relax_sigma=relaxation, x_mask=x_mask, b_mask=b_mask)
-    x = np.zeros(x_shape, dtype=tau.dtype) if x0 is None else np.array(x0).copy()
+    if precondition:
+        sigma, tau = diagonal_scaling(fp, bp, b, x_shape, reg_tau=4.0, relax_tau=relaxation, relax_sigma=relaxation, x_mask=x_mask, b_mask=b_mask)
+    else:
+        sigma, tau = lipschitz_scaling(fp, bp, b, reg_tau=4.0, relax_tau=relaxation, relax_sigma=relaxation)
+    x = np.zeros(x_shape, dtype=b.dtype) if x0 is None else np.array(x0).copy()
     x_relax = x.copy()
     sigma_data = 4 * sigma * np.fmax(b, 0.0)
     p = np.zeros_like(b)
-    q = np.zeros((2, *x_shape), dtype=tau.dtype)
+    q = np.zeros((2, *x_shape), dtype=x.dtype)
     track = tolerance is not None or b_test_mask is not None
     for _ in range(iterations):
         p += fp(x_relax) * sigma
@@ -502,12 +526,16 @@ def pdhg_kl_tv(fp, bp, b: NDArray, iterations: int, x_shape, lam: float, relaxat
 
 
 def fista(fp, bp, b: NDArray, iterations: int, x_shape, relaxation: float = 1.0, x0=None, lower_limit=None, upper_limit=None,
-          x_mask=None, b_mask=None, b_test_mask=None, tolerance=None, restart_period=None, residuals=None, residuals_cv=None):
-    """FISTA, l2 data term, diagonal preconditioning, no regularizer (``solvers.py:1395-1513``)."""
+          x_mask=None, b_mask=None, b_test_mask=None, tolerance=None, restart_period=None, residuals=None, residuals_cv=None,
+          precondition: bool = True):
+    """FISTA, l2 data term, no regularizer (``solvers.py:1395-1513``); diagonal or Lipschitz scaling."""
     b = np.array(b)
     b_mask, b_test_mask = b_masks(b, b_mask, b_test_mask)
-    sigma, tau = diagonal_scaling(fp, bp, b, x_shape, relax_tau=relaxation, x_mask=x_mask, b_mask=b_mask)
-    x = np.zeros(x_shape, dtype=tau.dtype) if x0 is None else np.array(x0).copy()
+    if precondition:
+        sigma, tau = diagonal_scaling(fp, bp, b, x_shape, relax_tau=relaxation, x_mask=x_mask, b_mask=b_mask)
+    else:
+        sigma, tau = lipschitz_scaling(fp, bp, b, relax_tau=relaxation)
+    x = np.zeros(x_shape, dtype=b.dtype) if x0 is None else np.array(x0).copy()
     if x_mask is not None:
         x *= x_mask
     y = x.copy()

@@ -46,6 +46,9 @@ class BatchedSolver:
         after ``_initialize_b_masks``.
     x_shared : (S, n, n) tensor or None
         MLEM only: use this tensor as the iterate, in place and without initialising it.
+    scaling : (sigma, tau) or None
+        SIRT / PDHG: scalar step sizes instead of the diagonal scaling (the reference's
+        ``precondition=False``).
     joint_stop : bool
         The S slices are one 3-D volume: a single stopping test on the residual summed over the
         slices (the reference's norm over the whole volume, compared with ``tolerance[0]``); the
@@ -72,6 +75,7 @@ class BatchedSolver:
         x_shared: torch.Tensor | None = None,
         b_mask: torch.Tensor | None = None,
         b_test_mask: torch.Tensor | None = None,
+        scaling: tuple[float, float] | None = None,
     ):
         self.core = core
         self.device = core.device
@@ -119,6 +123,12 @@ class BatchedSolver:
                 self.x = torch.ones((s, n, n), **f32) if x0 is None else x0.to(**f32).clone().contiguous()
                 if x_mask is not None:
                     self.x *= x_mask
+        elif scaling is not None:
+            # scalar (sigma, tau), e.g. compute_Lipschitz_scaling (solvers.py:120-158)
+            self.tau = torch.full((s, n, n), float(scaling[1]), **f32)
+            self.tau_shared = 0
+            self.sigma = torch.full(tuple(self.b.shape), float(scaling[0]), **f32)
+            self.x = torch.zeros((s, n, n), **f32) if x0 is None else x0.to(**f32).clone().contiguous()
         else:
             relax = relaxation if relaxation is not None else (1.95 if self.method == "sirt" else 0.95)
             reg_tau = 4.0 if self.method == "pdhg" else 0.0

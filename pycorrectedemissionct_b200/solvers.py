@@ -92,6 +92,28 @@ def _as_batch(A, b, x0, x_mask):
     return bt, x0t, mt, maps, as_np
 
 
+def _operator_norm(A, b, bt: torch.Tensor, bp_mode: str, maps) -> float:
+    """``power_method`` (corrct ``solvers.py:26-57``, 5 iterations) with the device fp / bp.  Its
+    start is ``np.random.rand`` in the data's own shape and dtype, the reference's draw."""
+    shape = tuple(b.shape)
+    dtype = b.dtype if isinstance(b, np.ndarray) else np.float32
+    xr = np.random.rand(*shape).astype(dtype)
+    xr /= np.linalg.norm(xr)
+    s, n_det, n_ang, n = bt.shape
+    x = _tensor(xr, bt.device).reshape(n_det, s, n_ang, n).permute(1, 0, 2, 3).contiguous()
+    core = A.core
+    bp_maps = maps if bp_mode == "symmetric" else None
+    v = core.bp(x, bp_mode, bp_maps)
+    v_norm = float(torch.linalg.norm(v.double()).item())
+    L = v_norm
+    for _ in range(5):
+        v = (v / v_norm).contiguous()
+        v = core.bp(core.fp(v, maps), bp_mode, bp_maps)
+        v_norm = float(torch.linalg.norm(v.double()).item())
+        L = float(np.sqrt(v_norm))
+    return L
+
+
 def _is_volume(A) -> bool:
     return len(A.vol_shape) == 3
 
@@ -246,17 +268,20 @@ class PDHG(Solver):
 
     def __call__(self, A, b, iterations: int, x0=None, lower_limit=None, upper_limit=None, x_mask=None, b_mask=None, b_test_mask=None, precondition: bool = True):
         _check_projector(A)
-        if not precondition:
-            raise NotImplementedError("PDHG without diagonal preconditioning is not supported by the B200 solvers")
         bt, x0t, mt, maps, as_np = _as_batch(A, b, x0, x_mask)
         bm, btm = self._masks(A, b_mask, b_test_mask)
         bp_mode = "symmetric" if getattr(A, "is_symmetric", False) else "reference"
         if self.tv_weight is None:
             raise NotImplementedError("the fused PDHG needs a TV2D regularizer")
+        scaling = None
+        if not precondition:
+            # compute_Lipschitz_scaling (solvers.py:120-158); the TV term adds 2 * ndims to tau
+            L = _operator_norm(A, b, bt, bp_mode, maps)
+            scaling = (self.relaxation / L, self.relaxation / (L + 4.0))
         solver = BatchedSolver(
             A.core, maps, bt, "pdhg", x0=x0t, x_mask=mt, lower_limit=lower_limit, upper_limit=upper_limit,
             relaxation=self.relaxation, tv_lambda=self.tv_weight, bp_mode=bp_mode, background=self.background,
-            joint_stop=_is_volume(A), b_mask=bm,
+            joint_stop=_is_volume(A), b_mask=bm, scaling=scaling,
         )
         info = SolutionInfo(self.info(), max_iterations=iterations, tolerance=self.tolerance)
         if self.tolerance is None and btm is None:
@@ -381,8 +406,6 @@ class FISTA(Solver):
 
     def __call__(self, A, b, iterations: int, x0=None, lower_limit=None, upper_limit=None, x_mask=None, b_mask=None, b_test_mask=None, precondition: bool = True):
         _check_projector(A)
-        if not precondition:
-            raise NotImplementedError("FISTA without diagonal preconditioning is not supported by the B200 solvers")
         bt, x0t, mt, maps, as_np = _as_batch(A, b, x0, x_mask)
         bm, btm = self._masks(A, b_mask, b_test_mask)
         core = A.core
@@ -391,16 +414,21 @@ class FISTA(Solver):
         bp = lambda y: core.bp(y, bp_mode, maps if bp_mode == "symmetric" else None)  # noqa: E731
         n = core.n
         z = bt.shape[0]
-        # compute_diagonal_scaling (solvers.py:60-117), relaxation on tau
-        tau = bp(torch.ones_like(bt) if bm is None else bm.clone()).abs()
-        tau = torch.where(tau / tau.max() < 1e-5, torch.ones_like(tau), tau)
-        tau = self.relaxation / tau
-        x_ones = torch.ones((z, n, n), device=core.device)
-        if mt is not None:
-            x_ones = x_ones * mt
-        sigma = fp(x_ones).abs()
-        sigma = torch.where(sigma / sigma.max() < 1e-5, torch.ones_like(sigma), sigma)
-        sigma = 1.0 / sigma
+        if precondition:
+            # compute_diagonal_scaling (solvers.py:60-117), relaxation on tau
+            tau = bp(torch.ones_like(bt) if bm is None else bm.clone()).abs()
+            tau = torch.where(tau / tau.max() < 1e-5, torch.ones_like(tau), tau)
+            tau = self.relaxation / tau
+            x_ones = torch.ones((z, n, n), device=core.device)
+            if mt is not None:
+                x_ones = x_ones * mt
+            sigma = fp(x_ones).abs()
+            sigma = torch.where(sigma / sigma.max() < 1e-5, torch.ones_like(sigma), sigma)
+            sigma = 1.0 / sigma
+        else:
+            # compute_Lipschitz_scaling (solvers.py:120-158) without regularizers
+            L = _operator_norm(A, b, bt, bp_mode, maps)
+            sigma, tau = 1.0 / L, self.relaxation / L
         x = torch.zeros((z, n, n), device=core.device) if x0t is None else x0t.clone()
         if mt is not None:
             x = x * mt

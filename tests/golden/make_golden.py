@@ -172,6 +172,13 @@ def make_mask_case(corrct):
     xf, info = fista(p, b, iterations=ITERATIONS, b_mask=b_mask, b_test_mask=b_test)
     out.update(fista_x=xf, fista_res=info.residuals[:ITERATIONS], fista_res_cv=info.residuals_cv[:ITERATIONS],
                fista_res0=info.residual0, fista_res0_cv=info.residual0_cv)
+    # without diagonal preconditioning PDHG and FISTA scale by the operator norm from a power
+    # method that starts from np.random.rand (solvers.py:26-57, 120-158)
+    np.random.seed(11)
+    pdhg_l = corrct.solvers.PDHG(data_term="kl", regularizer=corrct.regularizers.Regularizer_TV2D(1e-2), verbose=False)
+    out["pdhg_lipschitz_x"] = pdhg_l(p, b, iterations=ITERATIONS, precondition=False)[0]
+    np.random.seed(12)
+    out["fista_lipschitz_x"] = corrct.solvers.FISTA(verbose=False)(p, b, iterations=ITERATIONS, precondition=False)[0]
     # SART draws its angle order from np.random (solvers.py:603); its tolerance path cannot run
     # here (compute_residual, solvers.py:503-505, subtracts (A, n) data from an (n, A) stack)
     np.random.seed(5)

@@ -188,6 +188,26 @@ def test_masked_solvers_match_reference(golden_cases, cuda):
     np.testing.assert_array_equal(xt, xo)
 
 
+def test_lipschitz_scaled_solvers_match_reference(golden_cases, cuda):
+    """PDHG and FISTA with precondition=False: the power method's random start drawn after the
+    same np.random.seed as the reference's run, its iterations on the device."""
+    import os
+
+    from conftest import GOLDEN
+    from pycorrectedemissionct_b200 import projectors, solvers
+
+    g = golden_cases["n32_a16"]
+    m = dict(np.load(os.path.join(GOLDEN, "mask_case.npz")))
+    n = int(g["n"])
+    p = projectors.ProjectorAttenuationXRF((n, n), g["angles"], att_maps=g["maps"], angles_detectors_rad=g["det_angles"])
+    np.random.seed(11)
+    xp, _ = solvers.PDHG(data_term="kl", regularizer=1e-2)(p, g["b"], iterations=10, precondition=False)
+    assert rel_l2(xp, m["pdhg_lipschitz_x"]) < TOL_RECON
+    np.random.seed(12)
+    xf, _ = solvers.FISTA()(p, g["b"], iterations=10, precondition=False)
+    assert rel_l2(xf, m["fista_lipschitz_x"]) < TOL_RECON
+
+
 @pytest.mark.parametrize("n,n_ang", [(66, 20), (130, 45), (128, 90), (256, 360)])
 def test_against_oracle_port_medium(n, n_ang, cuda):
     from oracle import port

@@ -84,6 +84,23 @@ def test_port_masked_solvers_match_reference_golden(golden_cases):
     np.testing.assert_allclose(cv, m["fista_res_cv"], rtol=1e-12)
 
 
+def test_port_lipschitz_scaled_solvers_match_reference_golden(golden_cases):
+    """PDHG and FISTA with precondition=False: sigma, tau from the power method's operator norm
+    (its random start drawn after np.random.seed, as in the reference's run)."""
+    g = golden_cases["n32_a16"]
+    m = np.load(os.path.join(GOLDEN, "mask_case.npz"))
+    n = int(g["n"])
+    _, deg32 = port.backend_angles(g["angles"])
+    fp = lambda v: port.fp_xrf(v, g["maps"], deg32)  # noqa: E731
+    bp = lambda s: port.bp_xrf(s, g["maps"], deg32)  # noqa: E731
+    np.random.seed(11)
+    xp = port.pdhg_kl_tv(fp, bp, g["b"], 10, (n, n), 1e-2, precondition=False)
+    assert rel_l2(xp, m["pdhg_lipschitz_x"]) < 1e-13
+    np.random.seed(12)
+    xf = port.fista(fp, bp, g["b"], 10, (n, n), precondition=False)
+    assert rel_l2(xf, m["fista_lipschitz_x"]) < 1e-13
+
+
 def test_reference_float32_maps_close_to_fp64(golden_cases):
     for g in golden_cases.values():
         assert rel_l2(g["maps_ref32"], g["maps"]) < 1e-6
