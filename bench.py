@@ -104,11 +104,19 @@ class ClockSampler:
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=self.fh, stderr=subprocess.DEVNULL,
             )
         except OSError:
             self.proc = None
+            return
+        # nvidia-smi takes a moment to start: wait (at most 3 s) for its first sample, so that the
+        # timed region that follows is covered from its start
+        t_end = time.time() + 3.0
+        while time.time() < t_end and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self) -> dict | None:
         if self.proc is None:
