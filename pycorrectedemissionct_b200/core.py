@@ -8,6 +8,7 @@ there is no CPU path.
 from __future__ import annotations
 
 import ctypes
+import threading
 from collections import OrderedDict
 
 import numpy as np
@@ -290,6 +291,7 @@ class XrfCore:
 
 _MAPS_TABLES: OrderedDict = OrderedDict()
 _MAPS_TABLES_MAX = 16
+_MAPS_TABLES_LOCK = threading.Lock()
 
 
 def _maps_tables(device, n, angles_rad32, det_angles, surfaces_mm2, distances_mm, sub_sampling, half_turns):
@@ -302,19 +304,22 @@ def _maps_tables(device, n, angles_rad32, det_angles, surfaces_mm2, distances_mm
 
     key = (str(device), int(n), a32.tobytes(), key_of(det_angles), key_of(surfaces_mm2), key_of(distances_mm),
            int(sub_sampling), bool(half_turns))
-    hit = _MAPS_TABLES.get(key)
-    if hit is not None:
-        _MAPS_TABLES.move_to_end(key)
-        return hit
+    with _MAPS_TABLES_LOCK:
+        hit = _MAPS_TABLES.get(key)
+        if hit is not None:
+            _MAPS_TABLES.move_to_end(key)
+            return hit
     rot_in, rot_out, n_sub = geometry.attenuation_rotations(a32, det_angles, n, surfaces_mm2, distances_mm, sub_sampling)
     rot_in_d = torch.from_numpy(np.ascontiguousarray(rot_in)).to(device)
     rot_out_d = torch.from_numpy(np.ascontiguousarray(rot_out)).to(device)
     pairs = geometry.half_turn_pairs(a32) if half_turns else None
     pairs_d = None if pairs is None else torch.from_numpy(pairs).to(device)
-    _MAPS_TABLES[key] = (rot_in_d, rot_out_d, n_sub, pairs_d)
-    while len(_MAPS_TABLES) > _MAPS_TABLES_MAX:
-        _MAPS_TABLES.popitem(last=False)
-    return _MAPS_TABLES[key]
+    entry = (rot_in_d, rot_out_d, n_sub, pairs_d)
+    with _MAPS_TABLES_LOCK:
+        _MAPS_TABLES[key] = entry
+        while len(_MAPS_TABLES) > _MAPS_TABLES_MAX:
+            _MAPS_TABLES.popitem(last=False)
+    return entry
 
 
 def compute_maps(

@@ -220,3 +220,29 @@ def test_pack_waves_and_default_schedule():
         assert k1 % 2 == 0 and k1 % k2 == 0 and (p1, p2) == (3, 2)
         engine.subset_permutation(a, [k1, k2])
     assert stream.default_schedule(720) == [(60, 3), (30, 2)]
+
+
+def test_maps_geometry_cache():
+    """compute_maps' host tables: built once per geometry, least recently used dropped past 16,
+    safe under concurrent callers (built here on the CPU device)."""
+    import concurrent.futures as cf
+
+    import torch
+
+    from pycorrectedemissionct_b200 import core, geometry, phantoms
+
+    core._MAPS_TABLES.clear()
+    dev = torch.device("cpu")
+    a = np.array(phantoms.angles(40), dtype=np.float32)
+    t1 = core._maps_tables(dev, 32, a, [np.pi / 2], None, None, 1, True)
+    t2 = core._maps_tables(dev, 32, a.copy(), [np.pi / 2], None, None, 1, True)
+    assert t1 is t2
+    rot_in, rot_out, n_sub = geometry.attenuation_rotations(a, [np.pi / 2], 32)
+    assert np.array_equal(t1[0].numpy(), rot_in) and np.array_equal(t1[1].numpy(), rot_out) and t1[2] == n_sub
+    assert np.array_equal(t1[3].numpy(), geometry.half_turn_pairs(a))
+    assert core._maps_tables(dev, 32, a, [np.pi / 2], None, None, 1, False)[3] is None
+    with cf.ThreadPoolExecutor(8) as ex:
+        outs = list(ex.map(lambda k: core._maps_tables(dev, 16 + k % 20, a, [np.pi / 2], None, None, 1, True), range(60)))
+    assert all(o[0].shape == (40, 2, 6) for o in outs)
+    assert len(core._MAPS_TABLES) <= core._MAPS_TABLES_MAX
+    core._MAPS_TABLES.clear()
