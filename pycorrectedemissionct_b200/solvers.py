@@ -297,7 +297,9 @@ class PDHG(Solver):
             r_cv = None if btm is None else _kl_residual_norm(ax, bt, self.background, btm, solver.sigma)
             return r, r_cv
 
-        info.residual0, info.residual0_cv = residuals(solver.x)
+        info.residual0, r0_cv = residuals(solver.x)
+        if r0_cv is not None:
+            info.residual0_cv = r0_cv
         for ii in range(iterations):
             info.iterations += 1
             solver.step()
