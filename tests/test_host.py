@@ -246,3 +246,72 @@ def test_maps_geometry_cache():
     assert all(o[0].shape == (40, 2, 6) for o in outs)
     assert len(core._MAPS_TABLES) <= core._MAPS_TABLES_MAX
     core._MAPS_TABLES.clear()
+
+
+def _column_range(ax, bx, ay, by, lim0, lim1, P, widen):
+    """Mirror of the maps scan's column_support (widen=True, limits (-1, n), open) and
+    column_inside (widen=False, closed limits) in csrc/cct_maps.cu."""
+    import math
+
+    tlo, thi = -1e300, 1e300
+    for a, b in ((ax, bx), (ay, by)):
+        if abs(b) < 1e-12:
+            inside = (lim0 < a < lim1) if widen else (lim0 <= a <= lim1)
+            if not inside:
+                return 1, 0
+        else:
+            t0, t1 = (lim0 - a) / b, (lim1 - a) / b
+            if t0 > t1:
+                t0, t1 = t1, t0
+            tlo, thi = max(tlo, t0), min(thi, t1)
+    if tlo > thi:
+        return 1, 0
+    if widen:
+        return max(0, math.floor(tlo) - 1), min(P - 1, math.ceil(thi) + 1)
+    return int(max(0.0, math.ceil(tlo))), int(min(P - 1.0, math.floor(thi)))
+
+
+@pytest.mark.parametrize("n,n_angles", [(2, 16), (3, 16), (16, 40), (33, 36), (512, 12), (1024, 4)])
+def test_maps_scan_fast_rows_stay_inside(n, n_angles):
+    """The scan kernel reads mu without per-tap tests on the rows where every lane of a warp is
+    inside (0.01, n - 1.01) by the FP64 column bounds; its FP32 coordinates (FMAs) there must give
+    taps in [0, n - 1] for every lane, at any angle, for the incident and emitted rotations."""
+    from pycorrectedemissionct_b200 import geometry
+
+    e, P = geometry.padded_size(n)
+    angles = np.concatenate([np.linspace(0, 2 * np.pi, n_angles, endpoint=False), [np.pi / 4, np.pi / 2, 1e-7, np.pi - 1e-7]])
+    rot_in, rot_out, _ = geometry.attenuation_rotations(np.array(angles, dtype=np.float32), [np.pi / 2, 1.0], n)
+    mats = [rot_in[a, 0] for a in range(len(angles))] + [rot_out[a, d, 0, 0] for a in range(len(angles)) for d in range(2)]
+
+    def fma32(a, b, c):
+        return (np.float64(a) * np.float64(b) + np.float64(c)).astype(np.float32)
+
+    checked = 0
+    for Md in mats:
+        m00, m01, m02 = np.float32(Md[0]), np.float32(Md[1]), np.float32(Md[2] - e)
+        m10, m11, m12 = np.float32(Md[3]), np.float32(Md[4]), np.float32(Md[5] - e)
+        for w0 in range(0, P, 32):
+            lanes = np.minimum(np.arange(w0, w0 + 32), P - 1)
+            ilo_w, ihi_w = -1, P
+            for c in lanes:
+                ax, ay = Md[0] * c + Md[2] - e, Md[3] * c + Md[5] - e
+                lo, hi = _column_range(ax, Md[1], ay, Md[4], -1.0, float(n), P, True)
+                if lo > hi:
+                    lo, hi = P, -1
+                ilo, ihi = _column_range(ax, Md[1], ay, Md[4], 0.01, n - 1.01, P, False) if n >= 2 else (P, -1)
+                ilo, ihi = max(ilo, lo), min(ihi, hi)
+                if ilo > ihi:
+                    ilo, ihi = P, -1
+                ilo_w, ihi_w = max(ilo_w, ilo), min(ihi_w, ihi)
+            if ilo_w > ihi_w:
+                continue
+            rows = np.arange(ilo_w, ihi_w + 1, dtype=np.float32)[:, None]
+            fc = lanes.astype(np.float32)[None, :]
+            x = fma32(m01, rows, fma32(m00, fc, m02))
+            y = fma32(m11, rows, fma32(m10, fc, m12))
+            fx, fy = np.floor(x), np.floor(y)
+            assert fx.min() >= 0 and fx.max() <= n - 2 and fy.min() >= 0 and fy.max() <= n - 2
+            checked += x.size
+    # below ~64 pixels every warp holds a column whose interior is empty (the whole warp takes the
+    # checked path); the benchmark's sizes use the fast rows
+    assert checked > 0 or n < 64
