@@ -315,3 +315,39 @@ def test_maps_scan_fast_rows_stay_inside(n, n_angles):
     # below ~64 pixels every warp holds a column whose interior is empty (the whole warp takes the
     # checked path); the benchmark's sizes use the fast rows
     assert checked > 0 or n < 64
+
+
+@pytest.mark.parametrize("n", [64, 130, 512])
+def test_fp_chunk_boxes_hold_every_tap(n):
+    """The forward projection stages a box per 64-bin x 64-row chunk (chunk_box in
+    csrc/cct_project.cu, at most 96 x 100) and reads the four taps of every sample from it without
+    tests: mirror the box and the FP32 sample coordinates and check every tap is inside."""
+    from pycorrectedemissionct_b200 import geometry
+
+    TC, TR, BOX_W, BOX_H = 64, 64, 100, 96
+    angles = np.concatenate([np.linspace(0, 2 * np.pi, 36, endpoint=False), [np.pi / 4, 3 * np.pi / 4, 1e-6]])
+    mats = geometry.fp_matrices(np.rad2deg(np.array(angles, dtype=np.float32)), n)
+
+    def sx(ma, mb, mc, c, r):  # sample_x: fmaf(mb, r, fmaf(ma, c, mc)) in FP32
+        inner = (np.float64(ma) * np.float64(c) + np.float64(mc)).astype(np.float32)
+        return (np.float64(mb) * np.float64(r) + np.float64(inner)).astype(np.float32)
+
+    for m in mats:
+        m00, m01, m02, m10, m11, m12 = (np.float32(v) for v in m)
+        for c0 in range(0, n, TC):
+            c_last = min(c0 + TC, n) - 1
+            for r0 in range(0, n, TR):
+                r_last = min(r0 + TR, n) - 1
+                cs = np.array([c0, c_last, c0, c_last], dtype=np.float32)
+                rs = np.array([r0, r0, r_last, r_last], dtype=np.float32)
+                xs, ys = sx(m00, m01, m02, cs, rs), sx(m10, m11, m12, cs, rs)
+                bx0 = (int(np.floor(xs.min())) - 1) & ~3
+                bx1 = int(np.floor(xs.max())) + 2
+                by0 = int(np.floor(ys.min())) - 1
+                by1 = int(np.floor(ys.max())) + 2
+                q4 = (bx1 - bx0) // 4 + 1
+                assert 4 * q4 <= BOX_W and by1 - by0 + 1 <= BOX_H
+                cc, rr = np.meshgrid(np.arange(c0, c_last + 1, dtype=np.float32), np.arange(r0, r_last + 1, dtype=np.float32))
+                x, y = np.floor(sx(m00, m01, m02, cc, rr)), np.floor(sx(m10, m11, m12, cc, rr))
+                assert x.min() >= bx0 and x.max() + 1 <= bx0 + 4 * q4 - 1
+                assert y.min() >= by0 and y.max() + 1 <= by1
