@@ -351,3 +351,36 @@ def test_fp_chunk_boxes_hold_every_tap(n):
                 x, y = np.floor(sx(m00, m01, m02, cc, rr)), np.floor(sx(m10, m11, m12, cc, rr))
                 assert x.min() >= bx0 and x.max() + 1 <= bx0 + 4 * q4 - 1
                 assert y.min() >= by0 and y.max() + 1 <= by1
+
+
+@pytest.mark.parametrize("n", [32, 130, 512])
+def test_bp_staged_bins_cover_every_lookup(n):
+    """The back projection stages, per 32 x 64 pixel tile and line, 80 (value, slope) pairs from
+    bin kbase = floor(tmin + K) - 1 (bp_cta in csrc/cct_project.cu) and looks a pixel's pair up
+    without tests: mirror the FP32 arithmetic and check every lookup of every pixel of the tile
+    (rows and columns past n included, as the kernel computes them) lands in [0, 80)."""
+    from pycorrectedemissionct_b200 import geometry
+
+    TJ, TI, KW = 32, 64, 80
+    angles = np.concatenate([np.linspace(0, 2 * np.pi, 90, endpoint=False), [np.pi / 4, 1e-6, np.pi / 2 + 1e-6]])
+    trig = geometry.bp_trig(np.rad2deg(np.array(angles, dtype=np.float32)))
+    R = K = n // 2
+
+    def fma32(a, b, c):
+        return (np.float64(a) * np.float64(b) + np.float64(c)).astype(np.float32)
+
+    for cs, sn in trig:
+        cs, sn = np.float32(cs), np.float32(sn)
+        for i0 in range(0, n, TI):
+            for j0 in range(0, n, TJ):
+                cj0, cj1 = np.float32(j0 - R), np.float32(j0 + TJ - 1 - R)
+                ci0, ci1 = np.float32(i0 - R), np.float32(i0 + TI - 1 - R)
+                ts = [fma32(cj, cs, np.float32(-(ci * sn))) for cj in (cj0, cj1) for ci in (ci0, ci1)]
+                tmin = min(ts)
+                kbase = int(np.floor(np.float32(tmin + np.float32(K)))) - 1
+                off = np.float32(K - kbase)
+                jj = np.arange(j0, j0 + TJ, dtype=np.float32)[None, :]
+                ii = np.arange(i0, i0 + TI, dtype=np.float32)[:, None]
+                base = fma32(jj - np.float32(R), cs, off)
+                idx = np.floor(fma32(-(ii - np.float32(R)), sn, base))
+                assert idx.min() >= 0 and idx.max() <= KW - 1
