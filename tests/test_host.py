@@ -384,3 +384,35 @@ def test_bp_staged_bins_cover_every_lookup(n):
                 base = fma32(jj - np.float32(R), cs, off)
                 idx = np.floor(fma32(-(ii - np.float32(R)), sn, base))
                 assert idx.min() >= 0 and idx.max() <= KW - 1
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """Every ctypes descriptor in _lib has the size and field offsets of its C struct in
+    include/corrct_b200.h (compiled here with gcc)."""
+    import ctypes
+    import shutil
+    import subprocess
+
+    from pycorrectedemissionct_b200 import _lib
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    pairs = {"cct_xrf_desc": _lib.XrfDesc, "cct_maps_desc": _lib.MapsDesc, "cct_noise_desc": _lib.NoiseDesc,
+             "cct_conv_desc": _lib.ConvDesc, "cct_solver_state": _lib.SolverState}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "corrct_b200.h"', "int main(void) {"]
+    for cname, cls in pairs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, cls in pairs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
