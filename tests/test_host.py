@@ -105,6 +105,14 @@ def test_validation_errors_map_to_value_error():
     assert lib.cct_maps_workspace_size(ctypes.byref(md), 2, ctypes.byref(out)) == _lib.CCT_OK
     p = geometry.padded_size(16)[1]
     assert out.value == 2 * (p * p + p) * 4  # W planes and the per-column constants of half-turn partners
+    table = (ctypes.c_int32 * 4)(0, 2, 1, 3)
+    md.pairs = ctypes.cast(table, ctypes.c_void_p)
+    for bad in (0, 5):  # entries must be in [1, n_angles]
+        md.n_entries = bad
+        assert lib.cct_maps_workspace_size(ctypes.byref(md), 1, ctypes.byref(out)) == _lib.CCT_ERR_VALUE
+        assert b"n_entries" in lib.cct_last_error()
+    md.n_entries = 2
+    assert lib.cct_maps_workspace_size(ctypes.byref(md), 1, ctypes.byref(out)) == _lib.CCT_OK
 
 
 def test_compute_paths_need_cuda():
