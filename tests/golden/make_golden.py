@@ -187,6 +187,27 @@ def make_mask_case(corrct):
     print(f"masks: maps {g['maps'].shape}")
 
 
+def make_options_case(corrct):
+    """MLEM, SIRT and PDHG (KL, TV2D 1e-2) with a solution mask and clipping limits
+    (solvers.py:747-752, 800-805, 966-980, 1182-1190) on the n32_a16 case."""
+    g = np.load(os.path.join(HERE, "xrf_n32_a16.npz"))
+    n, angles, b = int(g["n"]), g["angles"], g["b"]
+    p = corrct.projectors.ProjectorAttenuationXRF(
+        (n, n), angles, att_maps=g["maps"], angles_detectors_rad=g["det_angles"], use_multithreading=False,
+        backend="skimage", verbose=False,
+    )
+    yy, xx = np.mgrid[:n, :n]
+    x_mask = (np.hypot(yy - (n - 1) / 2, xx - (n - 1) / 2) <= n / 2 - 3).astype(np.float64)
+    out = dict(x_mask=x_mask)
+    out["mlem_x"] = corrct.solvers.MLEM(verbose=False)(p, b, iterations=ITERATIONS, x_mask=x_mask, lower_limit=0.0,
+                                                        upper_limit=2.0)[0]
+    out["sirt_x"] = corrct.solvers.SIRT(verbose=False)(p, b, iterations=ITERATIONS, x_mask=x_mask, lower_limit=0.0)[0]
+    pdhg = corrct.solvers.PDHG(data_term="kl", regularizer=corrct.regularizers.Regularizer_TV2D(1e-2), verbose=False)
+    out["pdhg_x"] = pdhg(p, b, iterations=ITERATIONS, x_mask=x_mask, lower_limit=0.0, upper_limit=3.0)[0]
+    np.savez_compressed(os.path.join(HERE, "options_case.npz"), **out)
+    print(f"options: maps {g['maps'].shape}")
+
+
 NOISE_CASES = [
     # name, photons, efficiency, poisson, readout std, background avg, background std, seed
     ("poisson", 1e3, 0.5, True, None, None, None, 101),
@@ -219,6 +240,7 @@ def main():
         make_noise_golden(corrct)
         make_surface_case(corrct)
         make_mask_case(corrct)
+        make_options_case(corrct)
     print("\n".join(line for line in log.getvalue().splitlines() if ":" in line and ("maps" in line or "noise" in line)))
 
 

@@ -188,6 +188,28 @@ def test_masked_solvers_match_reference(golden_cases, cuda):
     np.testing.assert_array_equal(xt, xo)
 
 
+def test_solvers_with_mask_and_limits_match_reference(golden_cases, cuda):
+    """MLEM, SIRT and PDHG through the drop-in solvers with a solution mask and clipping limits,
+    against the reference's own run."""
+    import os
+
+    from conftest import GOLDEN
+    from pycorrectedemissionct_b200 import projectors, solvers
+
+    g = golden_cases["n32_a16"]
+    o = dict(np.load(os.path.join(GOLDEN, "options_case.npz")))
+    n = int(g["n"])
+    p = projectors.ProjectorAttenuationXRF((n, n), g["angles"], att_maps=g["maps"], angles_detectors_rad=g["det_angles"])
+    m = o["x_mask"]
+    xm, _ = solvers.MLEM()(p, g["b"], iterations=10, x_mask=m, lower_limit=0.0, upper_limit=2.0)
+    assert rel_l2(xm, o["mlem_x"]) < TOL_RECON
+    xs, _ = solvers.SIRT()(p, g["b"], iterations=10, x_mask=m, lower_limit=0.0)
+    assert rel_l2(xs, o["sirt_x"]) < TOL_RECON
+    xp, _ = solvers.PDHG(data_term="kl", regularizer=1e-2)(p, g["b"], iterations=10, x_mask=m, lower_limit=0.0,
+                                                          upper_limit=3.0)
+    assert rel_l2(xp, o["pdhg_x"]) < TOL_RECON
+
+
 def test_lipschitz_scaled_solvers_match_reference(golden_cases, cuda):
     """PDHG and FISTA with precondition=False: the power method's random start drawn after the
     same np.random.seed as the reference's run, its iterations on the device."""

@@ -101,6 +101,23 @@ def test_port_lipschitz_scaled_solvers_match_reference_golden(golden_cases):
     assert rel_l2(xf, m["fista_lipschitz_x"]) < 1e-13
 
 
+def test_port_solvers_with_mask_and_limits_match_reference_golden(golden_cases):
+    """MLEM, SIRT and PDHG with a solution mask and clipping limits."""
+    g = golden_cases["n32_a16"]
+    o = np.load(os.path.join(GOLDEN, "options_case.npz"))
+    n = int(g["n"])
+    _, deg32 = port.backend_angles(g["angles"])
+    fp = lambda v: port.fp_xrf(v, g["maps"], deg32)  # noqa: E731
+    bp = lambda s: port.bp_xrf(s, g["maps"], deg32)  # noqa: E731
+    m = o["x_mask"]
+    xm, _ = port.mlem(fp, bp, g["b"], 10, x_mask=m, lower_limit=0.0, upper_limit=2.0)
+    assert rel_l2(xm, o["mlem_x"]) < 1e-13
+    xs = port.sirt(fp, bp, g["b"], 10, (n, n), x_mask=m, lower_limit=0.0)
+    assert rel_l2(xs, o["sirt_x"]) < 1e-13
+    xp = port.pdhg_kl_tv(fp, bp, g["b"], 10, (n, n), 1e-2, x_mask=m, lower_limit=0.0, upper_limit=3.0)
+    assert rel_l2(xp, o["pdhg_x"]) < 1e-13
+
+
 def test_reference_float32_maps_close_to_fp64(golden_cases):
     for g in golden_cases.values():
         assert rel_l2(g["maps_ref32"], g["maps"]) < 1e-6
