@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define CCT_ABI_VERSION 5
+#define CCT_ABI_VERSION 6
 
 /* Status codes. */
 #define CCT_OK 0
@@ -57,6 +57,10 @@ extern "C" {
 /* Kernel variants (results are identical; only the speed differs). */
 #define CCT_VARIANT_FP_TMA 1 /* forward projection stages its boxes with TMA bulk tensor copies
                                 (needs n % 8 == 0; otherwise the load/store staging is used) */
+#define CCT_VARIANT_FP_SLICES2 2 /* forward projection: one CTA per two slices of the batch (shared
+                                    sample coordinates, one 8-byte shared load per tap for both) */
+#define CCT_VARIANT_FP_SLICES4 4 /* four slices per CTA (16-byte taps); wins over SLICES2 when both
+                                    are set */
 
 /* Geometry of a batch of slices that share n, the angles and the detectors. */
 typedef struct cct_xrf_desc {
@@ -84,6 +88,10 @@ typedef struct cct_xrf_desc {
                                 slices); 0 = dense (n_angles * n_det * n * n, or n_angles * (1 + n_det)
                                 * n * n for fields).  Lets a call read an angle range of a larger array. */
   const float* channel_scale; /* device [n_channels]: s_c of CCT_DTYPE_FIELDS_F32 */
+  const int32_t* fp_bank_residues; /* device [A][2] or NULL: per angle, the row-stride residues (mod 16
+                                      and mod 8) of the slice-grouped forward projection's staged box,
+                                      chosen to spread the angle's bilinear taps over the shared-memory
+                                      banks; speed only, any values give the same results */
 } cct_xrf_desc;
 
 /* Library identity. */
@@ -155,7 +163,9 @@ int cct_compute_maps(const cct_maps_desc* desc, const float* mu_in, const float*
    forbids cudaMalloc in its callbacks, or cudaMalloc's implicit synchronisation is not allowed).
    Calls whose one-angle pass needs more than 32 MiB return CCT_ERR_VALUE.  The first call on a
    device looks up the array's device address (cudaGetSymbolAddress), so make that first call
-   before any stream capture.  All calls share the array: calls that overlap on the GPU race. */
+   before any stream capture; the address is kept for the life of the process's CUDA context on
+   that device (after a cudaDeviceReset the library must be reloaded).  All calls share the array:
+   calls that overlap on the GPU race. */
 int cct_compute_maps_noalloc(const cct_maps_desc* desc, const float* mu_in, const float* mu_out, void* maps,
                              void* stream);
 

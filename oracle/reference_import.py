@@ -3,8 +3,12 @@
 TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).  Used by
 ``tests/golden/make_golden.py`` to run the reference's own code (projectors,
 attenuation, solvers, data terms, regularizers) on the CPU and record golden
-fixtures.  It needs a local checkout of the reference (``CORRCT_SRC`` or the
-default below); where no checkout exists ``load_corrct`` raises ``ImportError``.
+fixtures, and by the drop-in tests, which run the reference's unchanged solvers
+and projector classes on this package's GPU projectors.  It needs a directory
+that holds the reference's ``corrct`` package: ``$CORRCT_SRC`` (a checkout's
+``src`` directory), else ``baseline/_ref`` at the repository root (where
+``pip install --no-deps --target baseline/_ref <checkout>`` puts it); where
+neither exists ``load_corrct`` raises ``ImportError``.
 
 The reference's ``corrct/__init__.py`` imports every submodule, which pulls in
 scikit-image, matplotlib, xraylib and pywt at import time; none of them is
@@ -27,7 +31,7 @@ import types
 
 from . import skimage_restated
 
-DEFAULT_SRC = "/root/reference/src"
+REPO_REF = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "baseline", "_ref")
 
 _STUB_ROOTS = ("skimage", "matplotlib", "mpl_toolkits", "xraylib", "pywt")
 
@@ -84,11 +88,21 @@ class _StubFinder(importlib.abc.MetaPathFinder):
         return None
 
 
+def reference_src() -> str | None:
+    """The directory holding the reference's ``corrct`` package, or None."""
+    for src in (os.environ.get("CORRCT_SRC"), REPO_REF):
+        if src and os.path.isdir(os.path.join(src, "corrct")):
+            return src
+    return None
+
+
 def load_corrct(src: str | None = None):
-    """Return the reference ``corrct`` package imported from ``src`` with stubs installed."""
-    src = src or os.environ.get("CORRCT_SRC", DEFAULT_SRC)
-    if not os.path.isdir(os.path.join(src, "corrct")):
-        raise ImportError(f"reference checkout not found under {src}")
+    """Return the reference ``corrct`` package imported from ``src`` (default: ``reference_src()``)
+    with stubs installed."""
+    src = src or reference_src()
+    if src is None or not os.path.isdir(os.path.join(src, "corrct")):
+        raise ImportError("the reference's corrct package was not found: set CORRCT_SRC to a checkout's src "
+                          "directory or install it into baseline/_ref")
     if "corrct" in sys.modules:
         return sys.modules["corrct"]
     if not any(isinstance(f, _StubFinder) for f in sys.meta_path):

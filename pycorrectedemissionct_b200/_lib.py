@@ -13,7 +13,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcorrct_b200.so")
 
-ABI_VERSION = 5  # CCT_ABI_VERSION of include/corrct_b200.h
+ABI_VERSION = 6  # CCT_ABI_VERSION of include/corrct_b200.h
 
 CCT_OK = 0
 CCT_ERR_VALUE = 1
@@ -29,6 +29,8 @@ CCT_BP_SYMMETRIC = 1
 CCT_BP_ADJOINT = 2
 
 CCT_VARIANT_FP_TMA = 1
+CCT_VARIANT_FP_SLICES2 = 2
+CCT_VARIANT_FP_SLICES4 = 4
 
 CCT_METHOD_MLEM = 0
 CCT_METHOD_SIRT = 1
@@ -53,6 +55,7 @@ class XrfDesc(ctypes.Structure):
         ("n_channels", ctypes.c_int32),
         ("maps_slice_stride", ctypes.c_int64),
         ("channel_scale", ctypes.c_void_p),
+        ("fp_bank_residues", ctypes.c_void_p),
     ]
 
 

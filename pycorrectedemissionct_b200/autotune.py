@@ -1,11 +1,13 @@
 """Kernel-variant autotuner with an on-disk cache.
 
-The fp kernel has two shared-memory staging variants with identical results: load/store
-staging (default) and TMA bulk-tensor staging (``CCT_VARIANT_FP_TMA``).  Which is faster
-depends on n, the angle count, the map type and the batch, so ``tune`` times both on the
-actual shape (CUDA events, a few launches over a batch of the real size) and caches the
-winner per (GPU, n, angles, detectors, slices, map dtype) in a JSON file
-(``$CCT_AUTOTUNE_CACHE`` or ``~/.cache/corrct_b200/autotune.json``).
+The fp kernel has four variants with identical results: one slice per CTA with load/store
+staging (default) or TMA bulk-tensor staging (``CCT_VARIANT_FP_TMA``), and two or four slices
+per CTA sharing the sample coordinates (``CCT_VARIANT_FP_SLICES2`` / ``SLICES4``).  Which is
+faster depends on n, the angle count, the map type, the batch and whether the maps are an
+angle range of a larger array (the TMA variant needs dense maps), so ``tune`` times every
+applicable variant on the actual call (CUDA events, a few launches over a batch of the real
+size) and caches the winner per (GPU, n, angles, detectors, slices, map dtype, layout) in a
+JSON file (``$CCT_AUTOTUNE_CACHE`` or ``~/.cache/corrct_b200/autotune.json``).
 """
 
 from __future__ import annotations
@@ -20,7 +22,7 @@ from . import _lib
 from .core import XrfCore
 
 _LOCK = threading.Lock()
-VARIANTS = (0, _lib.CCT_VARIANT_FP_TMA)
+VARIANTS = (0, _lib.CCT_VARIANT_FP_TMA, _lib.CCT_VARIANT_FP_SLICES2, _lib.CCT_VARIANT_FP_SLICES4)
 
 
 def cache_path() -> str:
@@ -47,9 +49,10 @@ def _store(cache: dict) -> None:
         pass
 
 
-def key(core: XrfCore, n_slices: int, maps_dtype: torch.dtype) -> str:
+def key(core: XrfCore, n_slices: int, maps_dtype: torch.dtype, dense: bool = True) -> str:
     name = torch.cuda.get_device_name(core.device).replace(" ", "_")
-    return f"{name}|n{core.n}|a{core.n_angles}|d{core.n_det}|s{n_slices}|{str(maps_dtype).split('.')[-1]}"
+    layout = "" if dense else "|strided"
+    return f"{name}|n{core.n}|a{core.n_angles}|d{core.n_det}|s{n_slices}|{str(maps_dtype).split('.')[-1]}{layout}"
 
 
 def time_fp(core: XrfCore, vol: torch.Tensor, maps: torch.Tensor, variant: int, reps: int = 3) -> float:
@@ -72,15 +75,20 @@ def time_fp(core: XrfCore, vol: torch.Tensor, maps: torch.Tensor, variant: int, 
 
 def tune(core: XrfCore, vol: torch.Tensor, maps: torch.Tensor, force: bool = False) -> int:
     """Pick the faster fp variant for this shape (cached); sets and returns ``core.variant``."""
-    k = key(core, vol.shape[0], maps.dtype)
+    dense = maps is None or maps.is_contiguous()
+    k = key(core, vol.shape[0], None if maps is None else maps.dtype, dense)
     with _LOCK:
         cache = _load()
-        if not force and k in cache:
+        if not force and k in cache and int(cache[k]["variant"]) in VARIANTS:
             core.variant = int(cache[k]["variant"])
             return core.variant
         times = {}
         for v in VARIANTS:
-            if v == _lib.CCT_VARIANT_FP_TMA and core.n % 8 != 0:
+            if v == _lib.CCT_VARIANT_FP_TMA and (core.n % 8 != 0 or not dense):
+                continue
+            if v == _lib.CCT_VARIANT_FP_SLICES2 and vol.shape[0] < 2:
+                continue
+            if v == _lib.CCT_VARIANT_FP_SLICES4 and vol.shape[0] < 3:
                 continue
             times[v] = time_fp(core, vol, maps, v)
         best = min(times, key=times.get)

@@ -93,6 +93,8 @@ class XrfCore:
         self.trig_np = geometry.bp_trig(self.angles_deg32)
         self.fp_mat = torch.from_numpy(self.fp_mat_np).to(self.device)
         self.trig = torch.from_numpy(self.trig_np).to(self.device)
+        # per-angle staged-box strides of the slice-grouped fp (speed only)
+        self.bank_res = torch.from_numpy(geometry.fp_bank_residues(self.fp_mat_np)).to(self.device)
         self.intensities_np = None
         self.line_scale = None
         self.psf = None
@@ -159,7 +161,7 @@ class XrfCore:
         sub.angles_rad32, sub.angles_deg32 = self.angles_rad32[rng], self.angles_deg32[rng]
         sub.n_angles = len(sub.angles_rad32)
         sub.fp_mat_np, sub.trig_np = self.fp_mat_np[rng], self.trig_np[rng]
-        sub.fp_mat, sub.trig = self.fp_mat[rng], self.trig[rng]
+        sub.fp_mat, sub.trig, sub.bank_res = self.fp_mat[rng], self.trig[rng], self.bank_res[rng]
         sub.intensities_np = None if self.intensities_np is None else self.intensities_np[rng]
         sub.line_scale = None if self.line_scale is None else self.line_scale[rng]
         sub.psf = self.psf
@@ -183,6 +185,7 @@ class XrfCore:
             d.bp_trig = self.trig.data_ptr()
             d.weights = _ptr(self.weights)
             d.line_scale = _ptr(self.line_scale)
+            d.fp_bank_residues = self.bank_res.data_ptr()
         else:
             a0, a1 = angles.start, angles.stop
             d.n_angles = a1 - a0
@@ -190,6 +193,7 @@ class XrfCore:
             d.bp_trig = self.trig[a0:a1].data_ptr()
             d.weights = None if self.weights is None else self.weights[a0:a1].data_ptr()
             d.line_scale = None if self.line_scale is None else self.line_scale[a0:a1].data_ptr()
+            d.fp_bank_residues = self.bank_res[a0:a1].data_ptr()
         d.psf = _ptr(self.psf)
         d.psf_len = 0 if self.psf is None else int(self.psf.numel())
         if maps_dtype == _lib.CCT_DTYPE_FIELDS_F32:
@@ -382,6 +386,12 @@ def compute_maps(
         "cct_compute_maps", ctypes.byref(desc), _ptr(mu_in), _ptr(mu_out), maps.data_ptr(), workspace.data_ptr(),
         workspace.numel() * workspace.element_size(), stream_handle(device),
     )
+    # the cached tables may be dropped from the cache (and freed) by a later call while this
+    # launch still reads them on this stream: tie their memory to the stream's pending work
+    stream = torch.cuda.current_stream(device)
+    for t in (rot_in_d, rot_out_d, pairs_d):
+        if t is not None:
+            t.record_stream(stream)
     # torch's caching allocator reuses a workspace allocated here only for work queued later on
     # the same stream, so dropping it here is safe
     return maps

@@ -73,6 +73,7 @@ static cct::FpArgs make_fp_args(const cct_xrf_desc* d, const float* vol, const v
   a.maps_slice_stride = maps_stride(d);
   a.n_channels = d->n_channels > 0 ? d->n_channels : 1;
   a.chan_scale = d->channel_scale;
+  a.bank_residues = d->fp_bank_residues;
   return a;
 }
 
@@ -151,6 +152,8 @@ int cct_compute_maps(const cct_maps_desc* desc, const float* mu_in, const float*
   CCT_REQUIRE(maps != nullptr && workspace != nullptr, "maps and workspace are required");
   CCT_REQUIRE(workspace_bytes >= need, "workspace smaller than one angle pass (cct_maps_workspace_size)");
   CCT_REQUIRE(desc->n_angles <= 65535 && desc->n_slices <= 65535, "too many angles or slices");
+  CCT_REQUIRE((int64_t)(desc->has_in ? 1 : 0) + (desc->has_out ? (int64_t)desc->n_det * desc->n_sub : 0) <= 65535,
+              "too many emitted directions (n_det * n_sub) per angle");
   rc = cct::launch_maps(desc, mu_in, mu_out, maps, workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
   if (rc != CCT_OK) return rc;
   return check_launch();

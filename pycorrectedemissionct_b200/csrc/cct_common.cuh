@@ -1,6 +1,8 @@
 // Shared helpers of the corrct B200 kernels (sm_100a only).
 #pragma once
 
+#include <atomic>
+
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -105,6 +107,26 @@ __device__ __forceinline__ float warp_sum_float(float v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+
+// The dynamic shared-memory limit is a per-device attribute of a kernel: set it once per device
+// (and kernel), thread-safe.  Devices beyond the first 64 set it before every launch.
+template <auto KERNEL>
+inline bool ensure_dynamic_smem(int bytes) {
+  static std::atomic<uint64_t> done{0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  const uint64_t bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+  if (bit != 0 && (done.load(std::memory_order_acquire) & bit) != 0) return true;
+  if (cudaFuncSetAttribute(KERNEL, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  done.fetch_or(bit, std::memory_order_acq_rel);
+  return true;
+}
+
+// After a launch with a fallback: false (and the launch error cleared) if it was refused.
+inline bool launched_ok() { return cudaGetLastError() == cudaSuccess; }
 
 }  // namespace cct
 

@@ -458,6 +458,11 @@ int launch_maps(const cct_maps_desc* d, const float* mu_in, const float* mu_out,
   if (entries < 1 || entries > d->n_angles) return CCT_ERR_VALUE;
   int per_pass = (int)std::min<int64_t>((int64_t)work_bytes / per_angle, (int64_t)entries);
   if (per_pass < 1) return CCT_ERR_VALUE;
+  // the scan grid's y dimension is entries x jobs (at most 65535): small slices with a large
+  // workspace take more passes instead
+  const int jobs = (d->has_in ? 1 : 0) + (d->has_out ? d->n_det * d->n_sub : 0);
+  per_pass = std::max(1, std::min(per_pass, 65535 / std::max(1, jobs)));
+  if ((int64_t)jobs > 65535) return CCT_ERR_VALUE;
   MapsPass p;
   p.n = d->n; p.P = P; p.e = e; p.n_det = d->n_det; p.n_sub = d->n_sub;
   p.has_in = d->has_in; p.has_out = d->has_out; p.maps_dtype = d->maps_dtype; p.n_angles = d->n_angles;

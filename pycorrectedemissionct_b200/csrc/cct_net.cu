@@ -152,7 +152,6 @@ __global__ void __launch_bounds__(NET_THREADS) conv_umma_kernel(ConvArgs a) {
   extern __shared__ __align__(1024) unsigned char net_smem[];
   __shared__ __align__(8) uint64_t mma_bar[2];
   __shared__ uint32_t tmem_base_sh;
-  __shared__ int timed_out;
 
   unsigned char* abuf[2] = {net_smem, net_smem + A_BYTES};
   unsigned char* bbuf[2] = {net_smem + 2 * A_BYTES, net_smem + 2 * A_BYTES + B_BYTES};
@@ -190,7 +189,6 @@ __global__ void __launch_bounds__(NET_THREADS) conv_umma_kernel(ConvArgs a) {
     net_mbar_init(&mma_bar[0]);
     net_mbar_init(&mma_bar[1]);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    timed_out = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -198,11 +196,15 @@ __global__ void __launch_bounds__(NET_THREADS) conv_umma_kernel(ConvArgs a) {
   const uint32_t tmem_d = tmem_base_sh;
   constexpr uint32_t IDESC = umma_idesc_bf16(NET_BM, BN);
 
+  // A wait that runs out sets this thread's flag; the flags are combined at the block's barrier
+  // (__syncthreads_or), so every thread leaves the loop after the same block.
+  bool timed_out = false;
+  int committed = 0;  // blocks whose MMAs were issued and committed (uniform across the CTA)
   for (int kb = 0; kb < kblocks; ++kb) {
     const int buf = kb & 1;
     if (kb >= 2) {
       // the MMAs that read this buffer (block kb - 2) must be done before it is overwritten
-      if (!net_mbar_wait(&mma_bar[buf], (uint32_t)(((kb - 2) >> 1) & 1))) timed_out = 1;
+      if (!net_mbar_wait(&mma_bar[buf], (uint32_t)(((kb - 2) >> 1) & 1))) timed_out = true;
     }
     const int64_t k0 = k_begin + (int64_t)kb * NET_BK;
     // ---- gather A: 128 rows x 8 chunks (thread = row)
@@ -235,8 +237,11 @@ __global__ void __launch_bounds__(NET_THREADS) conv_umma_kernel(ConvArgs a) {
       *reinterpret_cast<uint4*>(bbuf[buf] + kc * (BN * 16) + r * 16) = v;
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (timed_out) break;
+    if (__syncthreads_or(timed_out ? 1 : 0)) {
+      timed_out = true;
+      break;
+    }
+    committed = kb + 1;
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t a_base = net_smem_u32(abuf[buf]);
@@ -258,18 +263,18 @@ __global__ void __launch_bounds__(NET_THREADS) conv_umma_kernel(ConvArgs a) {
     }
   }
   // wait for the last committed block (its commit covers all earlier MMAs of this thread)
-  if (kblocks > 0 && !timed_out) {
-    const int last = kblocks - 1;
-    if (!net_mbar_wait(&mma_bar[last & 1], (uint32_t)((last >> 1) & 1))) timed_out = 1;
+  if (committed > 0 && !timed_out) {
+    const int last = committed - 1;
+    if (!net_mbar_wait(&mma_bar[last & 1], (uint32_t)((last >> 1) & 1))) timed_out = true;
   }
-  __syncthreads();
+  timed_out = __syncthreads_or(timed_out ? 1 : 0) != 0;
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
   if (timed_out) {
     if (tid == 0) {
       atomicExch(&g_net_timeout, 1);
-      if (kblocks > 0) {
-        const int last = kblocks - 1;
+      if (committed > 0) {  // one more bounded wait for the MMAs in flight before TMEM is freed
+        const int last = committed - 1;
         net_mbar_wait(&mma_bar[last & 1], (uint32_t)((last >> 1) & 1));
       }
     }
@@ -328,13 +333,9 @@ static int launch_conv_bn(const ConvArgs& a, cudaStream_t st) {
   // LBO = rows * 16 bytes, core matrices at SBO = 128 bytes), so 3-6 CTAs fit per SM, whose TMEM
   // columns (BN, at least 32, each) stay within the SM's 512
   const size_t smem = 2 * (NET_BM * NET_BK * 2) + 2 * (BN * NET_BK * 2);
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(conv_umma_kernel<MODE, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess) {
-      return CCT_ERR_CUDA;
-    }
-    attr = true;
+  if (!ensure_dynamic_smem<conv_umma_kernel<MODE, BN>>((int)smem)) {
+    cct_set_last_error("cudaFuncSetAttribute(MaxDynamicSharedMemorySize) failed for the convolution kernel");
+    return CCT_ERR_CUDA;
   }
   dim3 grid((unsigned)((a.m_total + NET_BM - 1) / NET_BM), (unsigned)((a.n_total + BN - 1) / BN), 1);
   if (MODE == NET_WGRAD) grid.z = (unsigned)((a.k_total + a.k_split - 1) / a.k_split);

@@ -504,6 +504,267 @@ __global__ void __launch_bounds__(FP_THREADS, 2)
 }
 
 // ------------------------------------------------------------------------------------------
+// Forward projection over groups of G slices per CTA (G = 2 or 4)
+//
+// All slices of a batch share the angle's sample positions, so one CTA owns (band, angle *
+// detector, group of G slices): it computes each sample's coordinates, tap offsets and weights
+// once, stages z = x * map of its G slices interleaved (one G-float element per pixel), and
+// reads every bilinear tap of all G slices with one vector shared load.  Two further savings
+// against fp_kernel, whose arithmetic per sample is otherwise identical (bit-identical results):
+//   * each staged box row holds only the columns the chunk's taps can read (the chunk's
+//     parallelogram clipped to the row's slab), not the whole axis-aligned bounding box;
+//   * the box row stride is chosen per angle (bank_residues, from the host) so that the eight
+//     (16-byte elements) or sixteen (8-byte) lanes of a shared-memory phase hit distinct banks
+//     as often as the angle's lattice allows.
+// Chunks are 64 columns x FPG_TR rows; the fill gives each warp whole box rows, one pixel per
+// lane (coalesced scalar loads of every slice, one conflict-free vector store per pixel).
+// ------------------------------------------------------------------------------------------
+constexpr int FPG_TR = 32;                         // rows per staged chunk
+constexpr int FPG_RPT = FPG_TR / FP_LR;            // 8 samples per thread per chunk
+// 64 x 32 chunk rotated: x extent <= sqrt(63^2 + 31^2) = 70.2 (+ 11 for taps, margins and the
+// float4-aligned origin of chunk_box) -> 80; y extent 70.2 + 5 -> 76 rows.
+constexpr int FPG_BOX_W = 80;
+constexpr int FPG_BOX_H = 76;
+constexpr int FPG_MAX_CHUNKS = (8192 + FPG_TR - 1) / FPG_TR;
+static_assert(FPG_MAX_CHUNKS <= FP_THREADS, "one thread per chunk box");
+constexpr int FPG_FILL_PX = (FPG_BOX_W + 31) / 32;  // pixels per lane per box row
+constexpr float FPG_SLAB_EPS = 0.01f;              // slab widening of a box row (y)
+constexpr float FPG_X_MARGIN = 0.5f;               // column range widening (x)
+
+template <int G>
+__host__ __device__ constexpr int fpg_bank_groups() { return 32 / G; }  // banks of G-float elements
+template <int G>
+constexpr size_t fpg_smem_bytes() {
+  return (size_t)(FPG_BOX_W + fpg_bank_groups<G>() - 1) * FPG_BOX_H * G * sizeof(float);
+}
+
+template <int G>
+struct FpgElem;
+template <>
+struct FpgElem<2> {
+  static __device__ __forceinline__ void load(const float* z, int e, float (&v)[2]) {
+    const float2 t = reinterpret_cast<const float2*>(z)[e];
+    v[0] = t.x; v[1] = t.y;
+  }
+  static __device__ __forceinline__ void store(float* z, int e, const float (&v)[2]) {
+    reinterpret_cast<float2*>(z)[e] = make_float2(v[0], v[1]);
+  }
+};
+template <>
+struct FpgElem<4> {
+  static __device__ __forceinline__ void load(const float* z, int e, float (&v)[4]) {
+    const float4 t = reinterpret_cast<const float4*>(z)[e];
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  }
+  static __device__ __forceinline__ void store(float* z, int e, const float (&v)[4]) {
+    reinterpret_cast<float4*>(z)[e] = make_float4(v[0], v[1], v[2], v[3]);
+  }
+};
+
+// Image columns [*lo, *hi] that the bilinear taps of a chunk can read in image row y.  Samples
+// whose floor(py) is y - 1 or y lie in the slab y - 1 <= py < y + 1; their x over the chunk's
+// parallelogram (corners (px[k], py[k]) in cyclic order, sample positions of the corner samples)
+// is the range of its edges clipped to the slab, widened by FPG_X_MARGIN against rounding and
+// by the right tap.  *lo > *hi when no sample reads the row.
+__device__ __forceinline__ void fpg_row_columns(const float (&px)[4], const float (&py)[4], int y, int* lo, int* hi) {
+  const float ylo = (float)y - 1.f - FPG_SLAB_EPS, yhi = (float)y + 1.f + FPG_SLAB_EPS;
+  float xmin = 3.0e38f, xmax = -3.0e38f;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const float xa = px[e], ya = py[e], xb = px[(e + 1) & 3], yb = py[(e + 1) & 3];
+    float t0 = 0.f, t1 = 1.f;
+    const float dy = yb - ya;
+    if (fabsf(dy) < 1e-6f) {
+      if (ya < ylo || ya > yhi) continue;
+    } else {
+      float ta = (ylo - ya) / dy, tb = (yhi - ya) / dy;
+      if (ta > tb) { const float t = ta; ta = tb; tb = t; }
+      t0 = fmaxf(ta, 0.f);
+      t1 = fminf(tb, 1.f);
+      if (t0 > t1) continue;
+    }
+    const float x0 = fmaf(t0, xb - xa, xa), x1 = fmaf(t1, xb - xa, xa);
+    xmin = fminf(xmin, fminf(x0, x1));
+    xmax = fmaxf(xmax, fmaxf(x0, x1));
+  }
+  if (xmin > xmax) {
+    *lo = 1;
+    *hi = 0;
+    return;
+  }
+  *lo = (int)floorf(xmin - FPG_X_MARGIN);
+  *hi = (int)floorf(xmax + FPG_X_MARGIN) + 1;
+}
+
+template <int EPI, bool HAS_MAPS, int MAPS_DTYPE, int G>
+__global__ void __launch_bounds__(FP_THREADS, G == 4 ? 2 : 3) fp_group_kernel(FpArgs args) {
+  extern __shared__ __align__(16) float zg[];  // [FPG_BOX_H][stride] elements of G floats
+  __shared__ double red_d[FP_TC / FP_LC];
+  __shared__ int4 box_sh[FPG_MAX_CHUNKS];
+  __shared__ int2 cols_sh[FPG_BOX_H];          // staged columns [x, y] of every box row
+
+  const int n = args.n;
+  const int band = blockIdx.x;
+  const int ad = blockIdx.y;
+  const int s0 = blockIdx.z * G;
+  bool ok[G];
+  bool any = false;
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
+    const int s = s0 + g;
+    ok[g] = s < args.n_slices && (args.active == nullptr || args.active[s] != 0);
+    any = any || ok[g];
+  }
+  if (!any) return;  // the whole CTA
+  const int a = ad / args.n_det;
+  const int d = ad - a * args.n_det;
+
+  const float* M = args.fp_matrix + 6 * a;
+  const float m00 = M[0], m01 = M[1], m02 = M[2], m10 = M[3], m11 = M[4], m12 = M[5];
+  constexpr int NB = fpg_bank_groups<G>();
+  const int res = args.bank_residues != nullptr ? args.bank_residues[2 * a + (G == 4 ? 1 : 0)] : FPG_BOX_W;
+  const int S = FPG_BOX_W + (((res - FPG_BOX_W) % NB) + NB) % NB;  // row stride in elements
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int lc = lane & (FP_LC - 1);
+  const int lr = lane / FP_LC;
+  const int c0 = band * FP_TC;
+  const int c = c0 + warp * FP_LC + lc;
+  const int c_last = min(c0 + FP_TC, n) - 1;
+
+  const float* vol[G];
+  MapRef mref[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
+    const int s = ok[g] ? s0 + g : s0;
+    vol[g] = args.vol + (int64_t)s * n * n;
+    mref[g] = make_map_ref(args.maps, MAPS_DTYPE, args.maps_slice_stride, args.n_angles, args.n_det, n, s, a, d,
+                           args.n_channels, args.chan_scale);
+  }
+  const float fc = (float)c;
+  const float pxc = fmaf(m00, fc, m02);
+  const float pyc = fmaf(m10, fc, m12);
+
+  if (tid * FPG_TR < n) {
+    int4 b;
+    chunk_box(m00, m01, m02, m10, m11, m12, c0, c_last, tid * FPG_TR, min((tid + 1) * FPG_TR, n) - 1, b.x, b.y, b.z,
+              b.w);
+    box_sh[tid] = b;
+  }
+  __syncthreads();
+
+  float acc[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) acc[g] = 0.f;
+
+  for (int r0 = 0; r0 < n; r0 += FPG_TR) {
+    const int r_last = min(r0 + FPG_TR, n) - 1;
+    const int4 box = box_sh[r0 / FPG_TR];
+    const int bx0 = box.x, bx1 = box.y, by0 = box.z, by1 = box.w;
+    const int q4 = (bx1 - bx0) / 4 + 1;
+    const int bh = by1 - by0 + 1;
+    if (4 * q4 > FPG_BOX_W || bh > FPG_BOX_H) {  // cannot happen for valid matrices; never trap
+      if (tid == 0) atomicExch(&g_box_overflow, 1);
+      return;
+    }
+
+    // columns of every box row that the chunk's taps read, clipped to the box
+    if (tid < bh) {
+      float px[4], py[4];
+      const float fc0 = (float)c0, fc1 = (float)c_last, fr0 = (float)r0, fr1 = (float)r_last;
+      px[0] = sample_x(m00, m01, m02, fc0, fr0); py[0] = sample_x(m10, m11, m12, fc0, fr0);
+      px[1] = sample_x(m00, m01, m02, fc1, fr0); py[1] = sample_x(m10, m11, m12, fc1, fr0);
+      px[2] = sample_x(m00, m01, m02, fc1, fr1); py[2] = sample_x(m10, m11, m12, fc1, fr1);
+      px[3] = sample_x(m00, m01, m02, fc0, fr1); py[3] = sample_x(m10, m11, m12, fc0, fr1);
+      int lo, hi;
+      fpg_row_columns(px, py, by0 + tid, &lo, &hi);
+      cols_sh[tid] = make_int2(max(lo, bx0), min(hi, bx0 + 4 * q4 - 1));
+    }
+    __syncthreads();
+
+    // stage z = x * map of the G slices: warp w fills box rows w, w + 8, ..., one pixel per lane
+    for (int rr = warp; rr < bh; rr += FP_THREADS / 32) {
+      const int2 cols = cols_sh[rr];
+      const int gy = by0 + rr;
+      const bool yin = (unsigned)gy < (unsigned)n;
+      float v[FPG_FILL_PX][G];
+#pragma unroll
+      for (int j = 0; j < FPG_FILL_PX; ++j) {
+        const int gx = cols.x + lane + 32 * j;
+        const bool in = yin && gx <= cols.y && (unsigned)gx < (unsigned)n;
+        const int off = gy * n + gx;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          float val = 0.f;
+          if (in && ok[g]) {
+            val = __ldg(vol[g] + off);
+            if (HAS_MAPS) val *= map_at<MAPS_DTYPE>(mref[g], off);
+          }
+          v[j][g] = val;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < FPG_FILL_PX; ++j) {
+        const int gx = cols.x + lane + 32 * j;
+        if (gx <= cols.y) FpgElem<G>::store(zg, rr * S + (gx - bx0), v[j]);
+      }
+    }
+    __syncthreads();
+
+    if (c <= c_last) {
+      const int zoff = -by0 * S - bx0;
+      float fr = (float)(r0 + lr);
+      const int rem = r_last - r0 - lr;
+      const int kmax = rem >= 0 ? rem / FP_LR + 1 : 0;
+#pragma unroll 2
+      for (int k = 0; k < kmax; ++k) {
+        const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
+        const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
+        const int q = fy.i * S + fx.i + zoff;
+        float t0[G], t1[G], b0[G], b1[G];
+        FpgElem<G>::load(zg, q, t0);
+        FpgElem<G>::load(zg, q + 1, t1);
+        FpgElem<G>::load(zg, q + S, b0);
+        FpgElem<G>::load(zg, q + S + 1, b1);
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          const float top = fmaf(fx.f, t1[g] - t0[g], t0[g]);
+          const float bot = fmaf(fx.f, b1[g] - b0[g], b0[g]);
+          acc[g] += fmaf(fy.f, bot - top, top);
+        }
+        fr += (float)FP_LR;
+      }
+    }
+    __syncthreads();
+  }
+
+  const int n_bands = gridDim.x;
+  const int n_ad = gridDim.y;
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
+    if (!ok[g]) continue;  // uniform across the CTA
+    const int s = s0 + g;
+    float col = acc[g];
+    col += __shfl_xor_sync(0xffffffffu, col, 8);
+    col += __shfl_xor_sync(0xffffffffu, col, 16);
+    double part = 0.0, ptest = 0.0;
+    if (lr == 0 && c <= c_last) {
+      float total = col;
+      if (args.weights != nullptr) total *= args.weights[a * args.n_det + d];
+      const int64_t idx = (((int64_t)s * args.n_det + d) * args.n_angles + a) * n + c;
+      part = fp_epilogue<EPI>(args, idx, total, &ptest);
+    }
+    if (EPI == FP_EPI_MLEM || EPI == FP_EPI_SIRT) {
+      const int64_t slot = (int64_t)s * n_bands * n_ad + (int64_t)ad * n_bands + band;
+      fp_write_partial(part, args.partials, slot, red_d, lane, warp, tid);
+      if (args.partials_test != nullptr) fp_write_partial(ptest, args.partials_test, slot, red_d, lane, warp, tid);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
 // Back projection (reference iradon discretisation, optional maps x weights)
 // ------------------------------------------------------------------------------------------
 constexpr int BP_TJ = 32;                                // tile columns (one per lane)
@@ -792,6 +1053,7 @@ void launch_psf(const FpArgs& a, const float* psf, int psf_len, cudaStream_t st)
 // ------------------------------------------------------------------------------------------
 // Launchers
 // ------------------------------------------------------------------------------------------
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link needed)
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -835,16 +1097,26 @@ static bool launch_fp_tma_inst(const FpArgs& a, const dim3& grid, cudaStream_t s
   }
   const size_t smem = FPT_BOX_H * FPT_BOX_W * sizeof(float) +
                       (HAS_MAPS ? FPT_BOX_H * FPT_BOX_W * (MAPS_DTYPE == CCT_DTYPE_BF16 ? 2 : 4) : 0);
-  static bool attr_set = false;
-  if (!attr_set) {
-    if (cudaFuncSetAttribute(fp_tma_kernel<EPI, HAS_MAPS, MAPS_DTYPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess) {
-      return false;
-    }
-    attr_set = true;
-  }
+  if (!ensure_dynamic_smem<fp_tma_kernel<EPI, HAS_MAPS, MAPS_DTYPE>>((int)smem)) return false;
   fp_tma_kernel<EPI, HAS_MAPS, MAPS_DTYPE><<<grid, FP_THREADS, smem, st>>>(a, tv, tm);
-  return true;
+  return launched_ok();
+}
+
+template <int EPI, bool HAS_MAPS, int MAPS_DTYPE, int G>
+static bool launch_fp_group_inst(const FpArgs& a, cudaStream_t st) {
+  const dim3 grid((a.n + FP_TC - 1) / FP_TC, a.n_angles * a.n_det, (a.n_slices + G - 1) / G);
+  const size_t smem = fpg_smem_bytes<G>();
+  if (!ensure_dynamic_smem<fp_group_kernel<EPI, HAS_MAPS, MAPS_DTYPE, G>>((int)smem)) return false;
+  fp_group_kernel<EPI, HAS_MAPS, MAPS_DTYPE, G><<<grid, FP_THREADS, smem, st>>>(a);
+  return launched_ok();
+}
+
+template <int EPI, int G>
+static bool launch_fp_group(const FpArgs& a, cudaStream_t st) {
+  if (a.maps == nullptr) return launch_fp_group_inst<EPI, false, CCT_DTYPE_F32, G>(a, st);
+  if (a.maps_dtype == CCT_DTYPE_BF16) return launch_fp_group_inst<EPI, true, CCT_DTYPE_BF16, G>(a, st);
+  if (a.maps_dtype == CCT_DTYPE_FIELDS_F32) return launch_fp_group_inst<EPI, true, CCT_DTYPE_FIELDS_F32, G>(a, st);
+  return launch_fp_group_inst<EPI, true, CCT_DTYPE_F32, G>(a, st);
 }
 
 // 16-byte staging loads need a 16-byte aligned volume, maps at 16 (FP32) or 8 (BF16) bytes and
@@ -858,6 +1130,9 @@ bool fp_vec4_ok(const FpArgs& a) {
 template <int EPI>
 static void launch_fp_epi(const FpArgs& a, cudaStream_t st) {
   const dim3 grid((a.n + FP_TC - 1) / FP_TC, a.n_angles * a.n_det, a.n_slices);
+  // slice groups: any n, maps stride and storage type; the plain kernel if the launch is refused
+  if ((a.variant & CCT_VARIANT_FP_SLICES4) && launch_fp_group<EPI, 4>(a, st)) return;
+  if ((a.variant & CCT_VARIANT_FP_SLICES2) && launch_fp_group<EPI, 2>(a, st)) return;
   // TMA path: rows and images must be 16-byte multiples for both FP32 and BF16 boxes
   const int64_t dense = (int64_t)a.n_angles * a.n_det * a.n * a.n;
   const bool aligned = (a.n % 8) == 0 && (reinterpret_cast<uintptr_t>(a.vol) % 16) == 0 &&

@@ -254,6 +254,8 @@ class BatchedSolver:
                 self.x *= self.x_mask
         else:
             self.x.copy_(x0)
+            if self.x_mask is not None and self.method == "mlem":
+                self.x *= self.x_mask  # as __init__ (the reference masks x0 too, solvers.py:750-752)
         if self.x_relax is not None:
             self.x_relax.copy_(self.x)
         if self.tv_dual is not None:

@@ -46,6 +46,56 @@ def fp_matrices(angles_deg32: NDArray, n: int) -> NDArray:
     return out
 
 
+FP_BANK_GROUPS = (16, 8)  # shared-memory banks of 8-byte (2-slice) and 16-byte (4-slice) elements
+
+
+def fp_bank_residues(fp_mat: NDArray, patches: int = 8) -> NDArray:
+    """``(A, 2)`` int32 row-stride residues of the slice-grouped forward projection's staged box:
+    column 0 modulo 16 (2 slices per element, 8-byte banks), column 1 modulo 8 (4 slices, 16-byte
+    banks).
+
+    A warp samples an 8 (columns) x 4 (rows) block of the rotated lattice (lane = 8 row-lane +
+    column-lane) and reads the four bilinear taps of every sample as one element each; the
+    shared-memory banks of an element are its index modulo the bank groups, taken per phase of
+    8 (16-byte) or 16 (8-byte) lanes.  For each angle this counts, over a few lattice blocks, the
+    wavefronts of every stride residue (distinct elements per bank, the largest per phase) and
+    keeps the cheapest.  The choice only affects speed; any residue gives the same results.
+    """
+    m = np.asarray(fp_mat, dtype=np.float64).reshape(-1, 6)
+    a = m.shape[0]
+    out = np.zeros((a, 2), dtype=np.int32)
+    if a == 0:
+        return out
+    lane = np.arange(32)
+    lc, lr = lane % 8, lane // 8
+    p = np.arange(patches)
+    c = (p[:, None] * 37 + 5) % 61 + lc[None, :]          # (P, 32) lattice columns
+    r = (p[:, None] * 53 + 11) % 59 + lr[None, :]         # rows
+    px = m[:, 0, None, None] * c + m[:, 1, None, None] * r + m[:, 2, None, None]
+    py = m[:, 3, None, None] * c + m[:, 4, None, None] * r + m[:, 5, None, None]
+    fx = np.floor(px).astype(np.int64)                    # (A, P, 32)
+    fy = np.floor(py).astype(np.int64)
+    taps = ((0, 0), (0, 1), (1, 0), (1, 1))
+    for col, nb in enumerate(FP_BANK_GROUPS):
+        lanes = nb  # a phase moves 128 bytes: nb elements of 128 / nb bytes
+        cand = np.arange(nb)
+        stride = 128 + cand                               # residue r <-> stride = r (mod nb)
+        cost = np.zeros((a, nb))
+        for dy, dx in taps:
+            e = (fy[:, None] + dy) * stride[None, :, None, None] + fx[:, None] + dx    # (A, C, P, 32)
+            e = e.reshape(a, nb, patches, 32 // lanes, lanes)
+            e = np.sort(e, axis=-1)
+            distinct = np.ones(e.shape, dtype=bool)
+            distinct[..., 1:] = e[..., 1:] != e[..., :-1]
+            bank = np.mod(e, nb)
+            groups = np.arange(e[..., 0].size).reshape(e.shape[:-1])
+            key = (groups[..., None] * nb + bank)[distinct]
+            counts = np.bincount(key, minlength=groups.size * nb).reshape(*e.shape[:-1], nb)
+            cost += counts.max(axis=-1).sum(axis=(-1, -2))
+        out[:, col] = np.argmin(cost, axis=1)
+    return out
+
+
 def bp_trig(angles_deg32: NDArray) -> NDArray:
     """``(A, 2)`` float32 ``(cos, sin)`` of iradon per angle."""
     angle = np.deg2rad(np.asarray(angles_deg32, dtype=np.float32))

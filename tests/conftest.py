@@ -29,3 +29,16 @@ def rel_l2(a, b) -> float:
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def report(name: str, value: float, bound: float) -> None:
+    """Print an error against the FP64 oracle with its bound; with $CCT_PARITY_REPORT set, also
+    append it there as one JSON line (the GPU runs collect these figures)."""
+    import json
+
+    line = {"case": name, "rel_l2": float(value), "bound": float(bound)}
+    print(f"parity {name}: rel-L2 {value:.3e} (bound {bound:.0e})")
+    path = os.environ.get("CCT_PARITY_REPORT")
+    if path:
+        with open(path, "a") as fh:
+            fh.write(json.dumps(line) + "\n")

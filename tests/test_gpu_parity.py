@@ -208,6 +208,19 @@ def test_solvers_with_mask_and_limits_match_reference(golden_cases, cuda):
     xp, _ = solvers.PDHG(data_term="kl", regularizer=1e-2)(p, g["b"], iterations=10, x_mask=m, lower_limit=0.0,
                                                           upper_limit=3.0)
     assert rel_l2(xp, o["pdhg_x"]) < TOL_RECON
+    # a restart from an unmasked x0 masks it, as the constructor does (solvers.py:750-752)
+    from pycorrectedemissionct_b200 import core, engine
+
+    c = core.XrfCore(n, g["angles"], device=cuda)
+    b = _t(g["b"], cuda).reshape(1, 1, len(g["angles"]), n)
+    sv = engine.BatchedSolver(c, _t(g["maps"], cuda)[None], b, "mlem", x_mask=_t(m, cuda), lower_limit=0.0,
+                              upper_limit=2.0)
+    sv.run(10, use_graph=False)
+    first = sv.x.clone()
+    assert rel_l2(first[0].cpu().numpy(), o["mlem_x"]) < TOL_RECON
+    sv.reset(torch.ones_like(sv.x))
+    sv.run(10, use_graph=False)
+    assert torch.equal(sv.x, first)
 
 
 def test_lipschitz_scaled_solvers_match_reference(golden_cases, cuda):
@@ -374,21 +387,80 @@ def test_engine_tolerance_and_graph(cuda):
     assert torch.equal(stop.history[:, : int(expect.min())], eager.history[:, : int(expect.min())])
 
 
-@pytest.mark.parametrize("n,n_ang,dtype", [(64, 48, torch.float32), (512, 90, torch.float32), (512, 90, torch.bfloat16)])
-def test_fp_variants_bit_identical(n, n_ang, dtype, cuda, tmp_path, monkeypatch):
-    from pycorrectedemissionct_b200 import _lib, autotune, core, phantoms
+ALL_FP_VARIANTS = ("tma", "slices2", "slices4")
+
+
+def _variant(name):
+    from pycorrectedemissionct_b200 import _lib
+
+    return {"ldg": 0, "tma": _lib.CCT_VARIANT_FP_TMA, "slices2": _lib.CCT_VARIANT_FP_SLICES2,
+            "slices4": _lib.CCT_VARIANT_FP_SLICES4}[name]
+
+
+@pytest.mark.parametrize("n,n_ang,dtype,s", [(64, 48, "float32", 5), (512, 90, "float32", 5), (512, 90, "bfloat16", 4),
+                                             (130, 45, "float32", 3), (1000, 12, "float32", 2), (66, 30, "fields", 6)])
+def test_fp_variants_bit_identical(n, n_ang, dtype, s, cuda, tmp_path, monkeypatch):
+    """Every fp variant (one slice per CTA with load/store or TMA staging, two or four slices per
+    CTA) gives bit-identical projections, for batches that are not a multiple of the group, for
+    every maps storage type and for an angle range of larger maps; the autotuner picks one of
+    them and caches it."""
+    from pycorrectedemissionct_b200 import autotune, core, phantoms
 
     rng = phantoms.slice_rng(77, n)
-    x = _t(np.stack([phantoms.ellipse_phantom(n, rng) for _ in range(2)]), cuda)
-    maps = _t(rng.uniform(0.3, 1.0, size=(2, n_ang, 1, n, n)), cuda, dtype)
+    x = _t(np.stack([phantoms.ellipse_phantom(n, rng) for _ in range(s)]), cuda)
     c = core.XrfCore(n, phantoms.angles(n_ang), device=cuda)
+    if dtype == "fields":
+        c.set_channels([0.5, 1.0, 3.0])
+        maps = _t(rng.uniform(0.0, 0.3, size=(s // 3, n_ang, 2, n, n)), cuda)
+    else:
+        maps = _t(rng.uniform(0.3, 1.0, size=(s, n_ang, 1, n, n)), cuda,
+                  torch.bfloat16 if dtype == "bfloat16" else torch.float32)
     ref = c.fp(x, maps)
-    c.variant = _lib.CCT_VARIANT_FP_TMA
-    assert torch.equal(c.fp(x, maps), ref)
+    sub = c.angle_range(slice(n_ang // 3, n_ang // 3 + 7))
+    ref_sub = sub.fp(x, maps[:, n_ang // 3: n_ang // 3 + 7])
+    for name in ALL_FP_VARIANTS:
+        c.variant = sub.variant = _variant(name)
+        assert torch.equal(c.fp(x, maps), ref), name
+        assert torch.equal(sub.fp(x, maps[:, n_ang // 3: n_ang // 3 + 7]), ref_sub), name
+    c.variant = 0
     monkeypatch.setenv("CCT_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
     v = autotune.tune(c, x, maps)
     assert v in autotune.VARIANTS and (tmp_path / "tune.json").exists()
     assert torch.equal(c.fp(x, maps), ref)
+
+
+@pytest.mark.parametrize("method", ["mlem", "sirt", "pdhg"])
+def test_fused_solvers_identical_across_fp_variants(method, cuda):
+    """The fused solver epilogues (MLEM ratio and KL residual, SIRT residual, PDHG dual) give the
+    same iterates, residuals and stopping decisions with every fp variant, including a slice that
+    stops early (its group-mates keep iterating)."""
+    from pycorrectedemissionct_b200 import core, engine, phantoms
+
+    n, n_ang, s = 96, 40, 5
+    angles = phantoms.angles(n_ang)
+    mus = np.stack([phantoms.disk_attenuation(n, phantoms.slice_rng(31, k), 0.02) for k in range(s)])
+    xs = np.stack([phantoms.ellipse_phantom(n, phantoms.slice_rng(32, k)) for k in range(s)])
+    maps = core.compute_maps(_t(mus, cuda), _t(0.7 * mus, cuda), np.array(angles, dtype=np.float32))
+    c = core.XrfCore(n, angles, device=cuda)
+    clean = c.fp(_t(xs, cuda), maps)
+    b = torch.poisson(clean / clean.amax(dim=(1, 2, 3), keepdim=True) * 1e4)
+    probe = engine.BatchedSolver(c, maps, b, method, history_len=6)
+    probe.run(6, check_every=6, use_graph=False)
+    res = probe.history.cpu().numpy()
+    tol = np.full(s, -1.0)
+    if method != "pdhg":
+        tol[1] = res[1, 2] * (1 + 1e-9)  # slice 1 stops after its third iteration
+    results = {}
+    for name in ("ldg",) + ALL_FP_VARIANTS:
+        c.variant = _variant(name)
+        sv = engine.BatchedSolver(c, maps, b, method, tolerance=tol, history_len=6)
+        sv.run(6, check_every=6, use_graph=False)
+        results[name] = (sv.x.clone(), sv.history.clone(), sv.iterations.clone())
+    for name in ALL_FP_VARIANTS:
+        for got, want in zip(results[name], results["ldg"]):
+            assert torch.equal(got, want), name
+    if method != "pdhg":
+        assert int(results["ldg"][2][1]) == 3
 
 
 def test_finite_surface_detectors_match_reference(cuda):

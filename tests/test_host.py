@@ -361,6 +361,83 @@ def test_fp_chunk_boxes_hold_every_tap(n):
                 assert y.min() >= by0 and y.max() + 1 <= by1
 
 
+def _fma32(a, b, c):
+    """fmaf in FP32 (exact product in FP64, then the sum rounded to FP32)."""
+    return (np.float64(a) * np.float64(b) + np.float64(c)).astype(np.float32)
+
+
+@pytest.mark.parametrize("n", [32, 130, 512, 1000])
+def test_fp_group_staged_columns_hold_every_tap(n):
+    """The slice-grouped forward projection (fp_group_kernel in csrc/cct_project.cu) stages, per
+    64 x 32 chunk, only the columns of each box row that fpg_row_columns finds (the chunk's
+    parallelogram clipped to the row's slab, widened by 0.5 and the right tap) and reads the taps
+    without tests: mirror that FP32 arithmetic and check that every tap of every sample lies in the
+    staged columns of its row, and that the box fits 80 x 76."""
+    from pycorrectedemissionct_b200 import geometry
+
+    TC, TR, BOX_W, BOX_H, EPS, MARGIN = 64, 32, 80, 76, np.float32(0.01), np.float32(0.5)
+    angles = np.concatenate([np.linspace(0, 2 * np.pi, 40, endpoint=False),
+                             [np.pi / 4, 3 * np.pi / 4, 1e-6, np.pi / 2 + 1e-7, 0.3e-3]])
+    mats = geometry.fp_matrices(np.rad2deg(np.array(angles, dtype=np.float32)), n)
+    f32 = np.float32
+
+    def row_columns(px, py, y):
+        ylo, yhi = f32(f32(y) - f32(1)) - EPS, f32(f32(y) + f32(1)) + EPS
+        xmin, xmax = f32(3e38), f32(-3e38)
+        for e in range(4):
+            xa, ya, xb, yb = px[e], py[e], px[(e + 1) % 4], py[(e + 1) % 4]
+            t0, t1 = f32(0), f32(1)
+            dy = f32(yb - ya)
+            if abs(dy) < f32(1e-6):
+                if ya < ylo or ya > yhi:
+                    continue
+            else:
+                ta, tb = f32(f32(ylo - ya) / dy), f32(f32(yhi - ya) / dy)
+                if ta > tb:
+                    ta, tb = tb, ta
+                t0, t1 = max(ta, f32(0)), min(tb, f32(1))
+                if t0 > t1:
+                    continue
+            x0, x1 = _fma32(t0, f32(xb - xa), xa), _fma32(t1, f32(xb - xa), xa)
+            xmin, xmax = min(xmin, x0, x1), max(xmax, x0, x1)
+        if xmin > xmax:
+            return 1, 0
+        return int(np.floor(f32(xmin - MARGIN))), int(np.floor(f32(xmax + MARGIN))) + 1
+
+    for m in mats:
+        m00, m01, m02, m10, m11, m12 = (f32(v) for v in m)
+        for c0 in range(0, n, TC):
+            c_last = min(c0 + TC, n) - 1
+            for r0 in range(0, n, TR):
+                r_last = min(r0 + TR, n) - 1
+                cs = np.array([c0, c_last, c_last, c0], dtype=np.float32)   # cyclic corner order
+                rs = np.array([r0, r0, r_last, r_last], dtype=np.float32)
+                px = _fma32(m01, rs, _fma32(m00, cs, m02))
+                py = _fma32(m11, rs, _fma32(m10, cs, m12))
+                bx0 = (int(np.floor(px.min())) - 1) & ~3
+                bx1 = int(np.floor(px.max())) + 2
+                by0 = int(np.floor(py.min())) - 1
+                by1 = int(np.floor(py.max())) + 2
+                q4 = (bx1 - bx0) // 4 + 1
+                bh = by1 - by0 + 1
+                assert 4 * q4 <= BOX_W and bh <= BOX_H
+                lo = np.empty(bh, dtype=np.int64)
+                hi = np.empty(bh, dtype=np.int64)
+                for t in range(bh):
+                    a_, b_ = row_columns(px, py, by0 + t)
+                    lo[t], hi[t] = max(a_, bx0), min(b_, bx0 + 4 * q4 - 1)
+                cc, rr = np.meshgrid(np.arange(c0, c_last + 1, dtype=np.float32),
+                                     np.arange(r0, r_last + 1, dtype=np.float32))
+                pxc = _fma32(m00, cc, m02)
+                pyc = _fma32(m10, cc, m12)
+                x = np.floor(_fma32(m01, rr, pxc)).astype(np.int64).ravel()
+                y = np.floor(_fma32(m11, rr, pyc)).astype(np.int64).ravel()
+                for dy in (0, 1):
+                    row = y + dy - by0
+                    assert row.min() >= 0 and row.max() < bh
+                    assert (x >= lo[row]).all() and (x + 1 <= hi[row]).all()
+
+
 @pytest.mark.parametrize("n", [32, 130, 512])
 def test_bp_staged_bins_cover_every_lookup(n):
     """The back projection stages, per 32 x 64 pixel tile and line, 80 (value, slope) pairs from
