@@ -59,8 +59,6 @@ extern "C" {
                                 (needs n % 8 == 0; otherwise the load/store staging is used) */
 #define CCT_VARIANT_FP_SLICES2 2 /* forward projection: one CTA per two slices of the batch (shared
                                     sample coordinates, one 8-byte shared load per tap for both) */
-#define CCT_VARIANT_FP_SLICES4 4 /* four slices per CTA (16-byte taps); wins over SLICES2 when both
-                                    are set */
 
 /* Geometry of a batch of slices that share n, the angles and the detectors. */
 typedef struct cct_xrf_desc {
@@ -88,10 +86,12 @@ typedef struct cct_xrf_desc {
                                 slices); 0 = dense (n_angles * n_det * n * n, or n_angles * (1 + n_det)
                                 * n * n for fields).  Lets a call read an angle range of a larger array. */
   const float* channel_scale; /* device [n_channels]: s_c of CCT_DTYPE_FIELDS_F32 */
-  const int32_t* fp_bank_residues; /* device [A][2] or NULL: per angle, the row-stride residues (mod 16
-                                      and mod 8) of the slice-grouped forward projection's staged box,
-                                      chosen to spread the angle's bilinear taps over the shared-memory
-                                      banks; speed only, any values give the same results */
+  const int32_t* fp_box_strides; /* device [A][2] or NULL (all 0): per angle, row-stride selectors of the
+                                    forward projection's staged box: column 1 for two slices per CTA
+                                    (stride 80 + 2v elements, v in 0..4; column 0 is reserved, 0),
+                                    chosen on the host to spread the angle's bilinear taps over the
+                                    shared-memory banks.  Speed only: any values give the same
+                                    results. */
 } cct_xrf_desc;
 
 /* Library identity. */

@@ -30,7 +30,6 @@ CCT_BP_ADJOINT = 2
 
 CCT_VARIANT_FP_TMA = 1
 CCT_VARIANT_FP_SLICES2 = 2
-CCT_VARIANT_FP_SLICES4 = 4
 
 CCT_METHOD_MLEM = 0
 CCT_METHOD_SIRT = 1
@@ -55,7 +54,7 @@ class XrfDesc(ctypes.Structure):
         ("n_channels", ctypes.c_int32),
         ("maps_slice_stride", ctypes.c_int64),
         ("channel_scale", ctypes.c_void_p),
-        ("fp_bank_residues", ctypes.c_void_p),
+        ("fp_box_strides", ctypes.c_void_p),
     ]
 
 

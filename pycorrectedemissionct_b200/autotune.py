@@ -1,8 +1,8 @@
 """Kernel-variant autotuner with an on-disk cache.
 
-The fp kernel has four variants with identical results: one slice per CTA with load/store
-staging (default) or TMA bulk-tensor staging (``CCT_VARIANT_FP_TMA``), and two or four slices
-per CTA sharing the sample coordinates (``CCT_VARIANT_FP_SLICES2`` / ``SLICES4``).  Which is
+The fp kernel has three variants with identical results: one slice per CTA with load/store
+staging (default) or TMA bulk-tensor staging (``CCT_VARIANT_FP_TMA``), and two slices per CTA
+sharing the sample coordinates (``CCT_VARIANT_FP_SLICES2``).  Which is
 faster depends on n, the angle count, the map type, the batch and whether the maps are an
 angle range of a larger array (the TMA variant needs dense maps), so ``tune`` times every
 applicable variant on the actual call (CUDA events, a few launches over a batch of the real
@@ -22,7 +22,7 @@ from . import _lib
 from .core import XrfCore
 
 _LOCK = threading.Lock()
-VARIANTS = (0, _lib.CCT_VARIANT_FP_TMA, _lib.CCT_VARIANT_FP_SLICES2, _lib.CCT_VARIANT_FP_SLICES4)
+VARIANTS = (0, _lib.CCT_VARIANT_FP_TMA, _lib.CCT_VARIANT_FP_SLICES2)
 
 
 def cache_path() -> str:
@@ -87,8 +87,6 @@ def tune(core: XrfCore, vol: torch.Tensor, maps: torch.Tensor, force: bool = Fal
             if v == _lib.CCT_VARIANT_FP_TMA and (core.n % 8 != 0 or not dense):
                 continue
             if v == _lib.CCT_VARIANT_FP_SLICES2 and vol.shape[0] < 2:
-                continue
-            if v == _lib.CCT_VARIANT_FP_SLICES4 and vol.shape[0] < 3:
                 continue
             times[v] = time_fp(core, vol, maps, v)
         best = min(times, key=times.get)

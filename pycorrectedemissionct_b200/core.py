@@ -94,7 +94,7 @@ class XrfCore:
         self.fp_mat = torch.from_numpy(self.fp_mat_np).to(self.device)
         self.trig = torch.from_numpy(self.trig_np).to(self.device)
         # per-angle staged-box strides of the slice-grouped fp (speed only)
-        self.bank_res = torch.from_numpy(geometry.fp_bank_residues(self.fp_mat_np)).to(self.device)
+        self.box_strides = torch.from_numpy(geometry.fp_box_strides(self.fp_mat_np)).to(self.device)
         self.intensities_np = None
         self.line_scale = None
         self.psf = None
@@ -161,7 +161,7 @@ class XrfCore:
         sub.angles_rad32, sub.angles_deg32 = self.angles_rad32[rng], self.angles_deg32[rng]
         sub.n_angles = len(sub.angles_rad32)
         sub.fp_mat_np, sub.trig_np = self.fp_mat_np[rng], self.trig_np[rng]
-        sub.fp_mat, sub.trig, sub.bank_res = self.fp_mat[rng], self.trig[rng], self.bank_res[rng]
+        sub.fp_mat, sub.trig, sub.box_strides = self.fp_mat[rng], self.trig[rng], self.box_strides[rng]
         sub.intensities_np = None if self.intensities_np is None else self.intensities_np[rng]
         sub.line_scale = None if self.line_scale is None else self.line_scale[rng]
         sub.psf = self.psf
@@ -185,7 +185,7 @@ class XrfCore:
             d.bp_trig = self.trig.data_ptr()
             d.weights = _ptr(self.weights)
             d.line_scale = _ptr(self.line_scale)
-            d.fp_bank_residues = self.bank_res.data_ptr()
+            d.fp_box_strides = self.box_strides.data_ptr()
         else:
             a0, a1 = angles.start, angles.stop
             d.n_angles = a1 - a0
@@ -193,7 +193,7 @@ class XrfCore:
             d.bp_trig = self.trig[a0:a1].data_ptr()
             d.weights = None if self.weights is None else self.weights[a0:a1].data_ptr()
             d.line_scale = None if self.line_scale is None else self.line_scale[a0:a1].data_ptr()
-            d.fp_bank_residues = self.bank_res[a0:a1].data_ptr()
+            d.fp_box_strides = self.box_strides[a0:a1].data_ptr()
         d.psf = _ptr(self.psf)
         d.psf_len = 0 if self.psf is None else int(self.psf.numel())
         if maps_dtype == _lib.CCT_DTYPE_FIELDS_F32:

@@ -73,7 +73,7 @@ static cct::FpArgs make_fp_args(const cct_xrf_desc* d, const float* vol, const v
   a.maps_slice_stride = maps_stride(d);
   a.n_channels = d->n_channels > 0 ? d->n_channels : 1;
   a.chan_scale = d->channel_scale;
-  a.bank_residues = d->fp_bank_residues;
+  a.box_strides = d->fp_box_strides;
   return a;
 }
 

@@ -36,7 +36,7 @@ struct FpArgs {
   const float* b_mask;       // data mask of the residual, or nullptr
   const float* b_test_mask;  // cross-validation mask, or nullptr
   double* partials_test;     // per-CTA test residual partials (with b_test_mask)
-  const int* bank_residues;  // [A][2] staged-box row-stride residues of the slice-grouped fp, or nullptr
+  const int* box_strides;    // [A][2] staged-box row-stride selectors per angle (speed only), or nullptr
 };
 
 struct BpArgs {

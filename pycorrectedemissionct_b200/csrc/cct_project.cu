@@ -53,6 +53,8 @@ constexpr int FP_BOX_W = 100;
 constexpr int FP_BOX_H = 96;
 constexpr int FP_STRIDE = FP_BOX_W;                // 16-byte rows: conflict-free float4 fills
 constexpr int FP_MAX_CHUNKS = (8192 + FP_TR - 1) / FP_TR;  // row chunks of the largest n
+constexpr float FP_SLAB_EPS = 0.01f;               // slab widening of a box row (y)
+constexpr float FP_ROW_MARGIN = 0.5f;              // column range widening (x)
 static_assert(FP_MAX_CHUNKS <= FP_THREADS, "one thread per chunk box");
 constexpr int FP_FILL_BATCH = 3;                   // float4 items whose loads are issued together
 
@@ -98,6 +100,49 @@ __device__ __forceinline__ void chunk_box(float m00, float m01, float m02, float
   bx1 = (int)floorf(xmax) + 2;
   by0 = (int)floorf(ymin) - 1;
   by1 = (int)floorf(ymax) + 2;
+}
+
+// Quads (4-column groups counted from the box origin bx0) of box row y that the bilinear taps
+// of a chunk can read.  Samples whose floor(py) is y - 1 or y lie in the slab y - 1 <= py < y + 1;
+// their x over the chunk's parallelogram (corners (px[k], py[k]) in cyclic order, the positions
+// of the corner samples) is the range of its edges clipped to the slab, widened by
+// FP_ROW_MARGIN against rounding (the approximate division moves it by far less) and by the
+// right tap.  Returns (first, last) clipped to [0, q4 - 1]; first > last when no tap reads it.
+__device__ __forceinline__ short2 fp_row_quads(const float (&px)[4], const float (&py)[4], int y, int bx0, int q4) {
+  const float ylo = (float)y - 1.f - FP_SLAB_EPS, yhi = (float)y + 1.f + FP_SLAB_EPS;
+  float xmin = 3.0e38f, xmax = -3.0e38f;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const float xa = px[e], ya = py[e], xb = px[(e + 1) & 3], yb = py[(e + 1) & 3];
+    float t0 = 0.f, t1 = 1.f;
+    const float dy = yb - ya;
+    if (fabsf(dy) < 1e-6f) {
+      if (ya < ylo || ya > yhi) continue;
+    } else {
+      float ta = __fdividef(ylo - ya, dy), tb = __fdividef(yhi - ya, dy);
+      if (ta > tb) { const float t = ta; ta = tb; tb = t; }
+      t0 = fmaxf(ta, 0.f);
+      t1 = fminf(tb, 1.f);
+      if (t0 > t1) continue;
+    }
+    const float x0 = fmaf(t0, xb - xa, xa), x1 = fmaf(t1, xb - xa, xa);
+    xmin = fminf(xmin, fminf(x0, x1));
+    xmax = fmaxf(xmax, fmaxf(x0, x1));
+  }
+  if (xmin > xmax) return make_short2(1, 0);
+  const int lo = (int)floorf(xmin - FP_ROW_MARGIN) - bx0;
+  const int hi = (int)floorf(xmax + FP_ROW_MARGIN) + 1 - bx0;
+  return make_short2((short)(max(lo, 0) >> 2), (short)min(hi >> 2, q4 - 1));
+}
+
+// Positions of the four corner samples of chunk columns [c0, c1] x rows [r0, r1], cyclic order.
+__device__ __forceinline__ void chunk_corners(float m00, float m01, float m02, float m10, float m11, float m12, int c0,
+                                              int c1, int r0, int r1, float (&px)[4], float (&py)[4]) {
+  const float fc0 = (float)c0, fc1 = (float)c1, fr0 = (float)r0, fr1 = (float)r1;
+  px[0] = sample_x(m00, m01, m02, fc0, fr0); py[0] = sample_x(m10, m11, m12, fc0, fr0);
+  px[1] = sample_x(m00, m01, m02, fc1, fr0); py[1] = sample_x(m10, m11, m12, fc1, fr0);
+  px[2] = sample_x(m00, m01, m02, fc1, fr1); py[2] = sample_x(m10, m11, m12, fc1, fr1);
+  px[3] = sample_x(m00, m01, m02, fc0, fr1); py[3] = sample_x(m10, m11, m12, fc0, fr1);
 }
 
 // CTA sum of one residual partial per thread (FP64, fixed order) into partials[slot]; red
@@ -504,126 +549,76 @@ __global__ void __launch_bounds__(FP_THREADS, 2)
 }
 
 // ------------------------------------------------------------------------------------------
-// Forward projection over groups of G slices per CTA (G = 2 or 4)
+// Forward projection, two slices per CTA
 //
 // All slices of a batch share the angle's sample positions, so one CTA owns (band, angle *
-// detector, group of G slices): it computes each sample's coordinates, tap offsets and weights
-// once, stages z = x * map of its G slices interleaved (one G-float element per pixel), and
-// reads every bilinear tap of all G slices with one vector shared load.  Two further savings
-// against fp_kernel, whose arithmetic per sample is otherwise identical (bit-identical results):
-//   * each staged box row holds only the columns the chunk's taps can read (the chunk's
-//     parallelogram clipped to the row's slab), not the whole axis-aligned bounding box;
-//   * the box row stride is chosen per angle (bank_residues, from the host) so that the eight
-//     (16-byte elements) or sixteen (8-byte) lanes of a shared-memory phase hit distinct banks
-//     as often as the angle's lattice allows.
-// Chunks are 64 columns x FPG_TR rows; the fill gives each warp whole box rows, one pixel per
-// lane (coalesced scalar loads of every slice, one conflict-free vector store per pixel).
+// detector, pair of slices): it computes each sample's coordinates and tap offsets once, stages
+// z = x * map of both slices interleaved (one float2 element per pixel) and reads every
+// bilinear tap of both with one 8-byte shared load.  The arithmetic per sample and slice is
+// fp_cta's (bit-identical results).  Chunks are 64 columns x 32 rows so that three CTAs fit per
+// SM; like fp_cta, only the quads of each box row that the taps read are staged, and the row
+// stride (80 + 2v elements, v in 0..4, even so that 16-byte stores stay aligned) is chosen per angle on
+// the host (column 1 of cct_xrf_desc::fp_box_strides).  The fill loads float4 quads of both
+// slices, and writes a quad as two 16-byte element pairs; lanes 4-7 of every 8-lane store phase
+// write their second pair first, which keeps the 16-byte stores of a phase on distinct banks.
+// Four CTAs fit per SM (64 registers, < 56 KB of shared memory each).
 // ------------------------------------------------------------------------------------------
-constexpr int FPG_TR = 32;                         // rows per staged chunk
-constexpr int FPG_RPT = FPG_TR / FP_LR;            // 8 samples per thread per chunk
+constexpr int FP2_TR = 32;                          // rows per staged chunk
+constexpr int FP2_RPT = FP2_TR / FP_LR;             // 8 samples per thread per chunk
 // 64 x 32 chunk rotated: x extent <= sqrt(63^2 + 31^2) = 70.2 (+ 11 for taps, margins and the
-// float4-aligned origin of chunk_box) -> 80; y extent 70.2 + 5 -> 76 rows.
-constexpr int FPG_BOX_W = 80;
-constexpr int FPG_BOX_H = 76;
-constexpr int FPG_MAX_CHUNKS = (8192 + FPG_TR - 1) / FPG_TR;
-static_assert(FPG_MAX_CHUNKS <= FP_THREADS, "one thread per chunk box");
-constexpr int FPG_FILL_PX = (FPG_BOX_W + 31) / 32;  // pixels per lane per box row
-constexpr float FPG_SLAB_EPS = 0.01f;              // slab widening of a box row (y)
-constexpr float FPG_X_MARGIN = 0.5f;               // column range widening (x)
+// float4-aligned origin) -> 80; y extent 70.2 + 5 -> 75 rows.
+constexpr int FP2_BOX_W = 80;
+constexpr int FP2_BOX_H = 75;
+constexpr int FP2_STRIDE_MAX = FP2_BOX_W + 8;       // strides 80, 82, ..., 88 elements
+constexpr int FP2_MAX_CHUNKS = (8192 + FP2_TR - 1) / FP2_TR;
+static_assert(FP2_MAX_CHUNKS <= FP_THREADS, "one thread per chunk box");
+constexpr int FP2_FILL_BATCH = 2;
+constexpr size_t FP2_SMEM_BYTES = (size_t)FP2_STRIDE_MAX * FP2_BOX_H * sizeof(float2);
 
-template <int G>
-__host__ __device__ constexpr int fpg_bank_groups() { return 32 / G; }  // banks of G-float elements
-template <int G>
-constexpr size_t fpg_smem_bytes() {
-  return (size_t)(FPG_BOX_W + fpg_bank_groups<G>() - 1) * FPG_BOX_H * G * sizeof(float);
-}
-
-template <int G>
-struct FpgElem;
-template <>
-struct FpgElem<2> {
-  static __device__ __forceinline__ void load(const float* z, int e, float (&v)[2]) {
-    const float2 t = reinterpret_cast<const float2*>(z)[e];
-    v[0] = t.x; v[1] = t.y;
-  }
-  static __device__ __forceinline__ void store(float* z, int e, const float (&v)[2]) {
-    reinterpret_cast<float2*>(z)[e] = make_float2(v[0], v[1]);
-  }
-};
-template <>
-struct FpgElem<4> {
-  static __device__ __forceinline__ void load(const float* z, int e, float (&v)[4]) {
-    const float4 t = reinterpret_cast<const float4*>(z)[e];
-    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-  }
-  static __device__ __forceinline__ void store(float* z, int e, const float (&v)[4]) {
-    reinterpret_cast<float4*>(z)[e] = make_float4(v[0], v[1], v[2], v[3]);
-  }
-};
-
-// Image columns [*lo, *hi] that the bilinear taps of a chunk can read in image row y.  Samples
-// whose floor(py) is y - 1 or y lie in the slab y - 1 <= py < y + 1; their x over the chunk's
-// parallelogram (corners (px[k], py[k]) in cyclic order, sample positions of the corner samples)
-// is the range of its edges clipped to the slab, widened by FPG_X_MARGIN against rounding and
-// by the right tap.  *lo > *hi when no sample reads the row.
-__device__ __forceinline__ void fpg_row_columns(const float (&px)[4], const float (&py)[4], int y, int* lo, int* hi) {
-  const float ylo = (float)y - 1.f - FPG_SLAB_EPS, yhi = (float)y + 1.f + FPG_SLAB_EPS;
-  float xmin = 3.0e38f, xmax = -3.0e38f;
-#pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    const float xa = px[e], ya = py[e], xb = px[(e + 1) & 3], yb = py[(e + 1) & 3];
-    float t0 = 0.f, t1 = 1.f;
-    const float dy = yb - ya;
-    if (fabsf(dy) < 1e-6f) {
-      if (ya < ylo || ya > yhi) continue;
-    } else {
-      float ta = (ylo - ya) / dy, tb = (yhi - ya) / dy;
-      if (ta > tb) { const float t = ta; ta = tb; tb = t; }
-      t0 = fmaxf(ta, 0.f);
-      t1 = fminf(tb, 1.f);
-      if (t0 > t1) continue;
+template <bool HAS_MAPS, int MAPS_DTYPE>
+__device__ __forceinline__ float4 fp2_quad(const float* vol, const MapRef& mref, int n, int gy, int gx, bool vec4,
+                                           bool ok) {
+  if (!ok) return make_float4(0.f, 0.f, 0.f, 0.f);
+  if (vec4) {
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if ((unsigned)gy < (unsigned)n && (unsigned)gx < (unsigned)n) {
+      const int off = gy * n + gx;
+      v = __ldg(reinterpret_cast<const float4*>(vol + off));
+      if (HAS_MAPS) {
+        const float4 mv = map_at4<MAPS_DTYPE>(mref, off);
+        v.x *= mv.x; v.y *= mv.y; v.z *= mv.z; v.w *= mv.w;
+      }
     }
-    const float x0 = fmaf(t0, xb - xa, xa), x1 = fmaf(t1, xb - xa, xa);
-    xmin = fminf(xmin, fminf(x0, x1));
-    xmax = fmaxf(xmax, fmaxf(x0, x1));
+    return v;
   }
-  if (xmin > xmax) {
-    *lo = 1;
-    *hi = 0;
-    return;
-  }
-  *lo = (int)floorf(xmin - FPG_X_MARGIN);
-  *hi = (int)floorf(xmax + FPG_X_MARGIN) + 1;
+  return fp_load_item<HAS_MAPS, MAPS_DTYPE>(vol, mref, n, gy, gx, false);
 }
 
-template <int EPI, bool HAS_MAPS, int MAPS_DTYPE, int G>
-__global__ void __launch_bounds__(FP_THREADS, G == 4 ? 2 : 3) fp_group_kernel(FpArgs args) {
-  extern __shared__ __align__(16) float zg[];  // [FPG_BOX_H][stride] elements of G floats
+template <int EPI, bool HAS_MAPS, int MAPS_DTYPE>
+__global__ void __launch_bounds__(FP_THREADS, 4) fp_pair_kernel(FpArgs args) {
+  extern __shared__ __align__(16) float2 z2[];  // [FP2_BOX_H][stride] elements (slice 0, slice 1)
   __shared__ double red_d[FP_TC / FP_LC];
-  __shared__ int4 box_sh[FPG_MAX_CHUNKS];
-  __shared__ int2 cols_sh[FPG_BOX_H];          // staged columns [x, y] of every box row
+  __shared__ short4 box_sh[FP2_MAX_CHUNKS];  // (bx0, by0, quads, rows) of every chunk's box
+  __shared__ short2 quads_sh[FP2_BOX_H];
 
   const int n = args.n;
   const int band = blockIdx.x;
   const int ad = blockIdx.y;
-  const int s0 = blockIdx.z * G;
-  bool ok[G];
-  bool any = false;
+  const int s0 = 2 * blockIdx.z;
+  bool ok[2];
 #pragma unroll
-  for (int g = 0; g < G; ++g) {
+  for (int g = 0; g < 2; ++g) {
     const int s = s0 + g;
     ok[g] = s < args.n_slices && (args.active == nullptr || args.active[s] != 0);
-    any = any || ok[g];
   }
-  if (!any) return;  // the whole CTA
+  if (!ok[0] && !ok[1]) return;  // the whole CTA
   const int a = ad / args.n_det;
   const int d = ad - a * args.n_det;
 
   const float* M = args.fp_matrix + 6 * a;
   const float m00 = M[0], m01 = M[1], m02 = M[2], m10 = M[3], m11 = M[4], m12 = M[5];
-  constexpr int NB = fpg_bank_groups<G>();
-  const int res = args.bank_residues != nullptr ? args.bank_residues[2 * a + (G == 4 ? 1 : 0)] : FPG_BOX_W;
-  const int S = FPG_BOX_W + (((res - FPG_BOX_W) % NB) + NB) % NB;  // row stride in elements
+  const int sel = args.box_strides != nullptr ? min(max(args.box_strides[2 * a + 1], 0), 4) : 0;
+  const int S = FP2_BOX_W + 2 * sel;  // row stride (elements), even
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -633,12 +628,14 @@ __global__ void __launch_bounds__(FP_THREADS, G == 4 ? 2 : 3) fp_group_kernel(Fp
   const int c0 = band * FP_TC;
   const int c = c0 + warp * FP_LC + lc;
   const int c_last = min(c0 + FP_TC, n) - 1;
+  const bool vec4 = args.vec4 != 0;
+  const bool swap = (lane & 4) != 0;  // lanes 4-7 of each store phase write their second pair first
 
-  const float* vol[G];
-  MapRef mref[G];
+  const float* vol[2];
+  MapRef mref[2];
 #pragma unroll
-  for (int g = 0; g < G; ++g) {
-    const int s = ok[g] ? s0 + g : s0;
+  for (int g = 0; g < 2; ++g) {
+    const int s = ok[g] ? s0 + g : s0 + (ok[0] ? 0 : 1);
     vol[g] = args.vol + (int64_t)s * n * n;
     mref[g] = make_map_ref(args.maps, MAPS_DTYPE, args.maps_slice_stride, args.n_angles, args.n_det, n, s, a, d,
                            args.n_channels, args.chan_scale);
@@ -647,94 +644,111 @@ __global__ void __launch_bounds__(FP_THREADS, G == 4 ? 2 : 3) fp_group_kernel(Fp
   const float pxc = fmaf(m00, fc, m02);
   const float pyc = fmaf(m10, fc, m12);
 
-  if (tid * FPG_TR < n) {
-    int4 b;
-    chunk_box(m00, m01, m02, m10, m11, m12, c0, c_last, tid * FPG_TR, min((tid + 1) * FPG_TR, n) - 1, b.x, b.y, b.z,
-              b.w);
-    box_sh[tid] = b;
+  // box coordinates fit 16 bits: |x|, |y| < 1.5 n + 3 for n <= 8192
+  if (tid * FP2_TR < n) {
+    int bx0, bx1, by0, by1;
+    chunk_box(m00, m01, m02, m10, m11, m12, c0, c_last, tid * FP2_TR, min((tid + 1) * FP2_TR, n) - 1, bx0, bx1, by0,
+              by1);
+    box_sh[tid] = make_short4((short)bx0, (short)by0, (short)((bx1 - bx0) / 4 + 1), (short)(by1 - by0 + 1));
+  }
+  __syncthreads();
+  {
+    const short4 b0 = box_sh[0];
+    if (tid < b0.w && tid < FP2_BOX_H) {
+      float px[4], py[4];
+      chunk_corners(m00, m01, m02, m10, m11, m12, c0, c_last, 0, min(FP2_TR, n) - 1, px, py);
+      quads_sh[tid] = fp_row_quads(px, py, b0.y + tid, b0.x, b0.z);
+    }
   }
   __syncthreads();
 
-  float acc[G];
-#pragma unroll
-  for (int g = 0; g < G; ++g) acc[g] = 0.f;
-
-  for (int r0 = 0; r0 < n; r0 += FPG_TR) {
-    const int r_last = min(r0 + FPG_TR, n) - 1;
-    const int4 box = box_sh[r0 / FPG_TR];
-    const int bx0 = box.x, bx1 = box.y, by0 = box.z, by1 = box.w;
-    const int q4 = (bx1 - bx0) / 4 + 1;
-    const int bh = by1 - by0 + 1;
-    if (4 * q4 > FPG_BOX_W || bh > FPG_BOX_H) {  // cannot happen for valid matrices; never trap
+  float acc0 = 0.f, acc1 = 0.f;
+  for (int r0 = 0; r0 < n; r0 += FP2_TR) {
+    const int r_last = min(r0 + FP2_TR, n) - 1;
+    const short4 box = box_sh[r0 / FP2_TR];
+    const int bx0 = box.x, by0 = box.y, q4 = box.z, bh = box.w;
+    if (4 * q4 > FP2_BOX_W || bh > FP2_BOX_H) {  // cannot happen for valid matrices; never trap
       if (tid == 0) atomicExch(&g_box_overflow, 1);
       return;
     }
 
-    // columns of every box row that the chunk's taps read, clipped to the box
-    if (tid < bh) {
-      float px[4], py[4];
-      const float fc0 = (float)c0, fc1 = (float)c_last, fr0 = (float)r0, fr1 = (float)r_last;
-      px[0] = sample_x(m00, m01, m02, fc0, fr0); py[0] = sample_x(m10, m11, m12, fc0, fr0);
-      px[1] = sample_x(m00, m01, m02, fc1, fr0); py[1] = sample_x(m10, m11, m12, fc1, fr0);
-      px[2] = sample_x(m00, m01, m02, fc1, fr1); py[2] = sample_x(m10, m11, m12, fc1, fr1);
-      px[3] = sample_x(m00, m01, m02, fc0, fr1); py[3] = sample_x(m10, m11, m12, fc0, fr1);
-      int lo, hi;
-      fpg_row_columns(px, py, by0 + tid, &lo, &hi);
-      cols_sh[tid] = make_int2(max(lo, bx0), min(hi, bx0 + 4 * q4 - 1));
-    }
-    __syncthreads();
-
-    // stage z = x * map of the G slices: warp w fills box rows w, w + 8, ..., one pixel per lane
-    for (int rr = warp; rr < bh; rr += FP_THREADS / 32) {
-      const int2 cols = cols_sh[rr];
-      const int gy = by0 + rr;
-      const bool yin = (unsigned)gy < (unsigned)n;
-      float v[FPG_FILL_PX][G];
+    const int items = q4 * bh;
+    const unsigned magic = (1048576u + (unsigned)q4 - 1u) / (unsigned)q4;  // it / q4 as in fp_cta
+    for (int base = tid; base < items; base += FP_THREADS * FP2_FILL_BATCH) {
+      float4 v0[FP2_FILL_BATCH], v1[FP2_FILL_BATCH];
+      int dst[FP2_FILL_BATCH];
 #pragma unroll
-      for (int j = 0; j < FPG_FILL_PX; ++j) {
-        const int gx = cols.x + lane + 32 * j;
-        const bool in = yin && gx <= cols.y && (unsigned)gx < (unsigned)n;
-        const int off = gy * n + gx;
-#pragma unroll
-        for (int g = 0; g < G; ++g) {
-          float val = 0.f;
-          if (in && ok[g]) {
-            val = __ldg(vol[g] + off);
-            if (HAS_MAPS) val *= map_at<MAPS_DTYPE>(mref[g], off);
+      for (int k = 0; k < FP2_FILL_BATCH; ++k) {
+        const int it = base + k * FP_THREADS;
+        dst[k] = -1;
+        v0[k] = v1[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (it < items) {
+          const int rr = (int)(((unsigned)it * magic) >> 20);
+          const int qq = it - rr * q4;
+          const short2 qr = quads_sh[rr];
+          if (qq >= qr.x && qq <= qr.y) {
+            const int gy = by0 + rr, gx = bx0 + 4 * qq;
+            dst[k] = rr * S + 4 * qq;
+            v0[k] = fp2_quad<HAS_MAPS, MAPS_DTYPE>(vol[0], mref[0], n, gy, gx, vec4, ok[0]);
+            v1[k] = fp2_quad<HAS_MAPS, MAPS_DTYPE>(vol[1], mref[1], n, gy, gx, vec4, ok[1]);
           }
-          v[j][g] = val;
         }
       }
 #pragma unroll
-      for (int j = 0; j < FPG_FILL_PX; ++j) {
-        const int gx = cols.x + lane + 32 * j;
-        if (gx <= cols.y) FpgElem<G>::store(zg, rr * S + (gx - bx0), v[j]);
+      for (int k = 0; k < FP2_FILL_BATCH; ++k) {
+        if (dst[k] >= 0) {
+          // elements 4q, 4q + 1 (lo) and 4q + 2, 4q + 3 (hi); the order of the two stores is
+          // selected per lane so that both store instructions run with every lane active
+          const float4 lo = make_float4(v0[k].x, v1[k].x, v0[k].y, v1[k].y);
+          const float4 hi = make_float4(v0[k].z, v1[k].z, v0[k].w, v1[k].w);
+          float4* q = reinterpret_cast<float4*>(z2 + dst[k]);
+          const int f = swap ? 1 : 0;
+          q[f] = swap ? hi : lo;
+          q[1 - f] = swap ? lo : hi;
+        }
       }
     }
     __syncthreads();
+
+    if (r0 + FP2_TR < n) {
+      const short4 nb = box_sh[r0 / FP2_TR + 1];
+      if (tid < nb.w && tid < FP2_BOX_H) {
+        float px[4], py[4];
+        chunk_corners(m00, m01, m02, m10, m11, m12, c0, c_last, r0 + FP2_TR, min(r0 + 2 * FP2_TR, n) - 1, px, py);
+        quads_sh[tid] = fp_row_quads(px, py, nb.y + tid, nb.x, nb.z);
+      }
+    }
 
     if (c <= c_last) {
       const int zoff = -by0 * S - bx0;
       float fr = (float)(r0 + lr);
       const int rem = r_last - r0 - lr;
       const int kmax = rem >= 0 ? rem / FP_LR + 1 : 0;
-#pragma unroll 2
-      for (int k = 0; k < kmax; ++k) {
-        const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
-        const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
-        const int q = fy.i * S + fx.i + zoff;
-        float t0[G], t1[G], b0[G], b1[G];
-        FpgElem<G>::load(zg, q, t0);
-        FpgElem<G>::load(zg, q + 1, t1);
-        FpgElem<G>::load(zg, q + S, b0);
-        FpgElem<G>::load(zg, q + S + 1, b1);
-#pragma unroll
-        for (int g = 0; g < G; ++g) {
-          const float top = fmaf(fx.f, t1[g] - t0[g], t0[g]);
-          const float bot = fmaf(fx.f, b1[g] - b0[g], b0[g]);
-          acc[g] += fmaf(fy.f, bot - top, top);
+      if (kmax >= FP2_RPT) {
+#pragma unroll 4
+        for (int k = 0; k < FP2_RPT; ++k) {
+          const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
+          const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
+          const int q = fy.i * S + fx.i + zoff;
+          const float2 t0 = z2[q], t1 = z2[q + 1], b0 = z2[q + S], b1 = z2[q + S + 1];
+          const float top0 = fmaf(fx.f, t1.x - t0.x, t0.x), bot0 = fmaf(fx.f, b1.x - b0.x, b0.x);
+          const float top1 = fmaf(fx.f, t1.y - t0.y, t0.y), bot1 = fmaf(fx.f, b1.y - b0.y, b0.y);
+          acc0 += fmaf(fy.f, bot0 - top0, top0);
+          acc1 += fmaf(fy.f, bot1 - top1, top1);
+          fr += (float)FP_LR;
         }
-        fr += (float)FP_LR;
+      } else {
+        for (int k = 0; k < kmax; ++k) {
+          const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
+          const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
+          const int q = fy.i * S + fx.i + zoff;
+          const float2 t0 = z2[q], t1 = z2[q + 1], b0 = z2[q + S], b1 = z2[q + S + 1];
+          const float top0 = fmaf(fx.f, t1.x - t0.x, t0.x), bot0 = fmaf(fx.f, b1.x - b0.x, b0.x);
+          const float top1 = fmaf(fx.f, t1.y - t0.y, t0.y), bot1 = fmaf(fx.f, b1.y - b0.y, b0.y);
+          acc0 += fmaf(fy.f, bot0 - top0, top0);
+          acc1 += fmaf(fy.f, bot1 - top1, top1);
+          fr += (float)FP_LR;
+        }
       }
     }
     __syncthreads();
@@ -743,10 +757,10 @@ __global__ void __launch_bounds__(FP_THREADS, G == 4 ? 2 : 3) fp_group_kernel(Fp
   const int n_bands = gridDim.x;
   const int n_ad = gridDim.y;
 #pragma unroll
-  for (int g = 0; g < G; ++g) {
+  for (int g = 0; g < 2; ++g) {
     if (!ok[g]) continue;  // uniform across the CTA
     const int s = s0 + g;
-    float col = acc[g];
+    float col = g == 0 ? acc0 : acc1;
     col += __shfl_xor_sync(0xffffffffu, col, 8);
     col += __shfl_xor_sync(0xffffffffu, col, 16);
     double part = 0.0, ptest = 0.0;
@@ -1102,21 +1116,20 @@ static bool launch_fp_tma_inst(const FpArgs& a, const dim3& grid, cudaStream_t s
   return launched_ok();
 }
 
-template <int EPI, bool HAS_MAPS, int MAPS_DTYPE, int G>
-static bool launch_fp_group_inst(const FpArgs& a, cudaStream_t st) {
-  const dim3 grid((a.n + FP_TC - 1) / FP_TC, a.n_angles * a.n_det, (a.n_slices + G - 1) / G);
-  const size_t smem = fpg_smem_bytes<G>();
-  if (!ensure_dynamic_smem<fp_group_kernel<EPI, HAS_MAPS, MAPS_DTYPE, G>>((int)smem)) return false;
-  fp_group_kernel<EPI, HAS_MAPS, MAPS_DTYPE, G><<<grid, FP_THREADS, smem, st>>>(a);
+template <int EPI, bool HAS_MAPS, int MAPS_DTYPE>
+static bool launch_fp_pair_inst(const FpArgs& a, cudaStream_t st) {
+  const dim3 grid((a.n + FP_TC - 1) / FP_TC, a.n_angles * a.n_det, (a.n_slices + 1) / 2);
+  if (!ensure_dynamic_smem<fp_pair_kernel<EPI, HAS_MAPS, MAPS_DTYPE>>((int)FP2_SMEM_BYTES)) return false;
+  fp_pair_kernel<EPI, HAS_MAPS, MAPS_DTYPE><<<grid, FP_THREADS, FP2_SMEM_BYTES, st>>>(a);
   return launched_ok();
 }
 
-template <int EPI, int G>
-static bool launch_fp_group(const FpArgs& a, cudaStream_t st) {
-  if (a.maps == nullptr) return launch_fp_group_inst<EPI, false, CCT_DTYPE_F32, G>(a, st);
-  if (a.maps_dtype == CCT_DTYPE_BF16) return launch_fp_group_inst<EPI, true, CCT_DTYPE_BF16, G>(a, st);
-  if (a.maps_dtype == CCT_DTYPE_FIELDS_F32) return launch_fp_group_inst<EPI, true, CCT_DTYPE_FIELDS_F32, G>(a, st);
-  return launch_fp_group_inst<EPI, true, CCT_DTYPE_F32, G>(a, st);
+template <int EPI>
+static bool launch_fp_pair(const FpArgs& a, cudaStream_t st) {
+  if (a.maps == nullptr) return launch_fp_pair_inst<EPI, false, CCT_DTYPE_F32>(a, st);
+  if (a.maps_dtype == CCT_DTYPE_BF16) return launch_fp_pair_inst<EPI, true, CCT_DTYPE_BF16>(a, st);
+  if (a.maps_dtype == CCT_DTYPE_FIELDS_F32) return launch_fp_pair_inst<EPI, true, CCT_DTYPE_FIELDS_F32>(a, st);
+  return launch_fp_pair_inst<EPI, true, CCT_DTYPE_F32>(a, st);
 }
 
 // 16-byte staging loads need a 16-byte aligned volume, maps at 16 (FP32) or 8 (BF16) bytes and
@@ -1130,9 +1143,12 @@ bool fp_vec4_ok(const FpArgs& a) {
 template <int EPI>
 static void launch_fp_epi(const FpArgs& a, cudaStream_t st) {
   const dim3 grid((a.n + FP_TC - 1) / FP_TC, a.n_angles * a.n_det, a.n_slices);
-  // slice groups: any n, maps stride and storage type; the plain kernel if the launch is refused
-  if ((a.variant & CCT_VARIANT_FP_SLICES4) && launch_fp_group<EPI, 4>(a, st)) return;
-  if ((a.variant & CCT_VARIANT_FP_SLICES2) && launch_fp_group<EPI, 2>(a, st)) return;
+  // two slices per CTA: any n, maps stride and storage type; the plain kernel if refused
+  if ((a.variant & CCT_VARIANT_FP_SLICES2) && a.n_slices >= 2) {
+    FpArgs v = a;
+    v.vec4 = fp_vec4_ok(a) ? 1 : 0;
+    if (launch_fp_pair<EPI>(v, st)) return;
+  }
   // TMA path: rows and images must be 16-byte multiples for both FP32 and BF16 boxes
   const int64_t dense = (int64_t)a.n_angles * a.n_det * a.n * a.n;
   const bool aligned = (a.n % 8) == 0 && (reinterpret_cast<uintptr_t>(a.vol) % 16) == 0 &&

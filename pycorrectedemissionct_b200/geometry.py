@@ -46,20 +46,25 @@ def fp_matrices(angles_deg32: NDArray, n: int) -> NDArray:
     return out
 
 
-FP_BANK_GROUPS = (16, 8)  # shared-memory banks of 8-byte (2-slice) and 16-byte (4-slice) elements
+# Row strides the forward projection may use for its staged box, per kernel: (candidate
+# strides, shared-memory banks per phase of the element size, lanes per phase).
+FP_STRIDE_CHOICES = (
+    (np.array([100]), 32, 32),         # one slice per CTA: fixed (immediate tap offsets)
+    (80 + 2 * np.arange(5), 16, 16),   # two slices per CTA: 8-byte elements, even strides
+)
 
 
-def fp_bank_residues(fp_mat: NDArray, patches: int = 8) -> NDArray:
-    """``(A, 2)`` int32 row-stride residues of the slice-grouped forward projection's staged box:
-    column 0 modulo 16 (2 slices per element, 8-byte banks), column 1 modulo 8 (4 slices, 16-byte
-    banks).
+def fp_box_strides(fp_mat: NDArray, patches: int = 8) -> NDArray:
+    """``(A, 2)`` int32 row-stride selectors of the forward projection's staged box: column 0 for
+    the one-slice kernel (always 0: its stride is fixed at 100 floats), column 1 for the two-slice
+    kernel (``80 + 2 v`` elements of two floats, v in 0..4).
 
     A warp samples an 8 (columns) x 4 (rows) block of the rotated lattice (lane = 8 row-lane +
-    column-lane) and reads the four bilinear taps of every sample as one element each; the
-    shared-memory banks of an element are its index modulo the bank groups, taken per phase of
-    8 (16-byte) or 16 (8-byte) lanes.  For each angle this counts, over a few lattice blocks, the
-    wavefronts of every stride residue (distinct elements per bank, the largest per phase) and
-    keeps the cheapest.  The choice only affects speed; any residue gives the same results.
+    column-lane) and reads each bilinear tap of a sample as one element; the shared-memory bank
+    of an element is its index modulo the banks per phase (32 four-byte banks for 32 lanes, or
+    16 eight-byte banks for each 16-lane half).  For each angle this counts, over a few lattice
+    blocks, the wavefronts of every candidate stride (distinct elements per bank, the largest per
+    phase) and keeps the cheapest.  Speed only: any choice gives the same results.
     """
     m = np.asarray(fp_mat, dtype=np.float64).reshape(-1, 6)
     a = m.shape[0]
@@ -75,21 +80,16 @@ def fp_bank_residues(fp_mat: NDArray, patches: int = 8) -> NDArray:
     py = m[:, 3, None, None] * c + m[:, 4, None, None] * r + m[:, 5, None, None]
     fx = np.floor(px).astype(np.int64)                    # (A, P, 32)
     fy = np.floor(py).astype(np.int64)
-    taps = ((0, 0), (0, 1), (1, 0), (1, 1))
-    for col, nb in enumerate(FP_BANK_GROUPS):
-        lanes = nb  # a phase moves 128 bytes: nb elements of 128 / nb bytes
-        cand = np.arange(nb)
-        stride = 128 + cand                               # residue r <-> stride = r (mod nb)
-        cost = np.zeros((a, nb))
-        for dy, dx in taps:
-            e = (fy[:, None] + dy) * stride[None, :, None, None] + fx[:, None] + dx    # (A, C, P, 32)
-            e = e.reshape(a, nb, patches, 32 // lanes, lanes)
-            e = np.sort(e, axis=-1)
+    for col, (strides, nb, lanes) in enumerate(FP_STRIDE_CHOICES):
+        k = len(strides)
+        cost = np.zeros((a, k))
+        for dy, dx in ((0, 0), (0, 1), (1, 0), (1, 1)):
+            e = (fy[:, None] + dy) * strides[None, :, None, None] + fx[:, None] + dx    # (A, K, P, 32)
+            e = np.sort(e.reshape(a, k, patches, 32 // lanes, lanes), axis=-1)
             distinct = np.ones(e.shape, dtype=bool)
             distinct[..., 1:] = e[..., 1:] != e[..., :-1]
-            bank = np.mod(e, nb)
             groups = np.arange(e[..., 0].size).reshape(e.shape[:-1])
-            key = (groups[..., None] * nb + bank)[distinct]
+            key = (groups[..., None] * nb + np.mod(e, nb))[distinct]
             counts = np.bincount(key, minlength=groups.size * nb).reshape(*e.shape[:-1], nb)
             cost += counts.max(axis=-1).sum(axis=(-1, -2))
         out[:, col] = np.argmin(cost, axis=1)

@@ -387,21 +387,20 @@ def test_engine_tolerance_and_graph(cuda):
     assert torch.equal(stop.history[:, : int(expect.min())], eager.history[:, : int(expect.min())])
 
 
-ALL_FP_VARIANTS = ("tma", "slices2", "slices4")
+ALL_FP_VARIANTS = ("tma", "slices2")
 
 
 def _variant(name):
     from pycorrectedemissionct_b200 import _lib
 
-    return {"ldg": 0, "tma": _lib.CCT_VARIANT_FP_TMA, "slices2": _lib.CCT_VARIANT_FP_SLICES2,
-            "slices4": _lib.CCT_VARIANT_FP_SLICES4}[name]
+    return {"ldg": 0, "tma": _lib.CCT_VARIANT_FP_TMA, "slices2": _lib.CCT_VARIANT_FP_SLICES2}[name]
 
 
 @pytest.mark.parametrize("n,n_ang,dtype,s", [(64, 48, "float32", 5), (512, 90, "float32", 5), (512, 90, "bfloat16", 4),
                                              (130, 45, "float32", 3), (1000, 12, "float32", 2), (66, 30, "fields", 6)])
 def test_fp_variants_bit_identical(n, n_ang, dtype, s, cuda, tmp_path, monkeypatch):
-    """Every fp variant (one slice per CTA with load/store or TMA staging, two or four slices per
-    CTA) gives bit-identical projections, for batches that are not a multiple of the group, for
+    """Every fp variant (one slice per CTA with load/store or TMA staging, two slices per CTA)
+    gives bit-identical projections, for batches that are not a multiple of the pair, for
     every maps storage type and for an angle range of larger maps; the autotuner picks one of
     them and caches it."""
     from pycorrectedemissionct_b200 import autotune, core, phantoms

@@ -367,21 +367,24 @@ def _fma32(a, b, c):
 
 
 @pytest.mark.parametrize("n", [32, 130, 512, 1000])
-def test_fp_group_staged_columns_hold_every_tap(n):
-    """The slice-grouped forward projection (fp_group_kernel in csrc/cct_project.cu) stages, per
-    64 x 32 chunk, only the columns of each box row that fpg_row_columns finds (the chunk's
-    parallelogram clipped to the row's slab, widened by 0.5 and the right tap) and reads the taps
-    without tests: mirror that FP32 arithmetic and check that every tap of every sample lies in the
-    staged columns of its row, and that the box fits 80 x 76."""
+def test_fp_pair_staged_quads_hold_every_tap(n):
+    """The two-slice forward projection (fp_pair_kernel in csrc/cct_project.cu: 64 x 32 chunks in
+    boxes of at most 75 x 80) stages, per box row, only the quads that fp_row_quads finds (the
+    chunk's parallelogram clipped to the row's slab, widened by 0.5 and the right tap) and reads
+    the taps without tests: mirror that
+    FP32 arithmetic and check that every tap of every sample lies in a staged quad of its row.
+    The kernel divides with __fdividef (a few ulp): that moves the range by far less than the
+    0.5 margin this check leaves."""
     from pycorrectedemissionct_b200 import geometry
 
-    TC, TR, BOX_W, BOX_H, EPS, MARGIN = 64, 32, 80, 76, np.float32(0.01), np.float32(0.5)
+    TC, EPS, MARGIN, tr = 64, np.float32(0.01), np.float32(0.5), 32
+    BOX_W, BOX_H = 80, 75
     angles = np.concatenate([np.linspace(0, 2 * np.pi, 40, endpoint=False),
                              [np.pi / 4, 3 * np.pi / 4, 1e-6, np.pi / 2 + 1e-7, 0.3e-3]])
     mats = geometry.fp_matrices(np.rad2deg(np.array(angles, dtype=np.float32)), n)
     f32 = np.float32
 
-    def row_columns(px, py, y):
+    def row_quads(px, py, y, bx0, q4):
         ylo, yhi = f32(f32(y) - f32(1)) - EPS, f32(f32(y) + f32(1)) + EPS
         xmin, xmax = f32(3e38), f32(-3e38)
         for e in range(4):
@@ -402,14 +405,16 @@ def test_fp_group_staged_columns_hold_every_tap(n):
             xmin, xmax = min(xmin, x0, x1), max(xmax, x0, x1)
         if xmin > xmax:
             return 1, 0
-        return int(np.floor(f32(xmin - MARGIN))), int(np.floor(f32(xmax + MARGIN))) + 1
+        lo = int(np.floor(f32(xmin - MARGIN))) - bx0
+        hi = int(np.floor(f32(xmax + MARGIN))) + 1 - bx0
+        return max(lo, 0) >> 2, min(hi >> 2, q4 - 1)
 
     for m in mats:
         m00, m01, m02, m10, m11, m12 = (f32(v) for v in m)
         for c0 in range(0, n, TC):
             c_last = min(c0 + TC, n) - 1
-            for r0 in range(0, n, TR):
-                r_last = min(r0 + TR, n) - 1
+            for r0 in range(0, n, tr):
+                r_last = min(r0 + tr, n) - 1
                 cs = np.array([c0, c_last, c_last, c0], dtype=np.float32)   # cyclic corner order
                 rs = np.array([r0, r0, r_last, r_last], dtype=np.float32)
                 px = _fma32(m01, rs, _fma32(m00, cs, m02))
@@ -421,21 +426,55 @@ def test_fp_group_staged_columns_hold_every_tap(n):
                 q4 = (bx1 - bx0) // 4 + 1
                 bh = by1 - by0 + 1
                 assert 4 * q4 <= BOX_W and bh <= BOX_H
-                lo = np.empty(bh, dtype=np.int64)
-                hi = np.empty(bh, dtype=np.int64)
+                qlo = np.empty(bh, dtype=np.int64)
+                qhi = np.empty(bh, dtype=np.int64)
                 for t in range(bh):
-                    a_, b_ = row_columns(px, py, by0 + t)
-                    lo[t], hi[t] = max(a_, bx0), min(b_, bx0 + 4 * q4 - 1)
+                    qlo[t], qhi[t] = row_quads(px, py, by0 + t, bx0, q4)
                 cc, rr = np.meshgrid(np.arange(c0, c_last + 1, dtype=np.float32),
                                      np.arange(r0, r_last + 1, dtype=np.float32))
                 pxc = _fma32(m00, cc, m02)
                 pyc = _fma32(m10, cc, m12)
-                x = np.floor(_fma32(m01, rr, pxc)).astype(np.int64).ravel()
+                x = np.floor(_fma32(m01, rr, pxc)).astype(np.int64).ravel() - bx0
                 y = np.floor(_fma32(m11, rr, pyc)).astype(np.int64).ravel()
                 for dy in (0, 1):
                     row = y + dy - by0
                     assert row.min() >= 0 and row.max() < bh
-                    assert (x >= lo[row]).all() and (x + 1 <= hi[row]).all()
+                    assert ((x >> 2) >= qlo[row]).all() and (((x + 1) >> 2) <= qhi[row]).all()
+
+
+def test_fp_box_strides_cut_modelled_bank_conflicts():
+    """The per-angle stride selectors (geometry.fp_box_strides) stay in range and lower the
+    modelled shared-memory wavefronts of the taps against the fixed strides."""
+    from pycorrectedemissionct_b200 import geometry
+
+    n = 512
+    mats = geometry.fp_matrices(np.linspace(0, 360, 72, endpoint=False).astype(np.float32), n)
+    sel = geometry.fp_box_strides(mats)
+    assert sel.shape == (72, 2) and (sel[:, 0] == 0).all()
+    assert sel[:, 1].min() >= 0 and sel[:, 1].max() <= 4
+
+    def wavefronts(m, stride, banks, lanes, rng):
+        # distinct elements per bank, the largest per phase, over random 8 x 4 lattice blocks
+        lc, lr = np.arange(32) % 8, np.arange(32) // 8
+        total = 0
+        for _ in range(16):
+            c = rng.integers(0, n - 8) + lc
+            r = rng.integers(0, n - 4) + lr
+            fx = np.floor(m[0] * c + m[1] * r + m[2]).astype(np.int64)
+            fy = np.floor(m[3] * c + m[4] * r + m[5]).astype(np.int64)
+            for dy, dx in ((0, 0), (0, 1), (1, 0), (1, 1)):
+                e = (fy + dy) * stride + fx + dx
+                for p0 in range(0, 32, lanes):
+                    u = np.unique(e[p0:p0 + lanes])
+                    total += np.bincount(np.mod(u, banks), minlength=banks).max()
+        return total
+
+    for col, (strides, banks, lanes) in list(enumerate(geometry.FP_STRIDE_CHOICES))[1:]:
+        chosen = sum(wavefronts(m.astype(np.float64), strides[v], banks, lanes, np.random.default_rng(k))
+                     for k, (m, v) in enumerate(zip(mats, sel[:, col])))
+        fixed = sum(wavefronts(m.astype(np.float64), strides[0], banks, lanes, np.random.default_rng(k))
+                    for k, m in enumerate(mats))
+        assert chosen < fixed, (col, chosen, fixed)
 
 
 @pytest.mark.parametrize("n", [32, 130, 512])
