@@ -59,10 +59,16 @@ def parse():
                     help="headline path (auto: ordered subsets); the others are timed beside it")
     ap.add_argument("--subsets", default="90:2,18:1", help="ordered-subsets schedule subsets:passes,...")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra-legs", action="store_true",
+                    help="skip the drop-in e2e, BF16-maps and FP64-error legs")
+    ap.add_argument("--fp64-angle-step", type=int, default=24,
+                    help="FP64 oracle check of the headline slice on every k-th angle")
     ap.add_argument("--fp-variant", default="auto", choices=["auto", "ldg", "tma"],
                     help="fp staging variant: the autotuner's choice (auto) or a fixed one")
-    ap.add_argument("--workload", default="batch", choices=["batch", "ragged"],
-                    help="batch: the 512x720 benchmark (default); ragged: the mixed-size stream")
+    ap.add_argument("--workload", default="batch", choices=["batch", "ragged", "waves"],
+                    help="batch: the 512x720 benchmark (default); ragged: the mixed-size stream; waves: "
+                         "512 slices of plain MLEM in HBM-sized waves, FP32 and BF16 maps")
+    ap.add_argument("--wave-slices", type=int, default=512)
     ap.add_argument("--ragged-slices", type=int, default=400)
     ap.add_argument("--cpu-sample-angles", type=int, default=144)
     return ap.parse_args()
@@ -435,6 +441,10 @@ def run_ours(a):
     h2d = S * (2 * n * n + a.angles * n) * 4
     d2h = S * n * n * 4
 
+    extra = {}
+    if rank == 0 and not a.no_extra_legs:
+        extra = extra_legs(a, dev, c, maps, mus_h, xs_h, b, tol_np, max_iters, variant)
+
     # ---- roofline of the dominant kernel (attenuated fp with the fused MLEM epilogue, plain path)
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
@@ -489,12 +499,205 @@ def run_ours(a):
         line["phases_ms_per_step"] = dict(zip(("compute_maps", "subset_passes", "judge_mlem"), ph.mean(axis=0).tolist()))
     for name, r in results.items():
         line[name] = dict(r, solver=solver_desc[name])
+    line.update(extra)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         plain_its = results.get("plain", {}).get("mean_iterations", float(a.iters))
         line["cpu_baseline"] = cpu_baseline(a, plain_its)
+        cpu_v = line["cpu_baseline"]["value"]
+        # like for like: the same algorithm (plain MLEM to the plain residual) on both sides; the
+        # headline ratio also contains the ordered-subsets warm start's algorithmic gain
+        line["vs_cpu"] = {
+            "plain_gpu_over_cpu": results["plain"]["value"] / cpu_v if "plain" in results else None,
+            "dropin_e2e_over_cpu": (extra["dropin_e2e"]["value"] / cpu_v) if "dropin_e2e" in extra else None,
+            "headline_over_cpu": value / cpu_v,
+            "note": "plain_gpu_over_cpu and dropin_e2e_over_cpu compare plain MLEM with plain MLEM; "
+                    "headline_over_cpu also counts the ordered-subsets warm start (fewer passes)",
+        }
     if rank == 0:
         print(json.dumps(line), flush=True)
     distributed.finalize()
+
+
+def fp64_errors(a, c, maps, mu0, x0, dev) -> dict:
+    """Relative L2 errors of the GPU maps, attenuated fp and reference bp of one headline slice
+    against the FP64 oracle, on every k-th angle of the full set (the oracle needs minutes per
+    slice for all 720)."""
+    import torch
+
+    from oracle import port
+    from pycorrectedemissionct_b200 import core
+
+    step = max(1, a.fp64_angle_step)
+    idx = np.arange(0, c.n_angles, step)
+    rad32 = c.angles_rad32[idx]
+    _, deg32 = port.backend_angles(rad32)
+    workers = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    mu64 = mu0.astype(np.float64)
+    ref_maps = port.compute_maps(mu64, mu64, rad32, workers=workers)
+    x64 = x0.astype(np.float64)
+    ref_fp = port.fp_xrf(x64, ref_maps, deg32, workers=workers)
+    y = ref_fp / ref_fp.max()
+    ref_bp = port.bp_uncorrected(y, deg32, c.n, workers=workers)
+    sub = core.XrfCore(c.n, rad32, device=dev)
+    sub.variant = c.variant
+    m_sub = maps[0:1, torch.from_numpy(idx).to(dev)].contiguous()
+    xs = torch.from_numpy(x0).to(dev)[None]
+
+    def rel(u, v):
+        u = np.asarray(u, np.float64)
+        return float(np.linalg.norm(u - v) / np.linalg.norm(v))
+
+    out = {
+        "maps": rel(m_sub[0].float().cpu().numpy(), ref_maps),
+        "maps_then_fp": rel(sub.fp(xs, m_sub)[0, 0].cpu().numpy(), ref_fp),
+        "fp_on_fp64_maps": rel(sub.fp(xs, torch.from_numpy(ref_maps.astype(np.float32)).to(dev)[None])[0, 0].cpu().numpy(),
+                               ref_fp),
+        "bp_reference": rel(sub.bp(torch.from_numpy(y.astype(np.float32)).to(dev)[None, None], "reference")[0].cpu().numpy(),
+                            ref_bp),
+        "sample": f"slice 0 of the batch, {len(idx)} of {c.n_angles} angles (every {step}th), FP64 oracle port "
+                  f"({time.perf_counter() - t0:.1f} s on {workers} host threads)",
+        "bound": 1e-5,
+    }
+    return out
+
+
+def extra_legs(a, dev, c, maps, mus_h, xs_h, b, tol_np, max_iters, variant) -> dict:
+    """Legs reported beside the headline: the drop-in call (numpy in and out) end to end, FP64
+    errors of the headline slice, and plain MLEM with BF16-stored maps."""
+    import torch
+
+    from pycorrectedemissionct_b200 import core, engine, projectors, solvers
+
+    out = {}
+    n, S = a.n, a.slices
+    angles = np.linspace(0, 2 * np.pi, a.angles, endpoint=False)
+    mu_t = torch.from_numpy(mus_h).to(dev)
+    # the shared maps buffer holds the last timed path's angle order: natural order again
+    core.compute_maps(mu_t, mu_t, c.angles_rad32, out=maps)
+    # ---- the drop-in call a corrct user makes: maps from mu on the GPU, plain MLEM to the
+    # plain residual, numpy in and out, timed end to end on the host clock
+    mu0, b0, tol0 = mus_h[0], b[0, 0].cpu().numpy(), float(tol_np[0])
+
+    def dropin_once():
+        p = projectors.ProjectorAttenuationXRF((n, n), angles, att_in=mu0, att_out=mu0, verbose=False)
+        x, info = solvers.MLEM(tolerance=tol0)(p, b0, iterations=max_iters)
+        return info.iterations, x
+
+    dropin_once()
+    reps = max(1, min(3, a.steps))
+    t0 = time.perf_counter()
+    its = [dropin_once()[0] for _ in range(reps)]
+    dt = (time.perf_counter() - t0) / reps
+    out["dropin_e2e"] = {
+        "value": 1.0 / dt, "unit": UNIT, "mean_iterations": float(np.mean(its)), "seconds_per_slice": dt,
+        "h2d_bytes_per_step": 2 * n * n * 4 + a.angles * n * 4, "d2h_bytes_per_step": n * n * 4,
+        "call": "projectors.ProjectorAttenuationXRF((n, n), angles, att_in=mu, att_out=mu) + "
+                "solvers.MLEM(tolerance)(p, b, iterations) on one numpy slice (plain MLEM, host clock)",
+    }
+    # ---- FP64 oracle errors of the headline slice
+    try:
+        out["fp64_error"] = fp64_errors(a, c, maps, mus_h[0], xs_h[0], dev)
+    except Exception as exc:  # the oracle is a checker: report, never fail the bench on it
+        out["fp64_error"] = {"unavailable": repr(exc)}
+    # ---- BF16-stored maps: map error against FP32 maps, plain MLEM (200 iterations) speed
+    m16 = torch.empty((S, a.angles, 1, n, n), dtype=torch.bfloat16, device=dev)
+    ws = torch.empty(16 * 2 * (core.geometry.padded_size(n)[1] ** 2 + core.geometry.padded_size(n)[1]) * 4 * S,
+                     dtype=torch.uint8, device=dev)
+    core.compute_maps(mu_t, mu_t, c.angles_rad32, maps_dtype="bfloat16", workspace=ws, out=m16)
+    torch.cuda.synchronize(dev)
+    e16 = float(((m16[0].float() - maps[0].float()).double().norm() / maps[0].double().norm()).item())
+    c16 = core.XrfCore(n, angles, device=dev)
+    c16.variant = variant
+    sv = engine.BatchedSolver(c16, m16, b, "mlem")
+    sv.step()
+    fps, bps = [], []
+    for _ in range(10):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        sv.step_timed(*e)
+        torch.cuda.synchronize(dev)
+        fps.append(e[0].elapsed_time(e[1]))
+        bps.append(e[1].elapsed_time(e[2]))
+    sv.reset()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    core.compute_maps(mu_t, mu_t, c.angles_rad32, maps_dtype="bfloat16", workspace=ws, out=m16)
+    sv.run(a.iters, check_every=a.iters, use_graph=True)
+    ev[1].record()
+    torch.cuda.synchronize(dev)
+    secs = ev[0].elapsed_time(ev[1]) / 1e3
+    res_ratio = (sv.residuals.cpu().numpy() / tol_np).tolist()
+    out["bf16_maps"] = {
+        "plain_mlem_slices_per_s": S / secs, "iterations": a.iters,
+        "fp_launch_us": 1e3 * float(np.median(fps)), "bp_launch_us": 1e3 * float(np.median(bps)),
+        "maps_rel_l2_vs_fp32": e16,
+        "final_residual_over_fp32_target": [float(np.min(res_ratio)), float(np.max(res_ratio))],
+        "note": "maps stored in bfloat16 (8-bit mantissa), FP32 arithmetic; the FP32 maps' own error against "
+                "FP64 is fp64_error.maps",
+    }
+    del m16, ws, sv
+    return out
+
+
+def run_waves(a):
+    """Config 2 as stated: --wave-slices independent 512x512 slices over 720 angles, plain MLEM for
+    200 iterations with all slices of a wave in one launch per operator and each block of
+    iterations in a CUDA graph; waves sized to HBM; FP32 and BF16 maps.  Data synthesis is
+    untimed; each wave's timed work is compute_maps + 200 MLEM iterations."""
+    import torch
+
+    from pycorrectedemissionct_b200 import core, engine, phantoms
+
+    dev = torch.device("cuda", 0)
+    n, A = a.n, a.angles
+    angles = np.linspace(0, 2 * np.pi, A, endpoint=False)
+    c = core.XrfCore(n, angles, device=dev)
+    free = torch.cuda.mem_get_info(dev)[0]
+    out = {}
+    for dtype, mb in (("float32", 4), ("bfloat16", 2)):
+        per_slice = A * n * n * mb + 8 * A * n * 4 + 6 * n * n * 4
+        wave = max(1, min(a.wave_slices, int(0.8 * free // per_slice)))
+        tdt = torch.float32 if dtype == "float32" else torch.bfloat16
+        total_s, done = 0.0, 0
+        _, P = core.geometry.padded_size(n)
+        ws = torch.empty(16 * 2 * (P * P + P) * 4 * wave, dtype=torch.uint8, device=dev)
+        maps = torch.empty((wave, A, 1, n, n), dtype=tdt, device=dev)
+        for w0 in range(0, a.wave_slices, wave):
+            k = min(wave, a.wave_slices - w0)
+            xs, mus = [], []
+            for s in range(w0, w0 + k):
+                r = phantoms.slice_rng(a.seed, s)
+                xs.append(phantoms.ellipse_phantom(n, r, 12))
+                mus.append(phantoms.disk_attenuation(n, r, 0.01))
+            x = torch.from_numpy(np.stack(xs)).to(dev)
+            mu = torch.from_numpy(np.stack(mus)).to(dev)
+            mk = maps[:k]
+            core.compute_maps(mu, mu, c.angles_rad32, maps_dtype=dtype, workspace=ws, out=mk)
+            clean = c.fp(x, mk)
+            gen = torch.Generator(device=dev)
+            gen.manual_seed(a.seed + w0)
+            bb = torch.poisson(clean / clean.amax(dim=(1, 2, 3), keepdim=True) * a.peak, generator=gen)
+            del clean
+            sv = engine.BatchedSolver(c, mk, bb, "mlem")
+            torch.cuda.synchronize(dev)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record()
+            core.compute_maps(mu, mu, c.angles_rad32, maps_dtype=dtype, workspace=ws, out=mk)
+            sv.run(a.iters, check_every=10, use_graph=True)
+            ev[1].record()
+            torch.cuda.synchronize(dev)
+            total_s += ev[0].elapsed_time(ev[1]) / 1e3
+            done += k
+            del sv, bb, x, mu
+        out[dtype] = {"slices": done, "wave": wave, "seconds": total_s, "slices_per_s": done / total_s}
+        del maps, ws
+        torch.cuda.empty_cache()
+    line = {"metric": f"plain MLEM slices/s, {a.wave_slices} slices of {n}x{n}x{A} in HBM-sized waves",
+            "value": out["float32"]["slices_per_s"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "config": {"workload": "config 2: independent slices, 200 MLEM iterations, FP32 vs BF16 maps",
+                       "iterations": a.iters}, "float32": out["float32"], "bfloat16": out["bfloat16"],
+            "data": "synthetic", "dtype": "f32"}
+    print(json.dumps(line), flush=True)
 
 
 def run_ragged(a):
@@ -573,6 +776,8 @@ def main():
         run_reference(a)
     elif a.workload == "ragged":
         run_ragged(a)
+    elif a.workload == "waves":
+        run_waves(a)
     else:
         run_ours(a)
 

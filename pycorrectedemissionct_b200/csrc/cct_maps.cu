@@ -109,7 +109,10 @@ __device__ __forceinline__ float bilin_square(const float* img, int P, float x, 
 }
 
 // Bilinear samples at (x, y) of a (P x P) image W and of the partner field K[c] - W[r][c]
-// (zero outside the frame for both).  *La is bilin_square(W) exactly.
+// (zero outside the frame for both).  *La is bilin_square(W) exactly.  Inside the frame the
+// partner's sample is the x-interpolated column constant minus *La (bilinear interpolation is
+// linear and K does not vary along rows); at the frame edge, where the partner field is zero
+// outside, its four taps are interpolated.
 __device__ __forceinline__ void bilin_square_pair(const float* img, const float* K, int P, float x, float y,
                                                   float* La, float* Lb) {
   const FloorSplit fx = floor_split(x), fy = floor_split(y);
@@ -119,7 +122,11 @@ __device__ __forceinline__ void bilin_square_pair(const float* img, const float*
     const float* q = img + (int64_t)y0 * P + x0;
     v00 = __ldg(q); v01 = __ldg(q + 1); v10 = __ldg(q + P); v11 = __ldg(q + P + 1);
     const float k0 = __ldg(K + x0), k1 = __ldg(K + x0 + 1);
-    u00 = k0 - v00; u01 = k1 - v01; u10 = k0 - v10; u11 = k1 - v11;
+    const float top = fmaf(fx.f, v01 - v00, v00);
+    const float bot = fmaf(fx.f, v11 - v10, v10);
+    *La = fmaf(fy.f, bot - top, top);
+    *Lb = fmaf(fx.f, k1 - k0, k0) - *La;
+    return;
   } else {
     const bool xin0 = x0 >= 0 && x0 < P, xin1 = x0 + 1 >= 0 && x0 + 1 < P;
     const bool yin0 = y0 >= 0 && y0 < P, yin1 = y0 + 1 >= 0 && y0 + 1 < P;
@@ -391,8 +398,8 @@ __global__ void __launch_bounds__(256, PAIRS ? 5 : 1) maps_resample_kernel(MapsP
     sample4(0, L, Lb);
 #pragma unroll
     for (int k = 0; k < RS_PIX; ++k) {
-      f_in[k] = expf(-L[k]);
-      f_inb[k] = paired ? expf(-Lb[k]) : 1.f;
+      f_in[k] = __expf(-L[k]);
+      f_inb[k] = paired ? __expf(-Lb[k]) : 1.f;
     }
     job = 1;
   } else {
@@ -412,8 +419,8 @@ __global__ void __launch_bounds__(256, PAIRS ? 5 : 1) maps_resample_kernel(MapsP
         sample4(job + d * p.n_sub + q, L, Lb);
 #pragma unroll
         for (int k = 0; k < RS_PIX; ++k) {
-          sum[k] += expf(-L[k]);
-          if (paired) sumb[k] += expf(-Lb[k]);
+          sum[k] += __expf(-L[k]);
+          if (paired) sumb[k] += __expf(-Lb[k]);
         }
       }
       if (p.n_sub == 1) {
