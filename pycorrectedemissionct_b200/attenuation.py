@@ -167,7 +167,7 @@ class AttenuationVolume:
         if roi is not None:
             raise NotImplementedError("Extracting a region of interest is not supported, yet.")
         if binning > 1:
-            raise NotImplementedError("Binning of the maps is not supported by the B200 backend.")
+            maps = bin_maps(maps, binning, len(self.vol_shape_zyx))
         return maps
 
     def get_projector_args(self, roi=None, rot_ind=None, det_ind=None, binning: int = 1) -> dict:
@@ -177,6 +177,28 @@ class AttenuationVolume:
         else:
             det_angles = self.detectors[det_ind].angle_rad
         return dict(att_maps=self.get_maps(roi=roi, rot_ind=rot_ind, det_ind=det_ind, binning=binning), angles_detectors_rad=det_angles)
+
+
+def bin_maps(maps: np.ndarray, binning, n_axes: int) -> np.ndarray:
+    """Integer binning of the last ``n_axes`` axes (the volume's) of ``maps`` by block means, after
+    cropping each of those axes to a multiple of ``binning`` (the excess split between both ends,
+    the larger half at the start): the integer branch of corrct's ``bin_imgs(..., auto_crop=True)``
+    (``processing/pre.py:180-231``) as ``get_maps`` calls it (``physics/attenuation.py:292-293``)."""
+    if int(binning) != binning:
+        raise NotImplementedError("Only integer binning of the maps is supported by the B200 backend.")
+    binning = int(binning)
+    axes = list(range(maps.ndim - n_axes, maps.ndim))
+    slicing = [slice(None)] * maps.ndim
+    for ax in axes:
+        excess = maps.shape[ax] % binning
+        if excess:
+            slicing[ax] = slice(excess - excess // 2, maps.shape[ax] - excess // 2)
+    maps = maps[tuple(slicing)]
+    shape = []
+    for ax, size in enumerate(maps.shape):
+        shape += [size // binning, binning] if ax in axes else [size]
+    mean_axes = tuple(i + 1 + k for k, i in enumerate(axes))
+    return maps.reshape(shape).mean(axis=mean_axes, dtype=np.float64).astype(maps.dtype)
 
 
 def _shape(vol) -> tuple:

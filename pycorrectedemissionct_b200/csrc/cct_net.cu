@@ -7,11 +7,12 @@
 // [Cout][3][3][Cin] bfloat16 ("K-major": k = tap * Cin + ci).
 //
 // GEMM tile: M = 128 rows (one TMEM lane each), N = BN columns (16..128, FP32 TMEM columns),
-// K blocks of 64 elements staged in shared memory in the canonical K-major, no-swizzle UMMA
-// layout: the 16-byte chunk kc (8 consecutive k) of row r sits at byte kc * ROWS * 16 + r * 16,
-// so one K=16 MMA step reads chunks {2s, 2s+1}: descriptor start = base + 2s * ROWS * 16,
-// leading-byte offset (between the two K chunks) = ROWS * 16, stride-byte offset (between
-// 8-row core matrices) = 128.  Two operand buffers alternate: all 128 threads gather block
+// K blocks of 64 elements staged in shared memory.  Forward (and data-gradient) convolutions use
+// the 128-byte swizzled K-major UMMA layout: 8 lanes gather one tile row's 128 contiguous bytes
+// (four rows per warp load) and write them as 8 chunks XOR-permuted by the row, conflict-free;
+// the weight-gradient GEMM uses the canonical no-swizzle layout (the 16-byte chunk kc of row r
+// at byte kc * ROWS * 16 + r * 16; descriptor start = base + 2s * ROWS * 16, leading-byte offset
+// ROWS * 16, stride-byte offset 128).  Two operand buffers alternate: all 128 threads gather block
 // kb + 1 while the tensor core works on block kb; one elected thread issues the four MMAs of a
 // block and commits them to that buffer's mbarrier.  Every wait is bounded; on timeout the
 // kernel raises g_net_timeout and leaves after waiting once more for its own MMAs.
@@ -58,6 +59,24 @@ __device__ __forceinline__ uint64_t umma_smem_desc(uint32_t addr, uint32_t lbo_b
   // base offset 0, legacy LBO mode, layout type 0 = SWIZZLE_NONE
   return d;
 }
+
+// K-major operand in the 128-byte swizzle layout: row r's 64 K elements (128 bytes) at r * 128 with
+// its 16-byte chunk c stored at chunk c ^ (r % 8), 8-row atoms 1024 bytes apart (stride-byte
+// offset), atom bases 1024-byte aligned; the leading-byte offset (between the two 16-byte chunks
+// of one K = 16 step) is one chunk.  A K = 16 step inside the row advances the start address by
+// 32 bytes; the tensor core applies the swizzle to the address bits.
+__device__ __forceinline__ uint64_t umma_sw128_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;            // leading-byte offset: 16 bytes
+  d |= (uint64_t)(1024 >> 4) << 32;  // stride-byte offset: 1024 bytes
+  d |= (uint64_t)1 << 46;            // descriptor version for sm_100
+  d |= (uint64_t)2 << 61;            // layout type SWIZZLE_128B
+  return d;
+}
+
+// Byte offset of 16-byte chunk kc of row r in a 128-byte swizzled K-major operand.
+__device__ __forceinline__ uint32_t sw128_offset(int r, int kc) { return (uint32_t)(r * 128 + ((kc ^ (r & 7)) << 4)); }
 
 __host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n) {
   return (1u << 4)                    // D format FP32
@@ -152,6 +171,7 @@ __global__ void __launch_bounds__(NET_THREADS) conv_umma_kernel(ConvArgs a) {
   extern __shared__ __align__(1024) unsigned char net_smem[];
   __shared__ __align__(8) uint64_t mma_bar[2];
   __shared__ uint32_t tmem_base_sh;
+  __shared__ int4 rows_sh[NET_BM];  // FWD: (y, x, output pixel or -1) of every tile row
 
   unsigned char* abuf[2] = {net_smem, net_smem + A_BYTES};
   unsigned char* bbuf[2] = {net_smem + 2 * A_BYTES, net_smem + 2 * A_BYTES + B_BYTES};
@@ -172,6 +192,7 @@ __global__ void __launch_bounds__(NET_THREADS) conv_umma_kernel(ConvArgs a) {
     px_ = rem - py * a.w;
     prow = a.x + m_row * a.cin;
   }
+  if (MODE == NET_FWD) rows_sh[tid] = make_int4(py, px_, row_valid ? (int)m_row : -1, 0);
   int64_t k_begin = 0, k_end = a.k_total;
   if (MODE == NET_WGRAD) {
     k_begin = (int64_t)blockIdx.z * a.k_split;
@@ -207,34 +228,49 @@ __global__ void __launch_bounds__(NET_THREADS) conv_umma_kernel(ConvArgs a) {
       if (!net_mbar_wait(&mma_bar[buf], (uint32_t)(((kb - 2) >> 1) & 1))) timed_out = true;
     }
     const int64_t k0 = k_begin + (int64_t)kb * NET_BK;
-    // ---- gather A: 128 rows x 8 chunks (thread = row)
-    {
+    if (MODE == NET_FWD) {
+      // ---- gather A: 8 lanes per tile row, one 16-byte chunk each, so that a warp's load covers
+      // four rows' contiguous K segments; 128-byte swizzled K-major layout
+      uint4 v[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int idx = i * NET_THREADS + tid;
+        const int r = idx >> 3, kc = idx & 7;
+        const int4 ri = rows_sh[r];
+        v[i] = load_im2col_row(a, a.x + (int64_t)max(ri.z, 0) * a.cin, ri.x, ri.y, ri.z >= 0, k0 + 8 * kc);
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int idx = i * NET_THREADS + tid;
+        *reinterpret_cast<uint4*>(abuf[buf] + sw128_offset(idx >> 3, idx & 7)) = v[i];
+      }
+      // ---- gather B: BN weight rows x 8 chunks, same layout
+      for (int it = tid; it < BN * 8; it += NET_THREADS) {
+        const int r = it >> 3, kc = it & 7;
+        const int64_t n = n0 + r;
+        const int64_t k = k0 + 8 * kc;
+        uint4 w = zero4();
+        if (n < a.n_total && k < a.k_total) w = __ldg(reinterpret_cast<const uint4*>(a.wt + n * a.k_total + k));
+        *reinterpret_cast<uint4*>(bbuf[buf] + sw128_offset(r, kc)) = w;
+      }
+    } else {
+      // ---- gather A: 128 rows x 8 chunks (thread = row), canonical no-swizzle layout
       const int64_t m = m0 + tid;
 #pragma unroll
       for (int kc = 0; kc < 8; ++kc) {
         const int64_t k = k0 + 8 * kc;
-        uint4 v;
-        if (MODE == NET_FWD) {
-          v = load_im2col_row(a, prow, py, px_, row_valid, k);
-        } else {
-          v = (k < k_end) ? load_wgrad_a(a, m, k) : zero4();
-        }
+        const uint4 v = (k < k_end) ? load_wgrad_a(a, m, k) : zero4();
         *reinterpret_cast<uint4*>(abuf[buf] + kc * (NET_BM * 16) + tid * 16) = v;
       }
-    }
-    // ---- gather B: BN rows x 8 chunks
-    for (int it = tid; it < BN * 8; it += NET_THREADS) {
-      const int r = it % BN;
-      const int kc = it / BN;
-      const int64_t n = n0 + r;
-      const int64_t k = k0 + 8 * kc;
-      uint4 v = zero4();
-      if (MODE == NET_FWD) {
-        if (n < a.n_total && k < a.k_total) v = __ldg(reinterpret_cast<const uint4*>(a.wt + n * a.k_total + k));
-      } else {
-        if (k < k_end) v = load_wgrad_b(a, n, k);
+      // ---- gather B: BN rows x 8 chunks
+      for (int it = tid; it < BN * 8; it += NET_THREADS) {
+        const int r = it % BN;
+        const int kc = it / BN;
+        const int64_t n = n0 + r;
+        const int64_t k = k0 + 8 * kc;
+        const uint4 v = (k < k_end) ? load_wgrad_b(a, n, k) : zero4();
+        *reinterpret_cast<uint4*>(bbuf[buf] + kc * (BN * 16) + r * 16) = v;
       }
-      *reinterpret_cast<uint4*>(bbuf[buf] + kc * (BN * 16) + r * 16) = v;
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (__syncthreads_or(timed_out ? 1 : 0)) {
@@ -248,8 +284,10 @@ __global__ void __launch_bounds__(NET_THREADS) conv_umma_kernel(ConvArgs a) {
       const uint32_t b_base = net_smem_u32(bbuf[buf]);
 #pragma unroll
       for (int s = 0; s < NET_BK / 16; ++s) {
-        const uint64_t ad = umma_smem_desc(a_base + 2 * s * NET_BM * 16, NET_BM * 16, 128);
-        const uint64_t bd = umma_smem_desc(b_base + 2 * s * BN * 16, BN * 16, 128);
+        const uint64_t ad = MODE == NET_FWD ? umma_sw128_desc(a_base + 32 * s)
+                                            : umma_smem_desc(a_base + 2 * s * NET_BM * 16, NET_BM * 16, 128);
+        const uint64_t bd = MODE == NET_FWD ? umma_sw128_desc(b_base + 32 * s)
+                                            : umma_smem_desc(b_base + 2 * s * BN * 16, BN * 16, 128);
         const uint32_t acc = (kb > 0 || s > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"

@@ -79,6 +79,15 @@ def test_reference_solvers_on_b200_projector(golden_cases, corrct, cuda):
     e = rel_l2(xa, m["sart_x"])
     report("corrct SART on the B200 projector", e, TOL_RECON)
     assert e < TOL_RECON
+    # or register the class with corrct's projector ABC: corrct's SART then takes its own
+    # projector branch (fp_angle / bp_angle(single_line=True)) with the B200 projector
+    corrct.projectors.ProjectorAttenuationXRF.register(projectors.ProjectorAttenuationXRF)
+    assert isinstance(p, corrct.projectors.ProjectorUncorrected)
+    np.random.seed(5)
+    xr, _ = sv.SART(verbose=False)(p, b, 3, b_mask=m["b_mask"])
+    e = rel_l2(xr, m["sart_x"])
+    report("corrct SART on the registered B200 projector", e, TOL_RECON)
+    assert e < TOL_RECON
 
 
 def test_reference_projector_with_b200_backend(golden_cases, corrct, cuda):

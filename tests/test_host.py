@@ -540,3 +540,25 @@ def test_ctypes_structs_match_the_c_header(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(cls), cname
         for fname, _ in cls._fields_:
             assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
+
+
+def test_get_maps_binning_matches_block_means():
+    """get_maps(binning=k): crop each volume axis to a multiple of k (excess split between both
+    ends, the larger half at the start) and average k x k blocks, the integer branch of corrct's
+    bin_imgs(auto_crop=True) (processing/pre.py:180-231)."""
+    from pycorrectedemissionct_b200 import attenuation
+
+    rng = np.random.default_rng(4)
+    maps = rng.uniform(size=(5, 2, 11, 11)).astype(np.float32)   # (A, D, y, x), 11 = 3 * 3 + 2
+    got = attenuation.bin_maps(maps, 3, 2)
+    assert got.shape == (5, 2, 3, 3) and got.dtype == np.float32
+    crop = maps[:, :, 1:10, 1:10].astype(np.float64)              # excess 2: one pixel off each end
+    want = crop.reshape(5, 2, 3, 3, 3, 3).mean(axis=(3, 5))
+    np.testing.assert_allclose(got, want, rtol=1e-6)
+    vol = rng.uniform(size=(3, 2, 5, 8, 8)).astype(np.float32)   # (A, D, z, y, x): all three axes
+    got3 = attenuation.bin_maps(vol, 2, 3)
+    want3 = vol[:, :, 1:5].astype(np.float64).reshape(3, 2, 2, 2, 4, 2, 4, 2).mean(axis=(3, 5, 7))
+    np.testing.assert_allclose(got3, want3, rtol=1e-6)
+    with pytest.raises(NotImplementedError):
+        attenuation.bin_maps(maps, 1.5, 2)
+
