@@ -317,6 +317,17 @@ __global__ void __launch_bounds__(FP_THREADS, 5) fp_kernel(FpArgs args) {
   fp_cta<EPI, HAS_MAPS, MAPS_DTYPE>(args, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y);
 }
 
+// Line-integral fields: the channels of a field slice read the same two planes per angle, so
+// they run as neighbouring CTAs (grid x = band * C + channel, z = field slice) and all but the
+// first find the planes in L2.  Same per-CTA work as fp_kernel.
+template <int EPI>
+__global__ void __launch_bounds__(FP_THREADS, 5) fp_fields_kernel(FpArgs args) {
+  const int C = args.n_channels;
+  const int band = blockIdx.x / C;
+  const int ch = blockIdx.x - band * C;
+  fp_cta<EPI, true, CCT_DTYPE_FIELDS_F32>(args, band, blockIdx.y, blockIdx.z * C + ch, gridDim.x / C, gridDim.y);
+}
+
 // Group g of a ragged launch owns CTAs [start[g], start[g + 1]); binary search over the groups.
 __device__ __forceinline__ int ragged_group(const int64_t* __restrict__ start, int n_groups, int64_t cta) {
   int lo = 0, hi = n_groups - 1;
@@ -1172,7 +1183,8 @@ static void launch_fp_epi(const FpArgs& a, cudaStream_t st) {
   } else if (a.maps_dtype == CCT_DTYPE_BF16) {
     fp_kernel<EPI, true, CCT_DTYPE_BF16><<<grid, FP_THREADS, 0, st>>>(v);
   } else if (a.maps_dtype == CCT_DTYPE_FIELDS_F32) {
-    fp_kernel<EPI, true, CCT_DTYPE_FIELDS_F32><<<grid, FP_THREADS, 0, st>>>(v);
+    const dim3 fgrid(grid.x * a.n_channels, grid.y, a.n_slices / a.n_channels);
+    fp_fields_kernel<EPI><<<fgrid, FP_THREADS, 0, st>>>(v);
   } else {
     fp_kernel<EPI, true, CCT_DTYPE_F32><<<grid, FP_THREADS, 0, st>>>(v);
   }
