@@ -4,22 +4,27 @@ plain (cold start) vs warm start.
 One step = the hot path over one batch of synthetic slices already resident in HBM:
 ``compute_maps`` (incident + emitted attenuation maps) followed by MLEM with the reference's
 KL-residual stopping rule, run until every slice reaches the residual that the plain solver
-reaches after 200 iterations (calibrated once, untimed).  Three paths are timed:
+reaches after 200 iterations (calibrated once, untimed).  Paths:
 
 * plain: MLEM from the default start;
-* learned: 10 MLEM iterations, the encoder-decoder on them (tensor-core kernels), MLEM to the
-  residual (when trained weights are present);
-* subsets: ordered-subsets EM passes (90 subsets x 2 passes, then 18 x 1; each pass costs one
-  MLEM iteration), then MLEM to the residual, which judges every slice.
+* subsets (the headline): ordered-subsets EM passes (90 subsets x 2 passes, then 18 x 1; each pass
+  costs one MLEM iteration), then MLEM to the residual, which judges every slice;
+* learned: on the learned part's own data (config 4's textured slices at 1e4 counts), the learned
+  start (one ordered-subsets pass keeping 10 snapshots, the tensor-core encoder-decoder, one pass
+  per ordered-subsets level) then MLEM to the residual, timed beside plain MLEM and the
+  ordered-subsets passes on the same slices.
 
 ``value`` = slices converged per second over the timed steps of the headline path (``--method``,
 default the ordered-subsets warm start); the other paths are reported beside it.  Max over ranks;
 weak scaling (each rank owns its own slices, no collective on the data path).
 
 ``e2e`` repeats the headline step through the public API from pinned host buffers (mu and the
-data copied in, the reconstruction copied out inside the timed region).  ``--impl reference``
-times the reference algorithm's CPU implementation (the oracle port in ``oracle/``) on the
-host cores on a bounded sample of the same workload.
+data copied in, the reconstruction copied out inside the timed region); ``dropin_e2e`` times the
+call a corrct user makes (projector from mu + MLEM with a tolerance, numpy in and out).
+``--impl reference`` times the reference algorithm's CPU implementation (the oracle port in
+``oracle/``) on the host cores on a bounded sample of the same workload.  Other workloads:
+``--workload ragged`` (mixed sizes), ``waves`` (config 2: 512 slices of plain MLEM, FP32 and BF16
+maps), ``channels`` (config 3: 8 fluorescence channels, PDHG-TV).
 """
 
 from __future__ import annotations
@@ -55,8 +60,9 @@ def parse():
     ap.add_argument("--maps-dtype", default="float32", choices=["float32", "bfloat16"])
     ap.add_argument("--peak", type=float, default=1e5)
     ap.add_argument("--seed", type=int, default=20240)
-    ap.add_argument("--method", default="auto", choices=["auto", "plain", "learned", "subsets"],
+    ap.add_argument("--method", default="auto", choices=["auto", "plain", "subsets"],
                     help="headline path (auto: ordered subsets); the others are timed beside it")
+    ap.add_argument("--learned-peak", type=float, default=1e4, help="learned leg: Poisson peak counts (config 4)")
     ap.add_argument("--subsets", default="90:2,18:1", help="ordered-subsets schedule subsets:passes,...")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra-legs", action="store_true",
@@ -223,9 +229,6 @@ def run_ours(a):
     import torch
 
     from pycorrectedemissionct_b200 import autotune, core, distributed, engine
-    from pycorrectedemissionct_b200 import train_warmstart as tw
-    from pycorrectedemissionct_b200.warmstart import N_ITERATES, WarmStartNet
-
     rank, world, local = distributed.env_ranks()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -278,25 +281,6 @@ def run_ours(a):
     max_iters = 2 * a.iters
 
     plain = engine.BatchedSolver(c, maps, b, "mlem", tolerance=tol_np)
-    net = None
-    if os.path.exists(WEIGHTS):
-        net = WarmStartNet(device=dev)
-        net.load(WEIGHTS)
-    elif a.method == "learned":
-        raise FileNotFoundError(f"no trained warm-start weights at {WEIGHTS}")
-    learned = first = None
-    k_l = net.pass_subsets(a.angles) if net is not None else 0
-    c_l, b_l, os_l = c, b, None
-    if k_l > 0:
-        # the network's inputs are snapshots of one ordered-subsets pass: its own angle order
-        perm_l_t = torch.from_numpy(engine.subset_permutation(a.angles, [k_l])).to(dev)
-        c_l = core.XrfCore(n, angles[perm_l_t.cpu().numpy()], device=dev)
-        c_l.variant = variant
-        b_l = b[:, :, perm_l_t].contiguous()
-        os_l = engine.OrderedSubsets(c_l, maps, b_l, [(k_l, 1)])
-    if net is not None:
-        learned = engine.BatchedSolver(c_l, maps, b_l, "mlem", tolerance=tol_np)
-        first = engine.BatchedSolver(c_l, maps, b_l, "mlem")
     subsets = engine.OrderedSubsets(c_os, maps, b_os, schedule)
     judge = engine.BatchedSolver(c_os, maps, b_os, "mlem", tolerance=tol_np, x_shared=subsets.x)
     launches_os_pass = sum(k * 3 * p for k, p in schedule)
@@ -329,29 +313,6 @@ def run_ours(a):
         solve_to_tol(plain, timed, max_iters)
         return float(plain.iterations.float().mean().item())
 
-    def step_learned(timed: bool) -> float:
-        if os_l is not None:
-            core.compute_maps(mu_in, mu_out, c_l.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
-            launches[0] += 2 * passes
-            os_l.reset()
-            its = tw.pass_snapshots(os_l)
-            launches[0] += 3 * k_l  # one pass: fp, residual and bp per subset
-            first_passes = 1
-        else:
-            maps_natural()
-            launches[0] += 2 * passes
-            first.reset()
-            its = tw.first_iterates(first)
-            launches[0] += 3 * N_ITERATES
-            first_passes = N_ITERATES
-        bpn = tw.normalized_backprojection(c_l, b_l, first.tau)
-        scale = tw.slice_means(its[-1])
-        x0 = net.predict(its + [bpn], base=its[-1], slice_scale=scale)
-        launches[0] += 2 + 90  # bp + ratio, network (~90 kernels)
-        learned.reset(x0)
-        solve_to_tol(learned, False, max_iters)
-        return float((learned.iterations.float() + first_passes).mean().item())
-
     phase_ms = []  # (maps, passes, judge) of timed ordered-subsets steps
 
     def step_subsets(timed: bool) -> float:
@@ -381,9 +342,7 @@ def run_ours(a):
         return t0.elapsed_time(t1) / 1e3, float(np.mean(its))
 
     paths = {"plain": step_plain, "subsets": step_subsets}
-    if net is not None:
-        paths["learned"] = step_learned
-    headline = {"auto": "subsets", "plain": "plain", "learned": "learned", "subsets": "subsets"}[a.method]
+    headline = {"auto": "subsets", "plain": "plain", "subsets": "subsets"}[a.method]
     if headline not in paths:
         raise RuntimeError(f"path {headline!r} is unavailable")
     for _ in range(a.warmup):
@@ -411,7 +370,7 @@ def run_ours(a):
     head_s = distributed.max_over_ranks(head_s, dev)
     clk = clocks.stop()
     head_launches = launches[0]
-    result = {"plain": plain, "learned": learned, "subsets": judge}[headline]
+    result = {"plain": plain, "subsets": judge}[headline]
     converged = int((result.residuals.cpu().numpy() <= tol_np).sum())
     total_slices = S * a.steps * world
     value = total_slices / head_s
@@ -430,9 +389,6 @@ def run_ours(a):
         if headline == "subsets":
             torch.index_select(b, 2, perm_t, out=b_os)
             subsets.set_data(b_os)
-        if headline == "learned" and os_l is not None:
-            torch.index_select(b, 2, perm_l_t, out=b_l)
-            os_l.set_data(b_l)
         its = paths[headline](False)
         x_h.copy_(result.x, non_blocking=True)
         return its
@@ -446,6 +402,9 @@ def run_ours(a):
     extra = {}
     if rank == 0 and not a.no_extra_legs:
         extra = extra_legs(a, dev, c, maps, mus_h, xs_h, b, tol_np, max_iters, variant)
+    learned_leg = None
+    if os.path.exists(WEIGHTS):
+        learned_leg = run_learned_leg(a, dev, rank, world, maps, ws, variant, schedule)
 
     # ---- roofline of the dominant kernel (attenuated fp with the fused MLEM epilogue, plain path)
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -462,9 +421,6 @@ def run_ours(a):
     achieved = fp_bytes / fp_avg_s / 1e9
     solver_desc = {
         "plain": "plain MLEM (cold start)",
-        "learned": ("MLEM warm-started by the learned encoder-decoder ("
-                    + (f"10 snapshots of one ordered-subsets pass over {k_l} subsets" if k_l else "10 MLEM iterations")
-                    + ", network, MLEM to the residual)"),
         "subsets": f"MLEM warm-started by ordered-subsets EM passes {schedule} (subsets, passes), then MLEM to the residual",
     }
     line = {
@@ -501,6 +457,8 @@ def run_ours(a):
         line["phases_ms_per_step"] = dict(zip(("compute_maps", "subset_passes", "judge_mlem"), ph.mean(axis=0).tolist()))
     for name, r in results.items():
         line[name] = dict(r, solver=solver_desc[name])
+    if learned_leg is not None:
+        line["learned"] = learned_leg
     line.update(extra)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         plain_its = results.get("plain", {}).get("mean_iterations", float(a.iters))
@@ -518,6 +476,106 @@ def run_ours(a):
     if rank == 0:
         print(json.dumps(line), flush=True)
     distributed.finalize()
+
+
+def run_learned_leg(a, dev, rank, world, maps, ws, variant, schedule) -> dict:
+    """The learned warm start on the learned part's own data (config 4's slices at the benchmark
+    shape): seeded textured phantoms (5-20 ellipses with a Gaussian-random-field texture), disk
+    attenuation with mu in [0, 0.02] and emitted mu = 0.7 incident mu, Poisson data at 1e4 peak
+    counts, held-out seeds.  Three paths on the same slices, each step = compute_maps + the solve
+    until every slice reaches the KL residual plain MLEM reaches after 200 iterations: plain MLEM,
+    the ordered-subsets passes alone, and the learned start (a snapshot pass, the network, one
+    pass per ordered-subsets level) followed by MLEM, which judges every slice."""
+    import torch
+
+    from pycorrectedemissionct_b200 import core, distributed, engine
+    from pycorrectedemissionct_b200 import train_warmstart as tw
+    from pycorrectedemissionct_b200.warmstart import WarmStartNet
+
+    net = WarmStartNet(device=dev)
+    net.load(WEIGHTS)
+    S, n, A = a.slices, a.n, a.angles
+    levels = net.os_levels(A)
+    if not levels:
+        return {"unavailable": "the committed network reads MLEM iterates, not ordered-subsets snapshots"}
+    seeds = [a.seed + 500_000 + rank * S + k for k in range(S)]
+    c4, maps4, b4, _, mu4 = tw.synth_batch(n, A, seeds, 0.02, a.learned_peak, dev, subsets=levels, return_mu=True)
+    c4.variant = variant
+    del maps4
+    maps4 = maps  # the shared maps buffer, recomputed by every step in this leg's angle order
+    mu4_out = 0.7 * mu4
+
+    def maps_step():
+        core.compute_maps(mu4, mu4_out, c4.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps4)
+
+    maps_step()
+    calib = engine.BatchedSolver(c4, maps4, b4, "mlem")
+    calib.run(a.iters, check_every=a.iters, use_graph=False)
+    tol = calib.residuals.cpu().numpy() * (1 + 1e-9)
+    del calib
+    plain = engine.BatchedSolver(c4, maps4, b4, "mlem", tolerance=tol)
+    os_ = engine.OrderedSubsets(c4, maps4, b4, [(levels[0], 1), (levels[1], 1)])
+    judge = engine.BatchedSolver(c4, maps4, b4, "mlem", tolerance=tol, x_shared=os_.x)
+    tau = plain.tau
+
+    def run_judge(block):
+        its = 0
+        while its < 2 * a.iters and int(judge.active.sum().item()) > 0:
+            for _ in range(block):
+                judge.step()
+            its += block
+        return judge.iterations
+
+    def step_plain():
+        maps_step()
+        plain.reset()
+        plain.run(2 * a.iters, check_every=10)
+        return float(plain.iterations.float().mean().item()), int(plain.iterations.max().item())
+
+    def step_subsets():
+        maps_step()
+        os_.reset()
+        os_.run_level(0, 2)
+        os_.run_level(1)
+        judge.reset(os_.x)
+        it = run_judge(1)
+        return float(it.float().mean().item()) + 3, int(it.max().item()) + 3
+
+    def step_learned():
+        maps_step()
+        os_.reset()
+        tw.learned_start(net, os_, c4, b4, tau)
+        judge.reset(os_.x)
+        it = run_judge(1)
+        return float(it.float().mean().item()) + 3, int(it.max().item()) + 3
+
+    out = {}
+    for name, fn, k in (("plain", step_plain, 1), ("subsets", step_subsets, a.steps), ("learned", step_learned, a.steps)):
+        for _ in range(1 if name == "plain" else max(1, a.warmup)):
+            fn()
+        distributed.barrier(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        its = [fn() for _ in range(k)]
+        e1.record()
+        distributed.barrier(dev)
+        secs = distributed.max_over_ranks(e0.elapsed_time(e1) / 1e3, dev)
+        out[name] = {"value": S * k * world / secs, "unit": UNIT, "ms_per_step": secs / k * 1e3,
+                     "mean_passes": float(np.mean([i[0] for i in its])), "max_passes": max(i[1] for i in its)}
+    res = {
+        "value": out["learned"]["value"], "unit": UNIT, "ms_per_step": out["learned"]["ms_per_step"],
+        "mean_passes": out["learned"]["mean_passes"], "max_passes": out["learned"]["max_passes"],
+        "solver": (f"learned start (one ordered-subsets pass over {levels[0]} subsets keeping 10 snapshots, the "
+                   f"encoder-decoder, one pass over {levels[0]} and one over {levels[1]} subsets), then MLEM to the "
+                   "plain residual"),
+        "data": (f"config 4 slices at {n}x{n}x{A}: {S} held-out seeds, textured phantoms, mu in [0, 0.02], "
+                 f"emitted mu 0.7 incident, Poisson {a.learned_peak:g} peak counts"),
+        "same_data": {"plain": out["plain"], "subsets": dict(out["subsets"], schedule=[(levels[0], 2), (levels[1], 1)])},
+        "learned_over_plain": out["learned"]["value"] / out["plain"]["value"],
+        "learned_over_subsets": out["learned"]["value"] / out["subsets"]["value"],
+    }
+    del plain, judge, os_, b4
+    return res
 
 
 def fp64_errors(a, c, maps, mu0, x0, dev) -> dict:

@@ -399,6 +399,13 @@ class OrderedSubsets:
         for sm in self.levels[level]:
             sm.step()
 
+    def run_level(self, level: int, passes: int = 1) -> torch.Tensor:
+        """``passes`` eager passes over the subsets of one level of the schedule (whatever the
+        schedule's own pass counts); returns the shared iterate."""
+        for _ in range(passes):
+            self._pass(level)
+        return self.x
+
     def run(self, use_graph: bool = True) -> torch.Tensor:
         """All passes of the schedule; returns the shared iterate."""
         for li, (_, passes) in enumerate(self.schedule):

@@ -3,11 +3,17 @@
 Pairs come from this package's own batched GPU MLEM on seeded synthetic slices (no dataset is
 public on this path): textured phantoms (5-20 ellipses with a smooth Gaussian-random-field
 texture, values in [0, 1]), disk attenuation (mu in [0, 0.02], emitted mu = 0.7 incident mu),
-Poisson data.  Input = the first 10 MLEM iterates plus the normalised back-projection
-A^T b / A^T 1, each slice divided by the mean of its 10th iterate; target = the iterate after
-``target_iterations`` MLEM iterations, as a correction to the 10th iterate in the same units.
+Poisson data.  Input = 10 snapshots of the iterate during one ordered-subsets pass over subsets of
+``net.pass_angles`` angles (in the subset order of ``net.os_levels``) plus the normalised
+back-projection A^T b / A^T 1, each slice divided by the mean of its last snapshot (with
+``pass_angles`` 0: the first 10 MLEM iterates); target = the iterate after ``target_iterations``
+MLEM iterations, as a correction to the last snapshot in the same units.
 
-Usage (GPU):  python -m pycorrectedemissionct_b200.train_warmstart --slices 1024 --steps 1500 --out w.pt
+The learned start (``learned_start``): the snapshot pass, the network, then one more pass at each
+of the two ordered-subsets levels; plain MLEM then finishes to the data-residual tolerance and
+judges every slice.
+
+Usage (GPU):  python -m pycorrectedemissionct_b200.train_warmstart --slices 20000 --steps 12000 --out w.pt
 """
 
 from __future__ import annotations
@@ -77,25 +83,30 @@ def pass_snapshots(os_: OrderedSubsets, count: int = N_ITERATES) -> list[torch.T
 
 
 def synth_batch(n: int, n_angles: int, seeds: list[int], mu_max: float, peak: float, device, textured: bool = True,
-                subsets: int = 0):
+                subsets=0, emitted_ratio: float = 0.7, return_mu: bool = False):
     """Phantoms, attenuation, maps and Poisson data for one batch of slices (angles in the
-    ``subset_permutation`` order of ``subsets`` subsets when ``subsets`` > 0)."""
+    ``subset_permutation`` order of ``subsets``, one count or a list of levels, when given).
+    Returns (core, maps, b, x), and the incident mu as a fifth item with ``return_mu``."""
     xs, mus = [], []
     for sd in seeds:
         rng = phantoms.slice_rng(sd, 0)
         xs.append(textured_phantom(n, rng) if textured else phantoms.ellipse_phantom(n, rng, 12))
         mus.append(phantoms.disk_attenuation(n, rng, mu_max))
     angles = phantoms.angles(n_angles)
-    if subsets > 0:
-        angles = angles[subset_permutation(n_angles, [subsets])]
+    levels = [subsets] if isinstance(subsets, int) else list(subsets)
+    levels = [k for k in levels if k > 0]
+    if levels:
+        angles = angles[subset_permutation(n_angles, levels)]
     c = core.XrfCore(n, angles, device=device)
     mu = torch.from_numpy(np.stack(mus)).to(device)
-    maps = core.compute_maps(mu, 0.7 * mu, c.angles_rad32)
+    maps = core.compute_maps(mu, emitted_ratio * mu, c.angles_rad32)
     x = torch.from_numpy(np.stack(xs)).to(device)
     clean = c.fp(x, maps)
     gen = torch.Generator(device=device)
     gen.manual_seed(int(seeds[0]))
     b = torch.poisson(clean / clean.amax(dim=(1, 2, 3), keepdim=True) * peak, generator=gen)
+    if return_mu:
+        return c, maps, b, x, mu
     return c, maps, b, x
 
 
@@ -105,13 +116,13 @@ def generate_pairs(n_slices: int, n: int = 256, n_angles: int = 360, seed: int =
     device = core.require_cuda(device)
     helper = net if net is not None else WarmStartNet(device=device)
     inputs, targets = [], []
-    n_sub = helper.pass_subsets(n_angles)
+    levels = helper.os_levels(n_angles)
     for s0 in range(0, n_slices, batch):
         seeds = [seed + k for k in range(s0, min(n_slices, s0 + batch))]
-        c, maps, b, _ = synth_batch(n, n_angles, seeds, mu_max, peak, device, subsets=n_sub)
+        c, maps, b, _ = synth_batch(n, n_angles, seeds, mu_max, peak, device, subsets=levels)
         solver = BatchedSolver(c, maps, b, "mlem")
-        if n_sub > 0:
-            its = pass_snapshots(OrderedSubsets(c, maps, b, [(n_sub, 1)]))
+        if levels:
+            its = pass_snapshots(OrderedSubsets(c, maps, b, [(levels[0], 1), (levels[1], 1)]))
             bpn = normalized_backprojection(c, b, solver.tau)
             solver.run(target_iterations, check_every=target_iterations, use_graph=False)
         else:
@@ -157,42 +168,94 @@ def train(net: WarmStartNet, inputs: torch.Tensor, targets: torch.Tensor, steps:
     return losses
 
 
+def learned_start(net: WarmStartNet, os_: OrderedSubsets, c: core.XrfCore, b: torch.Tensor,
+                  tau: torch.Tensor) -> torch.Tensor:
+    """The learned start on an ordered-subsets solver whose levels are ``net.os_levels(A)`` (data in
+    that order): one pass over the first level keeping 10 snapshots, the network on the snapshots
+    and the normalised back projection (A^T b / tau), then one pass over each level from the
+    network's prediction.  Three full-data passes and one network evaluation; returns the shared
+    iterate."""
+    its = pass_snapshots(os_)
+    bpn = normalized_backprojection(c, b, tau)
+    x0 = net.predict(its + [bpn], base=its[-1], slice_scale=slice_means(its[-1]))
+    os_.x.copy_(x0)
+    os_.run_level(0)
+    os_.run_level(1)
+    return os_.x
+
+
 def warm_started_solve(net: WarmStartNet, c: core.XrfCore, maps: torch.Tensor, b: torch.Tensor, tolerance,
-                       max_iterations: int = 400, check_every: int = 5, history_len: int = 0):
-    """10 plain MLEM iterations (or 10 snapshots of one ordered-subsets pass, by the network's
-    inputs) -> network -> MLEM from the prediction until `tolerance`.  With ordered-subsets inputs,
-    ``c``, ``maps`` and ``b`` must be in ``subset_permutation(A, [net.pass_subsets(A)])`` angle
-    order.
+                       max_iterations: int = 400, check_every: int = 1, history_len: int = 0, use_net: bool = True):
+    """The learned start (``learned_start``), then MLEM from it until `tolerance`; ``c``, ``maps`` and
+    ``b`` in ``subset_permutation(A, net.os_levels(A))`` angle order.  With ``use_net`` False the
+    network is skipped (the same three passes from the snapshot pass's end): the method without
+    the network.  Networks fed the first 10 MLEM iterates (``pass_angles`` 0) run them instead.
 
     Returns (solver, total full-data passes per slice as a numpy array)."""
     first = BatchedSolver(c, maps, b, "mlem")
-    n_sub = net.pass_subsets(c.n_angles)
-    if n_sub > 0:
-        its = pass_snapshots(OrderedSubsets(c, maps, b, [(n_sub, 1)]))
+    levels = net.os_levels(c.n_angles)
+    if levels:
+        os_ = OrderedSubsets(c, maps, b, [(levels[0], 1), (levels[1], 1)])
+        if use_net:
+            x0 = learned_start(net, os_, c, b, first.tau)
+        else:
+            os_.run_level(0)
+            os_.run_level(0)
+            x0 = os_.run_level(1)
+        passes = 3
     else:
         its = first_iterates(first)
-    bpn = normalized_backprojection(c, b, first.tau)
-    scale = slice_means(its[-1])
-    x0 = net.predict(its + [bpn], base=its[-1], slice_scale=scale)
+        bpn = normalized_backprojection(c, b, first.tau)
+        x0 = net.predict(its + [bpn], base=its[-1], slice_scale=slice_means(its[-1])) if use_net else its[-1]
+        passes = N_ITERATES
     solver = BatchedSolver(c, maps, b, "mlem", tolerance=tolerance, x0=x0, history_len=history_len)
-    solver.run(max_iterations, check_every=check_every)
-    return solver, solver.iterations.cpu().numpy() + (1 if n_sub > 0 else N_ITERATES)
+    solver.run(max_iterations, check_every=check_every, use_graph=False)
+    return solver, solver.iterations.cpu().numpy() + passes
+
+
+def evaluate(net: WarmStartNet, n: int, n_angles: int, n_slices: int, seed: int, batch: int = 32, device=None,
+             plain_iterations: int = 200) -> dict:
+    """Held-out evaluation on config-4-style slices: per slice, the full-data passes that plain
+    MLEM (cold start), the learned start + MLEM, and the same passes without the network need to
+    reach the KL residual plain MLEM reaches after ``plain_iterations`` iterations."""
+    device = core.require_cuda(device)
+    levels = net.os_levels(n_angles)
+    learned, without, ok = [], [], 0
+    for s0 in range(0, n_slices, batch):
+        seeds = [seed + k for k in range(s0, min(n_slices, s0 + batch))]
+        c, maps, b, _ = synth_batch(n, n_angles, seeds, 0.02, 1e4, device, subsets=levels)
+        plain = BatchedSolver(c, maps, b, "mlem")
+        plain.run(plain_iterations, check_every=plain_iterations, use_graph=False)
+        tol = plain.residuals.cpu().numpy() * (1 + 1e-9)
+        sv, total = warm_started_solve(net, c, maps, b, tol, max_iterations=2 * plain_iterations)
+        ok += int((sv.residuals.cpu().numpy() <= tol).sum())
+        learned.append(total)
+        _, total0 = warm_started_solve(net, c, maps, b, tol, max_iterations=2 * plain_iterations, use_net=False)
+        without.append(total0)
+        del maps, plain, sv
+    learned, without = np.concatenate(learned), np.concatenate(without)
+    return {"n": n, "angles": n_angles, "slices": int(learned.size), "plain_passes": plain_iterations,
+            "learned_mean": float(learned.mean()), "learned_max": int(learned.max()),
+            "without_network_mean": float(without.mean()), "without_network_max": int(without.max()),
+            "reached_residual": ok}
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--slices", type=int, default=1024)
+    ap.add_argument("--slices", type=int, default=20000)
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--angles", type=int, default=360)
-    ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--steps", type=int, default=12000)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--target-iterations", type=int, default=500)
     ap.add_argument("--additive", action="store_true", help="additive instead of log-ratio (multiplicative) targets")
     ap.add_argument("--log-floor", type=float, default=1e-3, help="floor of the log-ratio target, in slice means")
-    ap.add_argument("--pass-angles", type=int, default=0,
+    ap.add_argument("--pass-angles", type=int, default=8,
                     help="inputs: 10 snapshots of one ordered-subsets pass over subsets of this many angles "
                          "(0: the first 10 MLEM iterates)")
+    ap.add_argument("--finish-factor", type=int, default=5)
+    ap.add_argument("--eval-slices", type=int, default=0, help="held-out slices per evaluation shape")
     ap.add_argument("--out", default="warmstart.pt")
     a = ap.parse_args()
     dev = core.require_cuda()
@@ -201,11 +264,13 @@ def main():
     net.multiplicative = not a.additive
     net.log_floor = a.log_floor
     net.pass_angles = a.pass_angles
-    inputs, targets = generate_pairs(a.slices, a.n, a.angles, target_iterations=a.target_iterations, device=dev, net=net)
+    net.finish_factor = a.finish_factor
+    inputs, targets = generate_pairs(a.slices, a.n, a.angles, target_iterations=a.target_iterations, device=dev,
+                                     net=net, batch=128)
     torch.cuda.synchronize()
     t1 = time.time()
     print(f"pairs: {inputs.shape[0]} in {t1 - t0:.1f} s; params {net.n_params()}", flush=True)
-    losses = train(net, inputs, targets, a.steps, a.batch, a.lr)
+    losses = train(net, inputs, targets, a.steps, a.batch, a.lr, log_every=1000)
     torch.cuda.synchronize()
     print(f"trained {a.steps} steps in {time.time() - t1:.1f} s; loss {losses[0]:.4f} -> {losses[-1]:.4f}", flush=True)
     v = ctypes.c_int32(0)
@@ -213,6 +278,14 @@ def main():
     if v.value:
         raise RuntimeError("a tensor-core wait timed out during training")
     net.save(a.out)
+    del inputs, targets
+    torch.cuda.empty_cache()
+    if a.eval_slices > 0:
+        import json
+
+        for n, n_ang in ((a.n, a.angles), (2 * a.n, 2 * a.angles)):
+            r = evaluate(net, n, n_ang, a.eval_slices, seed=900_000 + n, device=dev)
+            print("eval", json.dumps(r), flush=True)
 
 
 if __name__ == "__main__":

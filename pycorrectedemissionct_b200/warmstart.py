@@ -90,11 +90,25 @@ class WarmStartNet:
         # inputs: 0 = the first 10 MLEM iterates; k > 0 = 10 snapshots of the iterate taken during
         # one ordered-subsets pass over subsets of k angles each (A // k subsets)
         self.pass_angles = 0
+        # ordered-subsets levels around the network: the snapshot pass's level and a finishing
+        # level with about finish_factor times fewer subsets (os_levels)
+        self.finish_factor = 5
 
     # ------------------------------------------------------------------ helpers
     def pass_subsets(self, n_angles: int) -> int:
         """Subsets of the one ordered-subsets pass that makes the inputs (0: MLEM inputs)."""
         return 0 if self.pass_angles <= 0 else min(n_angles, max(N_ITERATES, n_angles // self.pass_angles))
+
+    def os_levels(self, n_angles: int) -> list[int]:
+        """Subset counts [k1, k2] of the ordered-subsets passes around the network: k1 is the snapshot
+        pass's, k2 the largest divisor of k1 that is at most k1 / finish_factor.  Data, maps and
+        geometry go in ``engine.subset_permutation(A, os_levels(A))`` order."""
+        k1 = self.pass_subsets(n_angles)
+        if k1 <= 0:
+            return []
+        cap = max(1, k1 // max(1, self.finish_factor))
+        k2 = max(d for d in range(1, cap + 1) if k1 % d == 0)
+        return [k1, k2]
 
     def n_params(self) -> int:
         return sum(l.w.numel() + l.b.numel() for l in self.layers.values())
@@ -258,7 +272,7 @@ class WarmStartNet:
         """BF16 weights, FP32 biases and the target parameterisation."""
         st = {k: (l.w.to(BF16).cpu(), l.b.cpu()) for k, l in self.layers.items()}
         st.update(step=self.step_count, multiplicative=self.multiplicative, log_floor=self.log_floor,
-                  pass_angles=self.pass_angles)
+                  pass_angles=self.pass_angles, finish_factor=self.finish_factor)
         torch.save(st, path)
 
     def load(self, path: str) -> None:
@@ -271,3 +285,4 @@ class WarmStartNet:
         self.multiplicative = bool(st.get("multiplicative", False))
         self.log_floor = float(st.get("log_floor", 1e-2))
         self.pass_angles = int(st.get("pass_angles", 0))
+        self.finish_factor = int(st.get("finish_factor", 5))
