@@ -247,9 +247,11 @@ def run_ours(a):
     x_true = torch.from_numpy(xs_h).to(dev)
     tdt = torch.float32 if a.maps_dtype == "float32" else torch.bfloat16
     maps = torch.empty((S, a.angles, 1, n, n), dtype=tdt, device=dev)  # recomputed by every step, in its order
-    _, P = core.geometry.padded_size(n)
-    # maps workspace: ~16 angles of the whole batch per pass (incident + emitted W of P^2 floats)
-    ws = torch.empty(max(core.DEFAULT_MAPS_WORKSPACE, 16 * 2 * (P * P + P) * 4 * S), dtype=torch.uint8, device=dev)
+    # maps workspace: the entries per pass (half-turn pairs of angles) the autotuner picks for this
+    # batch within 6 GB
+    entries = autotune.tune_maps(mu_in, mu_out, c.angles_rad32, maps_dtype=a.maps_dtype, budget_bytes=6 << 30,
+                                 out=maps)
+    ws = torch.empty(entries * core.maps_entry_bytes(n, S), dtype=torch.uint8, device=dev)
 
     def maps_natural():
         core.compute_maps(mu_in, mu_out, c.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
@@ -662,8 +664,7 @@ def extra_legs(a, dev, c, maps, mus_h, xs_h, b, tol_np, max_iters, variant) -> d
         out["fp64_error"] = {"unavailable": repr(exc)}
     # ---- BF16-stored maps: map error against FP32 maps, plain MLEM (200 iterations) speed
     m16 = torch.empty((S, a.angles, 1, n, n), dtype=torch.bfloat16, device=dev)
-    ws = torch.empty(16 * 2 * (core.geometry.padded_size(n)[1] ** 2 + core.geometry.padded_size(n)[1]) * 4 * S,
-                     dtype=torch.uint8, device=dev)
+    ws = torch.empty(16 * core.maps_entry_bytes(n, S), dtype=torch.uint8, device=dev)
     core.compute_maps(mu_t, mu_t, c.angles_rad32, maps_dtype="bfloat16", workspace=ws, out=m16)
     torch.cuda.synchronize(dev)
     e16 = float(((m16[0].float() - maps[0].float()).double().norm() / maps[0].double().norm()).item())
@@ -719,8 +720,7 @@ def run_waves(a):
         wave = max(1, min(a.wave_slices, int(0.8 * free // per_slice)))
         tdt = torch.float32 if dtype == "float32" else torch.bfloat16
         total_s, done = 0.0, 0
-        _, P = core.geometry.padded_size(n)
-        ws = torch.empty(16 * 2 * (P * P + P) * 4 * wave, dtype=torch.uint8, device=dev)
+        ws = torch.empty(16 * core.maps_entry_bytes(n, wave), dtype=torch.uint8, device=dev)
         maps = torch.empty((wave, A, 1, n, n), dtype=tdt, device=dev)
         for w0 in range(0, a.wave_slices, wave):
             k = min(wave, a.wave_slices - w0)
@@ -788,8 +788,7 @@ def run_channels(a):
             xs.append(phantoms.ellipse_phantom(n, phantoms.slice_rng(a.seed + 37, f * C + ch), 12))
     mu = torch.from_numpy(np.stack(mus)).to(dev)
     x_true = torch.from_numpy(np.stack(xs)).to(dev)
-    _, P = core.geometry.padded_size(n)
-    ws = torch.empty(8 * 2 * (P * P + P) * 4 * F, dtype=torch.uint8, device=dev)
+    ws = torch.empty(8 * core.maps_entry_bytes(n, F), dtype=torch.uint8, device=dev)
     fields = core.compute_maps(mu, mu, c.angles_rad32, maps_dtype="fields-float32", workspace=ws)
     clean = c.fp(x_true, fields)
     gen = torch.Generator(device=dev)

@@ -1,4 +1,4 @@
-"""Kernel-variant autotuner with an on-disk cache.
+"""Kernel-variant and pass-size autotuner with an on-disk cache.
 
 The fp kernel has three variants with identical results: one slice per CTA with load/store
 staging (default) or TMA bulk-tensor staging (``CCT_VARIANT_FP_TMA``), and two slices per CTA
@@ -8,6 +8,12 @@ angle range of a larger array (the TMA variant needs dense maps), so ``tune`` ti
 applicable variant on the actual call (CUDA events, a few launches over a batch of the real
 size) and caches the winner per (GPU, n, angles, detectors, slices, map dtype, layout) in a
 JSON file (``$CCT_AUTOTUNE_CACHE`` or ``~/.cache/corrct_b200/autotune.json``).
+
+``tune_maps`` does the same for ``compute_maps``: how many entries (angles, or half-turn pairs)
+one pass of the scan and resample kernels covers, i.e. the workspace size, timed within a memory
+budget (larger passes keep more of the GPU busy per launch; their rotated-frame workspace spills
+from L2 either way).  ``maps_entries`` returns a cached choice without timing (the ragged stream
+consults it for each of its groups).
 """
 
 from __future__ import annotations
@@ -16,9 +22,10 @@ import json
 import os
 import threading
 
+import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, core
 from .core import XrfCore
 
 _LOCK = threading.Lock()
@@ -94,3 +101,53 @@ def tune(core: XrfCore, vol: torch.Tensor, maps: torch.Tensor, force: bool = Fal
         _store(cache)
         core.variant = best
         return best
+
+
+MAPS_ENTRIES = (4, 8, 16, 32)
+
+
+def maps_key(device, n: int, n_angles: int, n_det: int, n_slices: int, maps_dtype: str) -> str:
+    name = torch.cuda.get_device_name(device).replace(" ", "_")
+    return f"maps|{name}|n{n}|a{n_angles}|d{n_det}|s{n_slices}|{maps_dtype}"
+
+
+def maps_entries(device, n: int, n_angles: int, n_det: int, n_slices: int, maps_dtype: str = "float32") -> int | None:
+    """The cached entries per pass of ``tune_maps`` for this shape, or None."""
+    hit = _load().get(maps_key(device, n, n_angles, n_det, n_slices, maps_dtype))
+    return None if hit is None else int(hit["entries"])
+
+
+def tune_maps(mu_in: torch.Tensor, mu_out: torch.Tensor, angles_rad32, det_angles=(np.pi / 2,),
+              maps_dtype: str = "float32", budget_bytes: int = 4 << 30, out: torch.Tensor | None = None,
+              force: bool = False) -> int:
+    """Entries per pass of ``compute_maps`` for this batch (cached): times every choice of
+    ``MAPS_ENTRIES`` whose workspace fits ``budget_bytes`` (two calls each, CUDA events)."""
+    ref = mu_in if mu_in is not None else mu_out
+    s, n = ref.shape[0], ref.shape[-1]
+    n_det = len(np.atleast_1d(det_angles))
+    n_angles = len(np.atleast_1d(angles_rad32))
+    k = maps_key(ref.device, n, n_angles, n_det, s, maps_dtype)
+    with _LOCK:
+        cache = _load()
+        if not force and k in cache:
+            return int(cache[k]["entries"])
+        per_entry = core.maps_entry_bytes(n, s, n_det, 1, mu_in is not None, mu_out is not None)
+        choices = [e for e in MAPS_ENTRIES if e * per_entry <= budget_bytes] or [1]
+        times = {}
+        for e in choices:
+            ws = torch.empty(e * per_entry, dtype=torch.uint8, device=ref.device)
+            out = core.compute_maps(mu_in, mu_out, angles_rad32, det_angles, maps_dtype=maps_dtype, workspace=ws,
+                                    out=out)
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            for _ in range(2):
+                core.compute_maps(mu_in, mu_out, angles_rad32, det_angles, maps_dtype=maps_dtype, workspace=ws, out=out)
+            stop.record()
+            stop.synchronize()
+            times[e] = start.elapsed_time(stop) / 2
+            del ws
+        best = min(times, key=times.get)
+        cache[k] = {"entries": best, "ms": {str(e): t for e, t in times.items()}}
+        _store(cache)
+        return best
+

@@ -397,6 +397,18 @@ def compute_maps(
     return maps
 
 
+def maps_entry_bytes(n: int, n_slices: int, n_det: int = 1, n_sub: int = 1, has_in: bool = True,
+                     has_out: bool = True) -> int:
+    """Workspace bytes ``compute_maps`` needs per entry of a pass (one angle, or one half-turn pair
+    of angles) for a batch of ``n_slices`` slices (``cct_maps_workspace_size``)."""
+    desc = _lib.MapsDesc()
+    desc.n, desc.n_angles, desc.n_det, desc.n_slices, desc.n_sub = int(n), 1, int(n_det), int(n_slices), int(n_sub)
+    desc.has_in, desc.has_out = int(has_in), int(has_out)
+    need = ctypes.c_size_t(0)
+    _lib.call("cct_maps_workspace_size", ctypes.byref(desc), 1, ctypes.byref(need))
+    return int(need.value)
+
+
 def reduce_norm(v: torch.Tensor, ord: int = 2) -> torch.Tensor:
     """Per-slice FP64 norm sums of a (S, ...) float32 CUDA tensor: sum |v| (ord 1) or sum v^2 (ord 2)."""
     device = require_cuda(v.device)

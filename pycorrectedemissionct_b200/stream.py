@@ -21,6 +21,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
+from . import autotune
 from . import core as _core
 from .engine import BatchedSolver, OrderedSubsets, RaggedSolvers, subset_permutation
 
@@ -95,6 +96,11 @@ class _Group:
         f32 = dict(dtype=torch.float32, device=device)
         mu_in = None if j0.mu_in is None else torch.from_numpy(np.stack([j.mu_in for j in jobs])).to(**f32)
         mu_out = None if j0.mu_out is None else torch.from_numpy(np.stack([j.mu_out for j in jobs])).to(**f32)
+        # the pass size the autotuner chose for this group's shape, when it has one
+        entries = autotune.maps_entries(device, j0.n, len(angles), 1, len(jobs), maps_dtype)
+        if entries is not None:
+            per_entry = _core.maps_entry_bytes(j0.n, len(jobs))
+            workspace = workspace[: min(workspace.numel(), entries * per_entry)]
         self.maps = _core.compute_maps(mu_in, mu_out, self.core.angles_rad32, maps_dtype=maps_dtype,
                                        workspace=workspace)
         b = np.stack([j.b for j in jobs])[:, None]

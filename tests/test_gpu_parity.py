@@ -428,6 +428,24 @@ def test_fp_variants_bit_identical(n, n_ang, dtype, s, cuda, tmp_path, monkeypat
     assert torch.equal(c.fp(x, maps), ref)
 
 
+def test_maps_pass_size_tuning(cuda, tmp_path, monkeypatch):
+    """The maps autotuner picks the entries per pass of compute_maps for a batch, caches the choice,
+    and every pass size gives bit-identical maps."""
+    from pycorrectedemissionct_b200 import autotune, core, phantoms
+
+    monkeypatch.setenv("CCT_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    n, n_ang, s = 96, 72, 3
+    rad32 = np.array(phantoms.angles(n_ang), dtype=np.float32)
+    mu = _t(np.stack([phantoms.disk_attenuation(n, phantoms.slice_rng(55, k), 0.03) for k in range(s)]), cuda)
+    ref = core.compute_maps(mu, 0.7 * mu, rad32)
+    assert autotune.maps_entries(cuda, n, n_ang, 1, s) is None
+    e = autotune.tune_maps(mu, 0.7 * mu, rad32)
+    assert e in autotune.MAPS_ENTRIES and autotune.maps_entries(cuda, n, n_ang, 1, s) == e
+    for entries in (1, 5, e):
+        ws = torch.empty(entries * core.maps_entry_bytes(n, s), dtype=torch.uint8, device=cuda)
+        assert torch.equal(core.compute_maps(mu, 0.7 * mu, rad32, workspace=ws), ref)
+
+
 @pytest.mark.parametrize("method", ["mlem", "sirt", "pdhg"])
 def test_fused_solvers_identical_across_fp_variants(method, cuda):
     """The fused solver epilogues (MLEM ratio and KL residual, SIRT residual, PDHG dual) give the
