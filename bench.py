@@ -250,14 +250,18 @@ def run_ours(a):
     # maps workspace: the entries per pass (half-turn pairs of angles) the autotuner picks for this
     # batch within 6 GB
     entries = autotune.tune_maps(mu_in, mu_out, c.angles_rad32, maps_dtype=a.maps_dtype, budget_bytes=6 << 30,
-                                 out=maps)
+                                 out=maps, emitted_scale=1.0)
     ws = torch.empty(entries * core.maps_entry_bytes(n, S), dtype=torch.uint8, device=dev)
 
+    # mu_out = mu_in in this workload: each emitted line integral is the incident one of the angle
+    # a quarter turn on (compute_maps' quarter-turn quads)
     def maps_natural():
-        core.compute_maps(mu_in, mu_out, c.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
+        core.compute_maps(mu_in, mu_out, c.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps,
+                          emitted_scale=1.0)
 
     def maps_subsets():
-        core.compute_maps(mu_in, mu_out, c_os.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps)
+        core.compute_maps(mu_in, mu_out, c_os.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps,
+                          emitted_scale=1.0)
 
     maps_natural()
     passes = core.compute_maps.last_passes  # two kernels per pass
@@ -508,7 +512,8 @@ def run_learned_leg(a, dev, rank, world, maps, ws, variant, schedule) -> dict:
     mu4_out = 0.7 * mu4
 
     def maps_step():
-        core.compute_maps(mu4, mu4_out, c4.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps4)
+        core.compute_maps(mu4, mu4_out, c4.angles_rad32, maps_dtype=a.maps_dtype, workspace=ws, out=maps4,
+                          emitted_scale=0.7)
 
     maps_step()
     calib = engine.BatchedSolver(c4, maps4, b4, "mlem")

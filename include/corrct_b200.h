@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define CCT_ABI_VERSION 6
+#define CCT_ABI_VERSION 7
 
 /* Status codes. */
 #define CCT_OK 0
@@ -145,6 +145,21 @@ typedef struct cct_maps_desc {
                             range indices are skipped. */
   int32_t n_entries;     /* entries of `pairs` (ignored when pairs is NULL) */
   int32_t reserved;
+  const int32_t* quads;  /* device [n_quads][6], or NULL.  Quarter-turn quads for one point detector
+                            whose emitted direction (angle + detector angle + pi) is, for every
+                            angle, the incident direction of another angle of the set, with
+                            mu_out = emitted_scale * mu_in: row (e, e', s0, s1, s2, s3) names two
+                            `pairs` entries, whose angles and partners are the quad's four angles
+                            k = 0..3 (e's angle, e's partner, e''s angle, e''s partner), and s_k, the
+                            one among them whose incident direction is angle k's emitted direction.
+                            Only incident fields are scanned (two per quad) and the map of angle k
+                            is exp(-L_in(k)) * exp(-emitted_scale * L_in(s_k)) (the emitted rotation
+                            then differs from the reference's by the float32 rounding of the angles,
+                            as a half-turn partner's does).  Needs pairs, n_det == n_sub == 1,
+                            has_in and has_out set, F32 or BF16 maps; mu_out is not read.
+                            Every pairs entry must be in exactly one quad. */
+  int32_t n_quads;
+  float emitted_scale;   /* quads: mu_out / mu_in (>= 0) */
 } cct_maps_desc;
 
 /* Workspace bytes needed to process `angles_per_pass` angles (entries, with pairs) per pass (>= 1). */

@@ -13,7 +13,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcorrct_b200.so")
 
-ABI_VERSION = 6  # CCT_ABI_VERSION of include/corrct_b200.h
+ABI_VERSION = 7  # CCT_ABI_VERSION of include/corrct_b200.h
 
 CCT_OK = 0
 CCT_ERR_VALUE = 1
@@ -73,6 +73,9 @@ class MapsDesc(ctypes.Structure):
         ("pairs", ctypes.c_void_p),
         ("n_entries", ctypes.c_int32),
         ("reserved", ctypes.c_int32),
+        ("quads", ctypes.c_void_p),
+        ("n_quads", ctypes.c_int32),
+        ("emitted_scale", ctypes.c_float),
     ]
 
 

@@ -106,27 +106,28 @@ def tune(core: XrfCore, vol: torch.Tensor, maps: torch.Tensor, force: bool = Fal
 MAPS_ENTRIES = (4, 8, 16, 32)
 
 
-def maps_key(device, n: int, n_angles: int, n_det: int, n_slices: int, maps_dtype: str) -> str:
+def maps_key(device, n: int, n_angles: int, n_det: int, n_slices: int, maps_dtype: str, quads: bool = False) -> str:
     name = torch.cuda.get_device_name(device).replace(" ", "_")
-    return f"maps|{name}|n{n}|a{n_angles}|d{n_det}|s{n_slices}|{maps_dtype}"
+    return f"maps|{name}|n{n}|a{n_angles}|d{n_det}|s{n_slices}|{maps_dtype}" + ("|quads" if quads else "")
 
 
-def maps_entries(device, n: int, n_angles: int, n_det: int, n_slices: int, maps_dtype: str = "float32") -> int | None:
+def maps_entries(device, n: int, n_angles: int, n_det: int, n_slices: int, maps_dtype: str = "float32",
+                 quads: bool = False) -> int | None:
     """The cached entries per pass of ``tune_maps`` for this shape, or None."""
-    hit = _load().get(maps_key(device, n, n_angles, n_det, n_slices, maps_dtype))
+    hit = _load().get(maps_key(device, n, n_angles, n_det, n_slices, maps_dtype, quads))
     return None if hit is None else int(hit["entries"])
 
 
 def tune_maps(mu_in: torch.Tensor, mu_out: torch.Tensor, angles_rad32, det_angles=(np.pi / 2,),
               maps_dtype: str = "float32", budget_bytes: int = 4 << 30, out: torch.Tensor | None = None,
-              force: bool = False) -> int:
+              force: bool = False, emitted_scale: float | None = None) -> int:
     """Entries per pass of ``compute_maps`` for this batch (cached): times every choice of
     ``MAPS_ENTRIES`` whose workspace fits ``budget_bytes`` (two calls each, CUDA events)."""
     ref = mu_in if mu_in is not None else mu_out
     s, n = ref.shape[0], ref.shape[-1]
     n_det = len(np.atleast_1d(det_angles))
     n_angles = len(np.atleast_1d(angles_rad32))
-    k = maps_key(ref.device, n, n_angles, n_det, s, maps_dtype)
+    k = maps_key(ref.device, n, n_angles, n_det, s, maps_dtype, emitted_scale is not None)
     with _LOCK:
         cache = _load()
         if not force and k in cache:
@@ -137,11 +138,12 @@ def tune_maps(mu_in: torch.Tensor, mu_out: torch.Tensor, angles_rad32, det_angle
         for e in choices:
             ws = torch.empty(e * per_entry, dtype=torch.uint8, device=ref.device)
             out = core.compute_maps(mu_in, mu_out, angles_rad32, det_angles, maps_dtype=maps_dtype, workspace=ws,
-                                    out=out)
+                                    out=out, emitted_scale=emitted_scale)
             start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             start.record()
             for _ in range(2):
-                core.compute_maps(mu_in, mu_out, angles_rad32, det_angles, maps_dtype=maps_dtype, workspace=ws, out=out)
+                core.compute_maps(mu_in, mu_out, angles_rad32, det_angles, maps_dtype=maps_dtype, workspace=ws, out=out,
+                                  emitted_scale=emitted_scale)
             stop.record()
             stop.synchronize()
             times[e] = start.elapsed_time(stop) / 2

@@ -318,7 +318,11 @@ def _maps_tables(device, n, angles_rad32, det_angles, surfaces_mm2, distances_mm
     rot_out_d = torch.from_numpy(np.ascontiguousarray(rot_out)).to(device)
     pairs = geometry.half_turn_pairs(a32) if half_turns else None
     pairs_d = None if pairs is None else torch.from_numpy(pairs).to(device)
-    entry = (rot_in_d, rot_out_d, n_sub, pairs_d)
+    quads = None
+    if pairs is not None and n_sub == 1 and rot_out.shape[1] == 1:
+        quads = geometry.quarter_turn_quads(a32, pairs, float(np.array(det_angles, ndmin=1, dtype=np.float64)[0]))
+    quads_d = None if quads is None else torch.from_numpy(quads).to(device)
+    entry = (rot_in_d, rot_out_d, n_sub, pairs_d, quads_d)
     with _MAPS_TABLES_LOCK:
         _MAPS_TABLES[key] = entry
         while len(_MAPS_TABLES) > _MAPS_TABLES_MAX:
@@ -339,11 +343,19 @@ def compute_maps(
     workspace_bytes: int = DEFAULT_MAPS_WORKSPACE,
     out: torch.Tensor | None = None,
     half_turns: bool = True,
+    emitted_scale: float | None = None,
+    quarter_turns: bool = True,
 ) -> torch.Tensor:
     """Attenuation maps (S, A, D, n, n) on the device from mu_in / mu_out (S, n, n) float32.
 
     ``half_turns``: angles whose half-turn partner (angle + pi) is also in the set share one
     rotation per direction (``geometry.half_turn_pairs``); False computes every angle on its own.
+    ``emitted_scale``: the caller's statement that mu_out = emitted_scale * mu_in (taken as 1 when
+    ``mu_out`` is ``mu_in`` itself).  With it, one point detector whose emitted direction is another
+    angle's incident direction (``geometry.quarter_turn_quads``, e.g. a detector at pi / 2 and an
+    angle count divisible by 4 over a full turn) and ``quarter_turns``, only incident fields are
+    scanned: each angle's emitted line integral is emitted_scale times the incident one of the
+    angle a quarter turn on.
     """
     ref = mu_in if mu_in is not None else mu_out
     if ref is None:
@@ -356,9 +368,13 @@ def compute_maps(
     if maps_dtype not in MAPS_DTYPES:
         raise ValueError(f"maps_dtype must be one of {sorted(MAPS_DTYPES)}")
     tdt, cdt = MAPS_DTYPES[maps_dtype]
-    rot_in_d, rot_out_d, n_sub, pairs_d = _maps_tables(
+    rot_in_d, rot_out_d, n_sub, pairs_d, quads_d = _maps_tables(
         device, n, angles_rad32, det_angles, surfaces_mm2, distances_mm, sub_sampling, half_turns
     )
+    if emitted_scale is None and mu_out is not None and mu_out is mu_in:
+        emitted_scale = 1.0
+    use_quads = (quarter_turns and quads_d is not None and emitted_scale is not None and mu_in is not None
+                 and mu_out is not None and cdt != _lib.CCT_DTYPE_FIELDS_F32)
     n_ang, n_det = rot_out_d.shape[0], rot_out_d.shape[1]
     desc = _lib.MapsDesc()
     desc.n, desc.n_angles, desc.n_det, desc.n_slices = n, n_ang, n_det, s
@@ -369,6 +385,9 @@ def compute_maps(
     if pairs_d is not None:
         desc.pairs, desc.n_entries = pairs_d.data_ptr(), pairs_d.shape[0]
         entries = pairs_d.shape[0]
+    if use_quads:
+        desc.quads, desc.n_quads, desc.emitted_scale = quads_d.data_ptr(), quads_d.shape[0], float(emitted_scale)
+        entries = quads_d.shape[0]  # a quad takes one entry's workspace (two incident fields)
     need = ctypes.c_size_t(0)
     _lib.call("cct_maps_workspace_size", ctypes.byref(desc), 1, ctypes.byref(need))
     if workspace is None:
@@ -389,7 +408,7 @@ def compute_maps(
     # the cached tables may be dropped from the cache (and freed) by a later call while this
     # launch still reads them on this stream: tie their memory to the stream's pending work
     stream = torch.cuda.current_stream(device)
-    for t in (rot_in_d, rot_out_d, pairs_d):
+    for t in (rot_in_d, rot_out_d, pairs_d, quads_d):
         if t is not None:
             t.record_stream(stream)
     # torch's caching allocator reuses a workspace allocated here only for work queued later on

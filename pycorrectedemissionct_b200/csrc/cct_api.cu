@@ -124,6 +124,18 @@ int cct_bp(const cct_xrf_desc* desc, int32_t mode, const float* sino, const void
   return check_launch();
 }
 
+// Quarter-turn quads (cct_maps_desc.quads): the combinations they need (the table itself is device
+// memory; the kernels skip rows that name entries out of range).
+static int validate_quads(const cct_maps_desc* d) {
+  if (d->quads == nullptr) return CCT_OK;
+  CCT_REQUIRE(d->pairs != nullptr && d->n_det == 1 && d->n_sub == 1 && d->has_in && d->has_out,
+              "quads need half-turn pairs, one point detector, and incident and emitted attenuation");
+  CCT_REQUIRE(d->maps_dtype == CCT_DTYPE_F32 || d->maps_dtype == CCT_DTYPE_BF16, "quads need F32 or BF16 maps");
+  CCT_REQUIRE(d->n_quads >= 1 && 2 * (int64_t)d->n_quads == d->n_entries, "quads must cover every pairs entry once");
+  CCT_REQUIRE(d->emitted_scale >= 0.f, "emitted_scale must be >= 0");
+  return CCT_OK;
+}
+
 int cct_maps_workspace_size(const cct_maps_desc* desc, int32_t angles_per_pass, size_t* bytes) {
   CCT_REQUIRE(desc != nullptr && bytes != nullptr, "descriptor and bytes are required");
   CCT_REQUIRE(desc->n >= 2 && desc->n <= 8192, "volume side n must be in [2, 8192]");
@@ -148,7 +160,10 @@ int cct_compute_maps(const cct_maps_desc* desc, const float* mu_in, const float*
   CCT_REQUIRE(desc->maps_dtype != CCT_DTYPE_FIELDS_F32 || desc->n_sub == 1,
               "line-integral fields need one emitted direction per detector (n_sub == 1)");
   CCT_REQUIRE(!desc->has_in || (mu_in != nullptr && desc->rot_in != nullptr), "incident volume or matrices missing");
-  CCT_REQUIRE(!desc->has_out || (mu_out != nullptr && desc->rot_out != nullptr), "emitted volume or matrices missing");
+  rc = validate_quads(desc);
+  if (rc != CCT_OK) return rc;
+  CCT_REQUIRE(!desc->has_out || desc->quads != nullptr || (mu_out != nullptr && desc->rot_out != nullptr),
+              "emitted volume or matrices missing");
   CCT_REQUIRE(maps != nullptr && workspace != nullptr, "maps and workspace are required");
   CCT_REQUIRE(workspace_bytes >= need, "workspace smaller than one angle pass (cct_maps_workspace_size)");
   CCT_REQUIRE(desc->n_angles <= 65535 && desc->n_slices <= 65535, "too many angles or slices");

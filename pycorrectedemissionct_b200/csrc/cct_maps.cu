@@ -33,11 +33,14 @@ namespace cct {
 
 struct MapsPass {
   int n, P, e, n_det, n_sub, has_in, has_out, maps_dtype, n_angles;
-  int a0, na;                 // entries of this pass (angles, or (angle, partner) pairs)
+  int a0, na;                 // first entry (first quad with quads) and scanned entries of this pass
+  int n_entries;              // entries of `pairs` (angles without)
   int jobs_per_angle;         // has_in + has_out * n_det * n_sub
   const double* rot_in;       // [A][2][6]
   const double* rot_out;      // [A][D][n_sub][2][6]
   const int* pairs;           // [entries][2] (angle, partner) or NULL
+  const int* quads;           // [quads][6] (entry, entry', emitted source of the 4 angles) or NULL
+  float emitted_scale;        // quads: mu_out = emitted_scale * mu_in
   const float* mu_in;         // [S][n][n]
   const float* mu_out;
   float* work;                // [S][na][jobs_per_angle][P][P]
@@ -45,8 +48,19 @@ struct MapsPass {
   void* maps;                 // [S][A][D][n][n]
 };
 
+// Entry scanned in slot ai of the pass: with quads, slots 2q and 2q + 1 are quad (a0 + q)'s two
+// entries (a0 counts quads); otherwise slot ai is entry a0 + ai.
+__device__ __forceinline__ int slot_entry(const MapsPass& p, int ai) {
+  if (p.quads == nullptr) return p.a0 + ai;
+  return p.quads[6 * (p.a0 + (ai >> 1)) + (ai & 1)];
+}
+
 // Angle of entry e and its half-turn partner (-1: none); a = -1 for an out-of-range entry.
 __device__ __forceinline__ void entry_angles(const MapsPass& p, int e, int* a, int* b) {
+  if (e < 0 || e >= p.n_entries) {
+    *a = *b = -1;
+    return;
+  }
   if (p.pairs == nullptr) {
     *a = e;
     *b = -1;
@@ -212,7 +226,7 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
   const int ai = job_lin / p.jobs_per_angle;
   const int job = job_lin - ai * p.jobs_per_angle;
   int a, b;
-  entry_angles(p, p.a0 + ai, &a, &b);
+  entry_angles(p, slot_entry(p, ai), &a, &b);
   if (a < 0) return;  // the whole CTA
   const double* Md = job_matrix(p, a, job, 0);  // rotate(-phi)
   const bool incident = p.has_in && job == 0;
@@ -443,6 +457,84 @@ __global__ void __launch_bounds__(256, PAIRS ? 5 : 1) maps_resample_kernel(MapsP
   }
 }
 
+// Quarter-turn quads (one point detector whose emitted direction is the incident direction of
+// another angle of the set, mu_out = emitted_scale * mu_in): the pass scanned only incident
+// fields, two per quad (slots 2q, 2q + 1), each a half-turn pair of angles.  At every pixel the two
+// pair samples give the incident line integrals L[0..3] of the quad's four angles (entry e's angle
+// and partner, entry e''s angle and partner); the map of angle k is
+// exp(-L[k]) * exp(-emitted_scale * L[src[k]]), src[k] naming which of the four angles the
+// emitted direction of angle k is (its rotation angle differs from the reference's emitted angle
+// only by the float32 rounding of the angles, like a half-turn partner's).  Four maps from two
+// gathers per pixel, where the per-pair resample needs two gathers for two maps.
+__global__ void __launch_bounds__(256, 5) maps_resample_quad_kernel(MapsPass p) {
+  __shared__ float qm[2][6];  // rotate(+phi) matrices of the two entries' angles
+  __shared__ int qa[4];       // the four angles
+  __shared__ int qs[4];       // emitted sources
+  const int n = p.n, P = p.P;
+  const int qi = blockIdx.y;
+  const int s = blockIdx.z;
+  const int* row = p.quads + 6 * (p.a0 + qi);
+  if (threadIdx.x < 2) {
+    int a, b;
+    entry_angles(p, slot_entry(p, 2 * qi + threadIdx.x), &a, &b);
+    qa[2 * threadIdx.x] = a;
+    qa[2 * threadIdx.x + 1] = b;
+  }
+  if (threadIdx.x >= 32 && threadIdx.x < 36) qs[threadIdx.x - 32] = row[2 + threadIdx.x - 32];
+  __syncthreads();
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) ok = ok && qa[k] >= 0 && qs[k] >= 0 && qs[k] < 4;
+  if (!ok) return;  // the whole CTA (only complete quads are valid)
+  if (threadIdx.x < 12) {
+    const int w = threadIdx.x / 6;
+    qm[w][threadIdx.x - 6 * w] = (float)job_matrix(p, qa[2 * w], 0, 1)[threadIdx.x - 6 * w];
+  }
+  __syncthreads();
+  const int tiles_x = (n + RS_TILE - 1) / RS_TILE;
+  const int ty = blockIdx.x / tiles_x, tx = blockIdx.x - ty * tiles_x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = tx * RS_TILE + (warp & 3) * 8 + (lane & 7);
+  const int i0 = ty * RS_TILE + (warp >> 2) * 4 + (lane >> 3);
+  if (j >= n || i0 >= n) return;
+  const float X = (float)(j + p.e);
+  const int64_t n2 = (int64_t)n * n;
+  const float sc = p.emitted_scale;
+  float L[4][RS_PIX];
+#pragma unroll
+  for (int w = 0; w < 2; ++w) {
+    const float* m = qm[w];
+    const int slot = 2 * qi + w;
+    const float* wf = p.work + ((int64_t)s * p.na + slot) * (int64_t)P * P;
+    const float* kc = p.kcol + ((int64_t)s * p.na + slot) * (int64_t)P;
+#pragma unroll
+    for (int k = 0; k < RS_PIX; ++k) {
+      const float Y = (float)(i0 + 8 * k + p.e);
+      const float x = fmaf(m[1], Y, fmaf(m[0], X, m[2]));
+      const float y = fmaf(m[4], Y, fmaf(m[3], X, m[5]));
+      bilin_square_pair(wf, kc, P, x, y, &L[2 * w][k], &L[2 * w + 1][k]);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int src = qs[q];
+    const int64_t plane = (int64_t)s * p.n_angles + qa[q];  // n_det == 1
+#pragma unroll
+    for (int k = 0; k < RS_PIX; ++k) {
+      const int i = i0 + 8 * k;
+      if (i >= n) break;
+      const float le = src == 0 ? L[0][k] : (src == 1 ? L[1][k] : (src == 2 ? L[2][k] : L[3][k]));
+      const float v = __expf(-L[q][k]) * __expf(-sc * le);
+      const int64_t off = plane * n2 + (int64_t)i * n + j;
+      if (p.maps_dtype == CCT_DTYPE_BF16) {
+        reinterpret_cast<__nv_bfloat16*>(p.maps)[off] = __float2bfloat16_rn(v);
+      } else {
+        reinterpret_cast<float*>(p.maps)[off] = v;
+      }
+    }
+  }
+}
+
 int padded_edge(int n) {
   // edges = ceil((ceil(sqrt(2 n^2)) - n) / 2)  (corrct: src/corrct/_projector_backends.py:75-77)
   const double min_size = ceil(sqrt(2.0 * (double)n * (double)n));
@@ -456,6 +548,35 @@ int64_t maps_bytes_per_angle(const cct_maps_desc* d) {
   return jobs * (P * P + P) * (int64_t)sizeof(float) * d->n_slices;  // W planes + partner constants
 }
 
+// Quarter-turn quads: per pass, the incident fields of 2 entries per quad (one job each, so a quad
+// takes the workspace of one entry with incident and emitted jobs), then one quad resample.
+static int launch_maps_quads(const cct_maps_desc* d, const float* mu_in, void* maps, void* work, size_t work_bytes,
+                             cudaStream_t st) {
+  const int e = padded_edge(d->n);
+  const int P = d->n + 2 * e;
+  const int64_t per_quad = 2 * ((int64_t)P * P + P) * (int64_t)sizeof(float) * d->n_slices;
+  int per_pass = (int)std::min<int64_t>((int64_t)work_bytes / per_quad, (int64_t)d->n_quads);
+  if (per_pass < 1) return CCT_ERR_VALUE;
+  per_pass = std::min(per_pass, 65535 / 2);
+  MapsPass p;
+  p.n = d->n; p.P = P; p.e = e; p.n_det = 1; p.n_sub = 1;
+  p.has_in = 1; p.has_out = 0; p.maps_dtype = d->maps_dtype; p.n_angles = d->n_angles;
+  p.jobs_per_angle = 1;
+  p.rot_in = d->rot_in; p.rot_out = d->rot_out; p.pairs = d->pairs; p.mu_in = mu_in; p.mu_out = nullptr;
+  p.quads = d->quads; p.emitted_scale = d->emitted_scale; p.n_entries = d->n_entries;
+  p.work = reinterpret_cast<float*>(work); p.maps = maps;
+  p.kcol = p.work + (int64_t)2 * per_pass * (int64_t)P * P * d->n_slices;
+  const int tiles = (d->n + RS_TILE - 1) / RS_TILE;
+  for (int q0 = 0; q0 < d->n_quads; q0 += per_pass) {
+    const int nq = std::min(per_pass, d->n_quads - q0);
+    p.a0 = q0;
+    p.na = 2 * nq;
+    maps_scan_kernel<true><<<dim3((P + 127) / 128, p.na, d->n_slices), 128, 0, st>>>(p);
+    maps_resample_quad_kernel<<<dim3((unsigned)(tiles * tiles), nq, d->n_slices), 256, 0, st>>>(p);
+  }
+  return CCT_OK;
+}
+
 int launch_maps(const cct_maps_desc* d, const float* mu_in, const float* mu_out, void* maps, void* work,
                 size_t work_bytes, cudaStream_t st) {
   const int e = padded_edge(d->n);
@@ -463,6 +584,7 @@ int launch_maps(const cct_maps_desc* d, const float* mu_in, const float* mu_out,
   const int64_t per_angle = maps_bytes_per_angle(d);
   const int entries = d->pairs != nullptr ? d->n_entries : d->n_angles;
   if (entries < 1 || entries > d->n_angles) return CCT_ERR_VALUE;
+  if (d->quads != nullptr) return launch_maps_quads(d, mu_in, maps, work, work_bytes, st);
   int per_pass = (int)std::min<int64_t>((int64_t)work_bytes / per_angle, (int64_t)entries);
   if (per_pass < 1) return CCT_ERR_VALUE;
   // the scan grid's y dimension is entries x jobs (at most 65535): small slices with a large
@@ -475,6 +597,7 @@ int launch_maps(const cct_maps_desc* d, const float* mu_in, const float* mu_out,
   p.has_in = d->has_in; p.has_out = d->has_out; p.maps_dtype = d->maps_dtype; p.n_angles = d->n_angles;
   p.jobs_per_angle = (d->has_in ? 1 : 0) + (d->has_out ? d->n_det * d->n_sub : 0);
   p.rot_in = d->rot_in; p.rot_out = d->rot_out; p.pairs = d->pairs; p.mu_in = mu_in; p.mu_out = mu_out;
+  p.quads = nullptr; p.emitted_scale = 0.f; p.n_entries = entries;
   p.work = reinterpret_cast<float*>(work); p.maps = maps;
   p.kcol = p.work + (int64_t)per_pass * p.jobs_per_angle * (int64_t)P * P * d->n_slices;
   for (int a0 = 0; a0 < entries; a0 += per_pass) {

@@ -68,6 +68,7 @@ extern "C" int cct_compute_maps_noalloc(const cct_maps_desc* desc, const float* 
   CCT_REQUIRE(desc->maps_dtype == CCT_DTYPE_F32 || desc->maps_dtype == CCT_DTYPE_BF16,
               "maps_dtype must be F32 or BF16");
   CCT_REQUIRE(!desc->has_in || (mu_in != nullptr && desc->rot_in != nullptr), "incident volume or matrices missing");
+  CCT_REQUIRE(desc->quads == nullptr, "cct_compute_maps_noalloc computes every direction on its own (quads = NULL)");
   CCT_REQUIRE(!desc->has_out || (mu_out != nullptr && desc->rot_out != nullptr), "emitted volume or matrices missing");
   CCT_REQUIRE(maps != nullptr, "maps is required");
   CCT_REQUIRE(desc->n_angles <= 65535 && desc->n_slices <= 65535, "too many angles or slices");

@@ -206,3 +206,54 @@ def half_turn_pairs(angles_rot_rad32: NDArray, tol: float = 1e-6) -> NDArray | N
     if all(p < 0 for _, p in entries):
         return None
     return np.array(entries, dtype=np.int32)
+
+
+def quarter_turn_quads(angles_rot_rad32: NDArray, pairs: NDArray | None, det_angle: float,
+                       tol: float = 1e-6) -> NDArray | None:
+    """(n_quads, 6) int32 quads of half-turn pair entries, or None when the angle set does not allow
+    them.
+
+    The emitted direction of angle a is a + det_angle + pi (``attenuation.py:108-120`` with the
+    ``invert`` half turn of ``_projector_backends.py:79-80``).  When it is, within ``tol`` radians,
+    the incident direction of another angle of the set, the emitted line integral of a is the
+    incident one of that angle (times mu_out / mu_in).  For a detector at +-pi / 2 this closes over
+    four angles, two half-turn pairs (e, e'): each row is (e, e', s0, s1, s2, s3) with the quad's
+    angles k = (e's angle, e's partner, e''s angle, e''s partner) and s_k the index (0..3) of the one
+    whose incident direction is angle k's emitted direction.  Every entry must have a partner and
+    every entry must land in one quad; otherwise None.
+    """
+    if pairs is None or len(pairs) % 2 or (pairs[:, 1] < 0).any():
+        return None
+    a = np.mod(np.array(angles_rot_rad32, ndmin=1, dtype=np.float32).astype(np.float64), 2 * np.pi)
+    entry_of = np.full(len(a), -1, dtype=np.int64)
+    entry_of[pairs[:, 0]] = np.arange(len(pairs))
+    entry_of[pairs[:, 1]] = np.arange(len(pairs))
+    order = np.argsort(a, kind="stable")
+    srt = a[order]
+
+    def emitted(i: int) -> int:
+        t = np.mod(a[i] + det_angle + np.pi, 2 * np.pi)
+        for target in (t, t - 2 * np.pi, t + 2 * np.pi):
+            k = int(np.searchsorted(srt, target - tol))
+            if k < len(srt) and abs(srt[k] - target) <= tol:
+                return int(order[k])
+        return -1
+
+    rows, used = [], np.zeros(len(pairs), dtype=bool)
+    for e in range(len(pairs)):
+        if used[e]:
+            continue
+        e2 = entry_of[emitted(int(pairs[e, 0]))] if emitted(int(pairs[e, 0])) >= 0 else -1
+        if e2 < 0 or e2 == e or used[e2]:
+            return None
+        quad = [int(pairs[e, 0]), int(pairs[e, 1]), int(pairs[e2, 0]), int(pairs[e2, 1])]
+        src = []
+        for k in quad:
+            m = emitted(k)
+            if m not in quad:
+                return None
+            src.append(quad.index(m))
+        used[e] = used[e2] = True
+        rows.append([e, int(e2)] + src)
+    return np.array(rows, dtype=np.int32)
+

@@ -146,6 +146,42 @@ def test_half_turn_pairs_match_single_angles(n, maps_dtype, cuda):
     assert rel_l2(got, want) < tol
 
 
+@pytest.mark.parametrize("n,n_ang,scale,maps_dtype", [(72, 40, 1.0, "float32"), (45, 48, 0.7, "float32"),
+                                                      (72, 40, 0.7, "bfloat16")])
+def test_quarter_turn_quads_match_every_direction(n, n_ang, scale, maps_dtype, cuda):
+    """Maps from quarter-turn quads (incident fields only; each emitted line integral is
+    mu_out / mu_in times the incident one of the angle a quarter turn on) against every direction
+    scanned on its own, within the float32 rounding of the angles; with a permuted angle order."""
+    from pycorrectedemissionct_b200 import core, geometry, phantoms
+
+    rad32 = np.array(phantoms.angles(n_ang), dtype=np.float32)[np.random.default_rng(5).permutation(n_ang)]
+    assert geometry.quarter_turn_quads(rad32, geometry.half_turn_pairs(rad32), np.pi / 2) is not None
+    mus = np.stack([phantoms.disk_attenuation(n, phantoms.slice_rng(78, k), 0.04) for k in range(2)])
+    mu = torch.from_numpy(mus).to(cuda)
+    quads = core.compute_maps(mu, scale * mu, rad32, maps_dtype=maps_dtype, emitted_scale=scale)
+    every = core.compute_maps(mu, scale * mu, rad32, maps_dtype=maps_dtype)
+    tol = 4e-3 if maps_dtype == "bfloat16" else 2e-6
+    assert rel_l2(quads.double().cpu().numpy(), every.double().cpu().numpy()) < tol
+    # mu_out given as mu_in itself: quads with scale 1
+    assert torch.equal(core.compute_maps(mu, mu, rad32, maps_dtype=maps_dtype),
+                       core.compute_maps(mu, mu.clone(), rad32, maps_dtype=maps_dtype, emitted_scale=1.0))
+
+
+@pytest.mark.parametrize("case", ["n32_a16", "n64_a48", "n32_a16_psf"])
+def test_quarter_turn_maps_match_reference(golden_cases, case, cuda):
+    """The golden cases' emitted attenuation is 0.7 times the incident one: quad maps against the
+    reference's own FP64 maps."""
+    from pycorrectedemissionct_b200 import core, geometry
+
+    g = golden_cases[case]
+    rad32 = np.array(g["angles"], dtype=np.float32)
+    assert np.allclose(g["mu_out"], 0.7 * g["mu_in"])
+    assert geometry.quarter_turn_quads(rad32, geometry.half_turn_pairs(rad32), float(g["det_angles"][0])) is not None
+    mu_in = _t(g["mu_in"], cuda)[None]
+    maps = core.compute_maps(mu_in, _t(g["mu_out"], cuda)[None], rad32, g["det_angles"], emitted_scale=0.7)
+    assert rel_l2(maps[0].cpu().numpy(), g["maps"]) < TOL
+
+
 def test_masked_solvers_match_reference(golden_cases, cuda):
     """MLEM, SIRT, PDHG and FISTA with b_mask and b_test_mask, and SART with b_mask, through the
     drop-in solvers: reconstruction, residuals and cross-validation residuals against the

@@ -75,6 +75,24 @@ def test_maps_fp_bp_at_benchmark_shape(n, n_full, step, mu_max, cuda):
     assert e < TOL
 
 
+def test_quarter_turn_maps_at_512(cuda):
+    """Maps of the benchmark slice from quarter-turn quads (mu_out = mu_in, detector at pi / 2) on
+    every 10th of 720 angles (a set closed under the quarter turn) against the FP64 port."""
+    from oracle import port
+    from pycorrectedemissionct_b200 import core, phantoms
+
+    n = 512
+    rng = phantoms.slice_rng(20240, 2)
+    phantoms.ellipse_phantom(n, rng, 12)
+    mu = phantoms.disk_attenuation(n, rng, 0.01, dtype=np.float64)
+    rad32, _ = port.backend_angles(phantoms.angles(720)[::10])
+    ref = port.compute_maps(mu, mu, rad32, workers=16)
+    m = _t(mu, cuda)[None]
+    e = rel_l2(core.compute_maps(m, m, rad32)[0].cpu().numpy(), ref)
+    report(f"maps from quarter-turn quads 512x{len(rad32)}/720", e, TOL)
+    assert e < TOL
+
+
 def test_channel_fields_at_1024(cuda):
     """Multi-channel workload: line-integral fields of one 1024 x 1024 slice, channels with emitted
     scales 1 and 3 (mu_out,c = s_c mu_in), on every 60th of 1440 angles: the channel maps

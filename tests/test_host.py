@@ -562,3 +562,30 @@ def test_get_maps_binning_matches_block_means():
     with pytest.raises(NotImplementedError):
         attenuation.bin_maps(maps, 1.5, 2)
 
+
+def test_quarter_turn_quads():
+    """Quads of half-turn pair entries whose emitted directions (angle + detector angle + pi) are
+    incident directions inside the quad: every entry in exactly one quad, and each source index
+    names the angle a quarter turn on (within float32 rounding); None when the set lacks them."""
+    from pycorrectedemissionct_b200 import geometry, phantoms
+
+    for n_ang in (16, 40, 720):
+        rad32 = np.array(phantoms.angles(n_ang), dtype=np.float32)
+        pairs = geometry.half_turn_pairs(rad32)
+        quads = geometry.quarter_turn_quads(rad32, pairs, np.pi / 2)
+        assert quads is not None and quads.shape == (n_ang // 4, 6)
+        entries = np.sort(quads[:, :2].ravel())
+        np.testing.assert_array_equal(entries, np.arange(len(pairs)))
+        for row in quads:
+            ang = [pairs[row[0], 0], pairs[row[0], 1], pairs[row[1], 0], pairs[row[1], 1]]
+            for k in range(4):
+                want = np.mod(np.float64(rad32[ang[k]]) + np.pi / 2 + np.pi, 2 * np.pi)
+                got = np.mod(np.float64(rad32[ang[row[2 + k]]]), 2 * np.pi)
+                d = abs(want - got)
+                assert min(d, 2 * np.pi - d) < 1e-6
+    rad32 = np.array(phantoms.angles(90), dtype=np.float32)   # 270 degrees is not in the set
+    assert geometry.quarter_turn_quads(rad32, geometry.half_turn_pairs(rad32), np.pi / 2) is None
+    rad32 = np.array(phantoms.angles(40), dtype=np.float32)
+    assert geometry.quarter_turn_quads(rad32, geometry.half_turn_pairs(rad32), np.pi / 3) is None
+    assert geometry.quarter_turn_quads(rad32, None, np.pi / 2) is None
+
