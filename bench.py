@@ -44,6 +44,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "converged slices/s, XRF MLEM 512²x720 to fixed residual: plain vs warm start"
 UNIT = "slices/s"
+# fp variants (cct_xrf_desc.variant): the label, the kernel and the DRAM bytes per slice of one
+# ncu capture at 512^2 x 720 FP32 maps (read + write)
+FP_VARIANT_NAMES = {0: "ldg", 1: "tma", 2: "slices2"}
+FP_KERNEL_NAMES = {0: "fp_kernel", 1: "fp_tma_kernel", 2: "fp_pair_kernel"}
+FP_TRAFFIC_PER_SLICE = {0: 1.4749e9 / 2, 1: 1.4616e9 / 2, 2: 2.8297e9 / 4}
 WEIGHTS = os.path.join(ROOT, "pycorrectedemissionct_b200", "weights", "warmstart.pt")
 
 
@@ -67,9 +72,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra-legs", action="store_true",
                     help="skip the drop-in e2e, BF16-maps and FP64-error legs")
+    ap.add_argument("--no-learned-leg", action="store_true", help="skip the learned warm-start leg")
     ap.add_argument("--fp64-angle-step", type=int, default=24,
                     help="FP64 oracle check of the headline slice on every k-th angle")
-    ap.add_argument("--fp-variant", default="auto", choices=["auto", "ldg", "tma"],
+    ap.add_argument("--fp-variant", default="auto", choices=["auto", "ldg", "tma", "slices2"],
                     help="fp staging variant: the autotuner's choice (auto) or a fixed one")
     ap.add_argument("--workload", default="batch", choices=["batch", "ragged", "waves", "channels"],
                     help="batch: the 512x720 benchmark (default); ragged: the mixed-size stream; waves: "
@@ -268,7 +274,8 @@ def run_ours(a):
     if a.fp_variant == "auto":
         variant = autotune.tune(c, x_true, maps)
     else:
-        variant = 0 if a.fp_variant == "ldg" else core._lib.CCT_VARIANT_FP_TMA
+        variant = {"ldg": 0, "tma": core._lib.CCT_VARIANT_FP_TMA, "slices2": core._lib.CCT_VARIANT_FP_SLICES2}[
+            a.fp_variant]
         c.variant = variant
     c_os.variant = variant
     clean = c.fp(x_true, maps)
@@ -409,7 +416,7 @@ def run_ours(a):
     if rank == 0 and not a.no_extra_legs:
         extra = extra_legs(a, dev, c, maps, mus_h, xs_h, b, tol_np, max_iters, variant)
     learned_leg = None
-    if os.path.exists(WEIGHTS):
+    if os.path.exists(WEIGHTS) and not a.no_learned_leg:
         learned_leg = run_learned_leg(a, dev, rank, world, maps, ws, variant, schedule)
 
     # ---- roofline of the dominant kernel (attenuated fp with the fused MLEM epilogue, plain path)
@@ -440,16 +447,16 @@ def run_ours(a):
             "parallelism": f"slices sharded over {world} GPU(s), no collective on the data path",
             "l2": "inputs larger than L2 (maps %.0f MB per slice)" % (a.angles * n * n * map_bytes / 1e6),
             "mean_iterations": head_its, "converged_slices_last_step": converged,
-            "fp_variant": "tma" if variant else "ldg",
+            "fp_variant": FP_VARIANT_NAMES[variant],
         },
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            # DRAM read + write bytes per launch from one ncu capture of each variant on 2 slices
-            # (fp_tma_kernel 1.4616 GB, fp_kernel 1.4749 GB), scaled by the slices per launch;
-            # only for the captures' own configuration
-            "traffic": ((1.4616e9 if variant else 1.4749e9) / 2 * S)
+            # DRAM read + write bytes per launch from one ncu capture of each variant
+            # (fp_tma_kernel 1.4616 GB and fp_kernel 1.4749 GB on 2 slices, fp_pair_kernel 2.8297 GB on
+            # 4 slices), scaled by the slices per launch; only for the captures' own configuration
+            "traffic": (FP_TRAFFIC_PER_SLICE[variant] * S)
             if (n == 512 and a.angles == 720 and a.maps_dtype == "float32") else None,
-            "kernel": ("fp_tma_kernel" if variant else "fp_kernel") + "<MLEM> (attenuated fp + ratio + KL residual)",
+            "kernel": FP_KERNEL_NAMES[variant] + "<MLEM> (attenuated fp + ratio + KL residual)",
             "peak_source": peak_src, "fp_launch_us": fp_avg_s * 1e6, "bp_launch_us": bp_avg_s * 1e6,
             "algorithmic_bytes_per_launch": fp_bytes,
         },

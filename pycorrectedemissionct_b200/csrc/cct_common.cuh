@@ -96,6 +96,34 @@ __device__ __forceinline__ FloorSplit floor_split(float x) {
   return r;
 }
 
+// Two bilinear samples of a staged box z (row stride STRIDE, zoff moving the origin) at the
+// positions (x.x, y.x) and (x.y, y.y), added to acc in that order, in packed FP32x2 arithmetic.
+// Every lane of every packed operation rounds like the scalar sequence
+//   (fx, fy) = floor_split(x), floor_split(y)
+//   top = fmaf(fx.f, t1 - t0, t0); bot = fmaf(fx.f, b1 - b0, b0); acc += fmaf(fy.f, bot - top, top)
+// (a - b is formed as fma(b, -1, a), which rounds the exact difference once), so the result is
+// bit-identical to it.
+template <int STRIDE>
+__device__ __forceinline__ float bilerp2(const float* z, int zoff, float2 x, float2 y, float acc) {
+  const float2 magic = make_float2(12582912.0f, 12582912.0f);  // 1.5 * 2^23, see floor_split
+  const float2 nmagic = make_float2(-12582912.0f, -12582912.0f);
+  const float2 neg1 = make_float2(-1.f, -1.f);
+  const float2 tx = __fadd2_rd(x, magic), ty = __fadd2_rd(y, magic);
+  const float2 fx = __ffma2_rn(__fadd2_rn(tx, nmagic), neg1, x);  // x - floor(x), exact
+  const float2 fy = __ffma2_rn(__fadd2_rn(ty, nmagic), neg1, y);
+  const int q0 = (__float_as_int(ty.x) - 0x4B400000) * STRIDE + (__float_as_int(tx.x) - 0x4B400000) + zoff;
+  const int q1 = (__float_as_int(ty.y) - 0x4B400000) * STRIDE + (__float_as_int(tx.y) - 0x4B400000) + zoff;
+  const float2 t0 = make_float2(z[q0], z[q1]), t1 = make_float2(z[q0 + 1], z[q1 + 1]);
+  const float2 b0 = make_float2(z[q0 + STRIDE], z[q1 + STRIDE]);
+  const float2 b1 = make_float2(z[q0 + STRIDE + 1], z[q1 + STRIDE + 1]);
+  const float2 top = __ffma2_rn(fx, __ffma2_rn(t0, neg1, t1), t0);
+  const float2 bot = __ffma2_rn(fx, __ffma2_rn(b0, neg1, b1), b0);
+  const float2 res = __ffma2_rn(fy, __ffma2_rn(top, neg1, bot), top);
+  acc += res.x;
+  acc += res.y;
+  return acc;
+}
+
 __device__ __forceinline__ double warp_sum_double(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

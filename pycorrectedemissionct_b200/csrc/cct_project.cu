@@ -267,16 +267,16 @@ __device__ __forceinline__ void fp_cta(const FpArgs& args, const int band, const
       const int rem = r_last - r0 - lr;                      // rows of this thread left in the chunk
       const int kmax = rem >= 0 ? rem / FP_LR + 1 : 0;       // samples of this thread in the chunk
       if (kmax >= FP_RPT) {
+        // two samples (rows r and r + FP_LR) per packed FP32x2 instruction, with the roundings
+        // of the scalar loop below
+        const float2 mx = make_float2(m01, m01), my = make_float2(m11, m11);
+        const float2 cx = make_float2(pxc, pxc), cy = make_float2(pyc, pyc);
+        const float2 step2 = make_float2(2.f * FP_LR, 2.f * FP_LR);
+        float2 fr2 = make_float2(fr, fr + (float)FP_LR);
 #pragma unroll 4
-        for (int k = 0; k < FP_RPT; ++k) {
-          const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
-          const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
-          const int q = fy.i * FP_STRIDE + fx.i + zoff;
-          const float t0 = z[q], t1 = z[q + 1], b0 = z[q + FP_STRIDE], b1 = z[q + FP_STRIDE + 1];
-          const float top = fmaf(fx.f, t1 - t0, t0);
-          const float bot = fmaf(fx.f, b1 - b0, b0);
-          acc += fmaf(fy.f, bot - top, top);
-          fr += (float)FP_LR;
+        for (int k = 0; k < FP_RPT; k += 2) {
+          acc = bilerp2<FP_STRIDE>(z, zoff, __ffma2_rn(mx, fr2, cx), __ffma2_rn(my, fr2, cy), acc);
+          fr2 = __fadd2_rn(fr2, step2);
         }
       } else {
         for (int k = 0; k < kmax; ++k) {
@@ -514,16 +514,14 @@ __global__ void __launch_bounds__(FP_THREADS, 2)
       const int rem = r_last - r0 - lr;
       const int kmax = rem >= 0 ? rem / FP_LR + 1 : 0;
       if (kmax >= FP_RPT) {
+        const float2 mx = make_float2(m01, m01), my = make_float2(m11, m11);
+        const float2 cx = make_float2(pxc, pxc), cy = make_float2(pyc, pyc);
+        const float2 step2 = make_float2(2.f * FP_LR, 2.f * FP_LR);
+        float2 fr2 = make_float2(fr, fr + (float)FP_LR);
 #pragma unroll 4
-        for (int k = 0; k < FP_RPT; ++k) {
-          const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
-          const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
-          const int q = fy.i * FPT_BOX_W + fx.i + zoff;
-          const float t0 = zb[q], t1 = zb[q + 1], b0 = zb[q + FPT_BOX_W], b1 = zb[q + FPT_BOX_W + 1];
-          const float top = fmaf(fx.f, t1 - t0, t0);
-          const float bot = fmaf(fx.f, b1 - b0, b0);
-          acc += fmaf(fy.f, bot - top, top);
-          fr += (float)FP_LR;
+        for (int k = 0; k < FP_RPT; k += 2) {
+          acc = bilerp2<FPT_BOX_W>(zb, zoff, __ffma2_rn(mx, fr2, cx), __ffma2_rn(my, fr2, cy), acc);
+          fr2 = __fadd2_rn(fr2, step2);
         }
       } else {
         for (int k = 0; k < kmax; ++k) {
@@ -736,18 +734,24 @@ __global__ void __launch_bounds__(FP_THREADS, 4) fp_pair_kernel(FpArgs args) {
       const int rem = r_last - r0 - lr;
       const int kmax = rem >= 0 ? rem / FP_LR + 1 : 0;
       if (kmax >= FP2_RPT) {
+        // both slices' lerps in packed FP32x2 arithmetic, rounding like the scalar loop below
+        // (a - b as fma(b, -1, a))
+        const float2 neg1 = make_float2(-1.f, -1.f);
+        float2 acc2 = make_float2(acc0, acc1);
 #pragma unroll 4
         for (int k = 0; k < FP2_RPT; ++k) {
           const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));
           const FloorSplit fy = floor_split(fmaf(m11, fr, pyc));
           const int q = fy.i * S + fx.i + zoff;
           const float2 t0 = z2[q], t1 = z2[q + 1], b0 = z2[q + S], b1 = z2[q + S + 1];
-          const float top0 = fmaf(fx.f, t1.x - t0.x, t0.x), bot0 = fmaf(fx.f, b1.x - b0.x, b0.x);
-          const float top1 = fmaf(fx.f, t1.y - t0.y, t0.y), bot1 = fmaf(fx.f, b1.y - b0.y, b0.y);
-          acc0 += fmaf(fy.f, bot0 - top0, top0);
-          acc1 += fmaf(fy.f, bot1 - top1, top1);
+          const float2 fxx = make_float2(fx.f, fx.f), fyy = make_float2(fy.f, fy.f);
+          const float2 top = __ffma2_rn(fxx, __ffma2_rn(t0, neg1, t1), t0);
+          const float2 bot = __ffma2_rn(fxx, __ffma2_rn(b0, neg1, b1), b0);
+          acc2 = __fadd2_rn(acc2, __ffma2_rn(fyy, __ffma2_rn(top, neg1, bot), top));
           fr += (float)FP_LR;
         }
+        acc0 = acc2.x;
+        acc1 = acc2.y;
       } else {
         for (int k = 0; k < kmax; ++k) {
           const FloorSplit fx = floor_split(fmaf(m01, fr, pxc));

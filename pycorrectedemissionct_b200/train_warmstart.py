@@ -13,7 +13,12 @@ The learned start (``learned_start``): the snapshot pass, the network, then one 
 of the two ordered-subsets levels; plain MLEM then finishes to the data-residual tolerance and
 judges every slice.
 
+The learned start also serves as PDHG's ``x0`` (``evaluate_pdhg``: passes until the PDHG-KL-TV
+iterate is within 1 % of its long-run solution, from zero and from the learned start).
+
 Usage (GPU):  python -m pycorrectedemissionct_b200.train_warmstart --slices 20000 --steps 12000 --out w.pt
+              python -m pycorrectedemissionct_b200.train_warmstart --weights w.pt --eval-slices 256 \
+                  --eval-pdhg-slices 64
 """
 
 from __future__ import annotations
@@ -240,6 +245,53 @@ def evaluate(net: WarmStartNet, n: int, n_angles: int, n_slices: int, seed: int,
             "reached_residual": ok}
 
 
+def pdhg_iterations_to(c: core.XrfCore, maps: torch.Tensor, b: torch.Tensor, x_target: torch.Tensor, rel: float,
+                       x0: torch.Tensor | None = None, max_iterations: int = 1000, check_every: int = 5,
+                       tv_lambda: float = 1e-2) -> np.ndarray:
+    """Per slice, the PDHG-KL-TV iterations from ``x0`` (default: the reference's zero start,
+    ``solvers.py:1133-1137``) until the iterate is within ``rel`` (relative L2) of ``x_target``,
+    counted in blocks of ``check_every``; -1 where ``max_iterations`` do not get there."""
+    sv = BatchedSolver(c, maps, b, "pdhg", x0=x0, tv_lambda=tv_lambda)
+    need = np.full(b.shape[0], -1, dtype=np.int64)
+    ref = x_target.flatten(1).norm(dim=1)
+    done = 0
+    while done < max_iterations and (need < 0).any():
+        sv.run(check_every, check_every=check_every, use_graph=False)
+        done += check_every
+        d = ((sv.x - x_target).flatten(1).norm(dim=1) / ref).cpu().numpy()
+        need[(need < 0) & (d <= rel)] = done
+    return need
+
+
+def evaluate_pdhg(net: WarmStartNet, n: int, n_angles: int, n_slices: int, seed: int, batch: int = 16, device=None,
+                  long_iterations: int = 1000, rel: float = 0.01, tv_lambda: float = 1e-2) -> dict:
+    """Held-out evaluation of the learned start as PDHG's ``x0``: per slice, the full-data passes
+    until the PDHG-KL-TV iterate is within ``rel`` (relative L2) of the solution after
+    ``long_iterations`` PDHG iterations from zero, from the reference's zero start and from the
+    learned start (its three ordered-subsets passes counted)."""
+    device = core.require_cuda(device)
+    levels = net.os_levels(n_angles)
+    cold, warm = [], []
+    for s0 in range(0, n_slices, batch):
+        seeds = [seed + k for k in range(s0, min(n_slices, s0 + batch))]
+        c, maps, b, _ = synth_batch(n, n_angles, seeds, 0.02, 1e4, device, subsets=levels)
+        long_run = BatchedSolver(c, maps, b, "pdhg", tv_lambda=tv_lambda)
+        long_run.run(long_iterations, check_every=50)
+        x_target = long_run.x.clone()
+        del long_run
+        cold.append(pdhg_iterations_to(c, maps, b, x_target, rel, None, long_iterations, tv_lambda=tv_lambda))
+        tau = BatchedSolver(c, maps, b, "mlem").tau
+        x0 = learned_start(net, OrderedSubsets(c, maps, b, [(levels[0], 1), (levels[1], 1)]), c, b, tau).clone()
+        w = pdhg_iterations_to(c, maps, b, x_target, rel, x0, long_iterations, tv_lambda=tv_lambda)
+        warm.append(np.where(w >= 0, w + 3, -1))
+        del maps
+    cold, warm = np.concatenate(cold), np.concatenate(warm)
+    return {"n": n, "angles": n_angles, "slices": int(cold.size), "rel": rel, "long_iterations": long_iterations,
+            "tv_lambda": tv_lambda, "cold_mean": float(cold[cold >= 0].mean()) if (cold >= 0).any() else None,
+            "cold_reached": int((cold >= 0).sum()), "learned_mean": float(warm[warm >= 0].mean()) if (warm >= 0).any()
+            else None, "learned_reached": int((warm >= 0).sum()), "learned_max": int(warm.max())}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--slices", type=int, default=20000)
@@ -256,6 +308,9 @@ def main():
                          "(0: the first 10 MLEM iterates)")
     ap.add_argument("--finish-factor", type=int, default=5)
     ap.add_argument("--eval-slices", type=int, default=0, help="held-out slices per evaluation shape")
+    ap.add_argument("--eval-pdhg-slices", type=int, default=0,
+                    help="held-out slices for the PDHG-KL-TV warm-start evaluation (at --n x --angles)")
+    ap.add_argument("--weights", default=None, help="evaluate these weights instead of training")
     ap.add_argument("--out", default="warmstart.pt")
     a = ap.parse_args()
     dev = core.require_cuda()
@@ -265,6 +320,10 @@ def main():
     net.log_floor = a.log_floor
     net.pass_angles = a.pass_angles
     net.finish_factor = a.finish_factor
+    if a.weights is not None:
+        net.load(a.weights)
+        evaluate_all(net, a, dev)
+        return
     inputs, targets = generate_pairs(a.slices, a.n, a.angles, target_iterations=a.target_iterations, device=dev,
                                      net=net, batch=128)
     torch.cuda.synchronize()
@@ -280,12 +339,19 @@ def main():
     net.save(a.out)
     del inputs, targets
     torch.cuda.empty_cache()
-    if a.eval_slices > 0:
-        import json
+    evaluate_all(net, a, dev)
 
+
+def evaluate_all(net: WarmStartNet, a, dev) -> None:
+    import json
+
+    if a.eval_slices > 0:
         for n, n_ang in ((a.n, a.angles), (2 * a.n, 2 * a.angles)):
             r = evaluate(net, n, n_ang, a.eval_slices, seed=900_000 + n, device=dev)
             print("eval", json.dumps(r), flush=True)
+    if a.eval_pdhg_slices > 0:
+        r = evaluate_pdhg(net, a.n, a.angles, a.eval_pdhg_slices, seed=950_000, device=dev)
+        print("eval_pdhg", json.dumps(r), flush=True)
 
 
 if __name__ == "__main__":
