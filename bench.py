@@ -632,6 +632,8 @@ def fp64_errors(a, c, maps, mu0, x0, dev) -> dict:
         "sample": f"slice 0 of the batch, {len(idx)} of {c.n_angles} angles (every {step}th), FP64 oracle port "
                   f"({time.perf_counter() - t0:.1f} s on {workers} host threads)",
         "bound": 1e-5,
+        # kept for the BF16 leg (removed before printing)
+        "_ref": (idx, ref_maps, ref_fp, sub, xs),
     }
     return out
 
@@ -641,7 +643,7 @@ def extra_legs(a, dev, c, maps, mus_h, xs_h, b, tol_np, max_iters, variant) -> d
     errors of the headline slice, and plain MLEM with BF16-stored maps."""
     import torch
 
-    from pycorrectedemissionct_b200 import core, engine, projectors, solvers
+    from pycorrectedemissionct_b200 import autotune, core, engine, projectors, solvers
 
     out = {}
     n, S = a.n, a.slices
@@ -681,7 +683,19 @@ def extra_legs(a, dev, c, maps, mus_h, xs_h, b, tol_np, max_iters, variant) -> d
     torch.cuda.synchronize(dev)
     e16 = float(((m16[0].float() - maps[0].float()).double().norm() / maps[0].double().norm()).item())
     c16 = core.XrfCore(n, angles, device=dev)
-    c16.variant = variant
+    bf16_variant = autotune.tune(c16, torch.from_numpy(xs_h).to(dev), m16)
+    bf16_fp64 = {}
+    ref = out.get("fp64_error", {}).pop("_ref", None)
+    if ref is not None:
+        idx, ref_maps, ref_fp, sub, xs = ref
+        m16_sub = m16[0:1, torch.from_numpy(idx).to(dev)].contiguous()
+        bf16_fp64 = {
+            "maps_rel_l2_vs_fp64": float(np.linalg.norm(m16_sub[0].float().cpu().numpy() - ref_maps)
+                                         / np.linalg.norm(ref_maps)),
+            "maps_then_fp_rel_l2_vs_fp64": float(np.linalg.norm(sub.fp(xs, m16_sub)[0, 0].cpu().numpy() - ref_fp)
+                                                 / np.linalg.norm(ref_fp)),
+        }
+        del m16_sub
     sv = engine.BatchedSolver(c16, m16, b, "mlem")
     sv.step()
     fps, bps = [], []
@@ -703,10 +717,10 @@ def extra_legs(a, dev, c, maps, mus_h, xs_h, b, tol_np, max_iters, variant) -> d
     out["bf16_maps"] = {
         "plain_mlem_slices_per_s": S / secs, "iterations": a.iters,
         "fp_launch_us": 1e3 * float(np.median(fps)), "bp_launch_us": 1e3 * float(np.median(bps)),
-        "maps_rel_l2_vs_fp32": e16,
+        "maps_rel_l2_vs_fp32": e16, **bf16_fp64, "fp_variant": FP_VARIANT_NAMES[bf16_variant],
         "final_residual_over_fp32_target": [float(np.min(res_ratio)), float(np.max(res_ratio))],
-        "note": "maps stored in bfloat16 (8-bit mantissa), FP32 arithmetic; the FP32 maps' own error against "
-                "FP64 is fp64_error.maps",
+        "note": "maps stored in bfloat16 (8-bit mantissa), FP32 arithmetic; errors against the FP64 oracle on the "
+                "fp64_error sample",
     }
     del m16, ws, sv
     return out

@@ -127,6 +127,9 @@ class AttenuationVolume:
             for ii, det in enumerate(self.detectors):
                 sub = geometry.detector_sub_angles(det.surface_mm2, det.distance_mm, self.emitted_sub_sampling)
                 print(f"Detector #{ii}: Super-sampling outgoing sub-angles: {np.round(np.rad2deg(sub), decimals=3)} deg")
+        # equal incident and emitted attenuation (mu_out = 1 * mu_in) lets compute_maps derive the
+        # emitted line integrals from the incident ones where the geometry allows it
+        same = mu_in is not None and mu_out is not None and mu_in.shape == mu_out.shape and torch.equal(mu_in, mu_out)
         self.maps_device = _core.compute_maps(
             mu_in,
             mu_out,
@@ -136,6 +139,7 @@ class AttenuationVolume:
             distances_mm=[d.distance_mm for d in self.detectors],
             sub_sampling=subs,
             maps_dtype=self.maps_dtype,
+            emitted_scale=1.0 if same else None,
         )
         self._maps_host = None
 
