@@ -329,16 +329,23 @@ def run_ours(a):
     phase_ms = []  # (maps, passes, judge) of timed ordered-subsets steps
 
     def step_subsets(timed: bool) -> float:
+        # NVTX ranges name the phases for a profiler (ncu --nvtx --nvtx-include "subset_passes/")
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         ev[0].record()
+        torch.cuda.nvtx.range_push("compute_maps")
         maps_subsets()
+        torch.cuda.nvtx.range_pop()
         ev[1].record()
         launches[0] += 2 * passes + launches_os_pass
+        torch.cuda.nvtx.range_push("subset_passes")
         subsets.reset()
         subsets.run()
+        torch.cuda.nvtx.range_pop()
         ev[2].record()
+        torch.cuda.nvtx.range_push("judge_mlem")
         judge.reset(subsets.x)
         solve_to_tol(judge, False, max_iters, block=2)
+        torch.cuda.nvtx.range_pop()
         ev[3].record()
         if timed:
             phase_ms.append(ev)

@@ -166,7 +166,11 @@ typedef struct cct_maps_desc {
 int cct_maps_workspace_size(const cct_maps_desc* desc, int32_t angles_per_pass, size_t* bytes);
 
 /* Compute maps.  mu_in / mu_out: device [S][n][n] float32 (NULL when absent).  The number of
-   angles per pass is the largest that fits in workspace_bytes.  maps_dtype = CCT_DTYPE_FIELDS_F32
+   angles per pass is the largest that fits in workspace_bytes.  When the workspace also holds
+   transposed copies of mu_in and mu_out (n * n * S floats each, 256-byte rounded) beside at least
+   half of that many entries, their start of the workspace holds those copies, which the column
+   scans read at angles whose columns run closer to y than to x (same results, coalesced loads).
+   maps_dtype = CCT_DTYPE_FIELDS_F32
    writes the line-integral fields [S][A][1 + D][n][n] (L_in, then L_out per detector; zero for an
    absent volume; needs n_sub == 1) instead of maps. */
 int cct_compute_maps(const cct_maps_desc* desc, const float* mu_in, const float* mu_out, void* maps,

@@ -43,6 +43,8 @@ struct MapsPass {
   float emitted_scale;        // quads: mu_out = emitted_scale * mu_in
   const float* mu_in;         // [S][n][n]
   const float* mu_out;
+  const float* mu_in_t;       // [S][n][n] transposed copies (mu_t[s][x][y] = mu[s][y][x]) or NULL
+  const float* mu_out_t;
   float* work;                // [S][na][jobs_per_angle][P][P]
   float* kcol;                // [S][na][jobs_per_angle][P] per-column constants of the partner scans
   void* maps;                 // [S][A][D][n][n]
@@ -103,6 +105,35 @@ __device__ __forceinline__ float bilin_inside(const float* img, int w, int hgt, 
   const int x0 = min(max(fx.i, 0), w - 2), y0 = min(max(fy.i, 0), hgt - 2);
   const float* q = img + (int64_t)y0 * w + x0;
   const float v00 = __ldg(q), v01 = __ldg(q + 1), v10 = __ldg(q + w), v11 = __ldg(q + w + 1);
+  const float top = fmaf(fx.f, v01 - v00, v00);
+  const float bot = fmaf(fx.f, v11 - v10, v10);
+  return fmaf(fy.f, bot - top, top);
+}
+
+// The same two samplers on an n x n image whose element (y, x) sits at y * sy + x * sx: row-major
+// (sy, sx) = (n, 1) or transposed (1, n).  The taps and the arithmetic are those of bilin_zero /
+// bilin_inside, so both layouts give bit-identical samples; the layout only decides which lanes
+// of a warp share memory sectors.
+__device__ __forceinline__ float bilin_zero_mu(const float* img, int n, int sy, int sx, float x, float y) {
+  const FloorSplit fx = floor_split(x), fy = floor_split(y);
+  const int x0 = fx.i, y0 = fy.i;
+  const bool xin0 = x0 >= 0 && x0 < n, xin1 = x0 + 1 >= 0 && x0 + 1 < n;
+  const bool yin0 = y0 >= 0 && y0 < n, yin1 = y0 + 1 >= 0 && y0 + 1 < n;
+  const int64_t q = (int64_t)y0 * sy + (int64_t)x0 * sx;
+  const float v00 = (yin0 && xin0) ? __ldg(img + q) : 0.f;
+  const float v01 = (yin0 && xin1) ? __ldg(img + q + sx) : 0.f;
+  const float v10 = (yin1 && xin0) ? __ldg(img + q + sy) : 0.f;
+  const float v11 = (yin1 && xin1) ? __ldg(img + q + sx + sy) : 0.f;
+  const float top = fmaf(fx.f, v01 - v00, v00);
+  const float bot = fmaf(fx.f, v11 - v10, v10);
+  return fmaf(fy.f, bot - top, top);
+}
+
+__device__ __forceinline__ float bilin_inside_mu(const float* img, int n, int sy, int sx, float x, float y) {
+  const FloorSplit fx = floor_split(x), fy = floor_split(y);
+  const int x0 = min(max(fx.i, 0), n - 2), y0 = min(max(fy.i, 0), n - 2);
+  const float* q = img + (y0 * sy + x0 * sx);  // < n * n
+  const float v00 = __ldg(q), v01 = __ldg(q + sx), v10 = __ldg(q + sy), v11 = __ldg(q + sx + sy);
   const float top = fmaf(fx.f, v01 - v00, v00);
   const float bot = fmaf(fx.f, v11 - v10, v10);
   return fmaf(fy.f, bot - top, top);
@@ -230,7 +261,12 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
   if (a < 0) return;  // the whole CTA
   const double* Md = job_matrix(p, a, job, 0);  // rotate(-phi)
   const bool incident = p.has_in && job == 0;
-  const float* mu = (incident ? p.mu_in : p.mu_out) + (int64_t)s * n * n;
+  // the lanes of a warp step along (m00, m10) in mu: where that is closer to y than to x, the
+  // transposed copy (if given) puts neighbouring lanes in neighbouring memory
+  const float* mu_t = incident ? p.mu_in_t : p.mu_out_t;
+  const bool tr = mu_t != nullptr && fabs(Md[3]) > fabs(Md[0]);
+  const float* mu = (tr ? mu_t : (incident ? p.mu_in : p.mu_out)) + (int64_t)s * n * n;
+  const int sy = tr ? 1 : n, sx = tr ? n : 1;  // element (y, x) of mu at y * sy + x * sx
   // mu coordinates = padded coordinates - e
   const float m00 = (float)Md[0], m01 = (float)Md[1], m02 = (float)(Md[2] - p.e);
   const float m10 = (float)Md[3], m11 = (float)Md[4], m12 = (float)(Md[5] - p.e);
@@ -262,7 +298,7 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
   double wrap = 0.0;
   if (P - 1 >= lo && P - 1 <= hi) {
     const float fr = (float)(P - 1);
-    wrap = 0.5 * (double)bilin_zero(mu, n, n, fmaf(m01, fr, xc), fmaf(m11, fr, yc));
+    wrap = 0.5 * (double)bilin_zero_mu(mu, n, sy, sx, fmaf(m01, fr, xc), fmaf(m11, fr, yc));
   }
   // W[r] = acc + U[r]/2 + wrap with acc = sum_{k<r} U[k] (FP64); U = 0 outside [lo, hi]
   double acc = 0.0;
@@ -272,7 +308,7 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
     if (valid) W[(int64_t)r * P] = w_before;
   for (; r < wilo; ++r) {
     const float fr = (float)r;
-    const float u = (r >= lo && r <= hi) ? bilin_zero(mu, n, n, fmaf(m01, fr, xc), fmaf(m11, fr, yc)) : 0.f;
+    const float u = (r >= lo && r <= hi) ? bilin_zero_mu(mu, n, sy, sx, fmaf(m01, fr, xc), fmaf(m11, fr, yc)) : 0.f;
     if (valid) W[(int64_t)r * P] = (float)(acc + 0.5 * (double)u + wrap);
     acc += (double)u;
   }
@@ -281,7 +317,7 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const float fr = (float)(r + k);
-      u[k] = bilin_inside(mu, n, n, fmaf(m01, fr, xc), fmaf(m11, fr, yc));
+      u[k] = bilin_inside_mu(mu, n, sy, sx, fmaf(m01, fr, xc), fmaf(m11, fr, yc));
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -291,13 +327,13 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
   }
   for (; r <= wihi; ++r) {
     const float fr = (float)r;
-    const float u = bilin_inside(mu, n, n, fmaf(m01, fr, xc), fmaf(m11, fr, yc));
+    const float u = bilin_inside_mu(mu, n, sy, sx, fmaf(m01, fr, xc), fmaf(m11, fr, yc));
     if (valid) W[(int64_t)r * P] = (float)(acc + 0.5 * (double)u + wrap);
     acc += (double)u;
   }
   for (; r <= whi; ++r) {
     const float fr = (float)r;
-    const float u = (r >= lo && r <= hi) ? bilin_zero(mu, n, n, fmaf(m01, fr, xc), fmaf(m11, fr, yc)) : 0.f;
+    const float u = (r >= lo && r <= hi) ? bilin_zero_mu(mu, n, sy, sx, fmaf(m01, fr, xc), fmaf(m11, fr, yc)) : 0.f;
     if (valid) W[(int64_t)r * P] = (float)(acc + 0.5 * (double)u + wrap);
     acc += (double)u;
   }
@@ -309,7 +345,7 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
     // about the centre, and its W at this frame's (r', c') is K[c'] - W[r'][c'] with
     // K = sum_k U[k] + U[0]/2 + U[P-1]/2 (the reverse roll + cumsum of the same column)
     double first = 0.0;
-    if (0 >= lo && 0 <= hi) first = 0.5 * (double)bilin_zero(mu, n, n, xc, yc);
+    if (0 >= lo && 0 <= hi) first = 0.5 * (double)bilin_zero_mu(mu, n, sy, sx, xc, yc);
     p.kcol[(((int64_t)s * p.na + ai) * p.jobs_per_angle + job) * P + cpr] = (float)(acc + first + wrap);
   }
 }
@@ -541,6 +577,49 @@ int padded_edge(int n) {
   return (int)ceil((min_size - n) / 2.0);
 }
 
+// mu_t[s][x][y] = mu[s][y][x] for the scan's transposed reads (32 x 32 tiles through shared
+// memory, coalesced on both sides).
+__global__ void __launch_bounds__(256) maps_transpose_kernel(const float* __restrict__ src, float* __restrict__ dst,
+                                                             int n) {
+  __shared__ float t[32][33];
+  const int64_t off = (int64_t)blockIdx.z * n * n;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int y = y0 + k, x = x0 + threadIdx.x;
+    if (y < n && x < n) t[k][threadIdx.x] = src[off + (int64_t)y * n + x];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int x = x0 + k, y = y0 + threadIdx.x;
+    if (x < n && y < n) dst[off + (int64_t)x * n + y] = t[threadIdx.x][k];
+  }
+}
+
+static size_t transposed_bytes(const cct_maps_desc* d) {
+  const size_t b = (size_t)d->n * d->n * sizeof(float) * d->n_slices;
+  return (b + 255) & ~(size_t)255;
+}
+
+static void launch_transpose(const float* src, float* dst, int n, int slices, cudaStream_t st) {
+  const int t = (n + 31) / 32;
+  maps_transpose_kernel<<<dim3(t, t, slices), dim3(32, 8), 0, st>>>(src, dst, n);
+}
+
+// Entries per pass and whether the workspace also holds `copies` transposed copies of mu at its
+// start: they are used when, after them, at least half the entries of a pass without them fit.
+static int plan_pass(const cct_maps_desc* d, size_t work_bytes, int64_t per_entry, int entries, int copies,
+                     size_t* prefix) {
+  const int64_t plain = std::min<int64_t>((int64_t)work_bytes / per_entry, entries);
+  const size_t tb = (size_t)copies * transposed_bytes(d);
+  const int64_t with_t = work_bytes > tb ? std::min<int64_t>((int64_t)(work_bytes - tb) / per_entry, entries) : 0;
+  if (copies > 0 && with_t >= 1 && 2 * with_t >= plain) {
+    *prefix = tb;
+    return (int)with_t;
+  }
+  *prefix = 0;
+  return (int)plain;
+}
+
 int64_t maps_bytes_per_angle(const cct_maps_desc* d) {
   const int e = padded_edge(d->n);
   const int64_t P = d->n + 2 * e;
@@ -555,10 +634,17 @@ static int launch_maps_quads(const cct_maps_desc* d, const float* mu_in, void* m
   const int e = padded_edge(d->n);
   const int P = d->n + 2 * e;
   const int64_t per_quad = 2 * ((int64_t)P * P + P) * (int64_t)sizeof(float) * d->n_slices;
-  int per_pass = (int)std::min<int64_t>((int64_t)work_bytes / per_quad, (int64_t)d->n_quads);
+  size_t prefix = 0;
+  int per_pass = plan_pass(d, work_bytes, per_quad, d->n_quads, 1, &prefix);
   if (per_pass < 1) return CCT_ERR_VALUE;
   per_pass = std::min(per_pass, 65535 / 2);
   MapsPass p;
+  p.mu_in_t = p.mu_out_t = nullptr;
+  if (prefix > 0) {
+    p.mu_in_t = reinterpret_cast<float*>(work);
+    launch_transpose(mu_in, const_cast<float*>(p.mu_in_t), d->n, d->n_slices, st);
+    work = reinterpret_cast<char*>(work) + prefix;
+  }
   p.n = d->n; p.P = P; p.e = e; p.n_det = 1; p.n_sub = 1;
   p.has_in = 1; p.has_out = 0; p.maps_dtype = d->maps_dtype; p.n_angles = d->n_angles;
   p.jobs_per_angle = 1;
@@ -585,7 +671,11 @@ int launch_maps(const cct_maps_desc* d, const float* mu_in, const float* mu_out,
   const int entries = d->pairs != nullptr ? d->n_entries : d->n_angles;
   if (entries < 1 || entries > d->n_angles) return CCT_ERR_VALUE;
   if (d->quads != nullptr) return launch_maps_quads(d, mu_in, maps, work, work_bytes, st);
-  int per_pass = (int)std::min<int64_t>((int64_t)work_bytes / per_angle, (int64_t)entries);
+  // transposed copies of mu_in and of a distinct mu_out
+  const bool out_own = d->has_out && (!d->has_in || mu_out != mu_in);
+  const int copies = (d->has_in ? 1 : 0) + (out_own ? 1 : 0);
+  size_t prefix = 0;
+  int per_pass = plan_pass(d, work_bytes, per_angle, entries, copies, &prefix);
   if (per_pass < 1) return CCT_ERR_VALUE;
   // the scan grid's y dimension is entries x jobs (at most 65535): small slices with a large
   // workspace take more passes instead
@@ -593,6 +683,23 @@ int launch_maps(const cct_maps_desc* d, const float* mu_in, const float* mu_out,
   per_pass = std::max(1, std::min(per_pass, 65535 / std::max(1, jobs)));
   if ((int64_t)jobs > 65535) return CCT_ERR_VALUE;
   MapsPass p;
+  p.mu_in_t = p.mu_out_t = nullptr;
+  if (prefix > 0) {
+    float* t = reinterpret_cast<float*>(work);
+    const size_t tb = transposed_bytes(d);
+    if (d->has_in) {
+      launch_transpose(mu_in, t, d->n, d->n_slices, st);
+      p.mu_in_t = t;
+      t = reinterpret_cast<float*>(reinterpret_cast<char*>(t) + tb);
+    }
+    if (out_own) {
+      launch_transpose(mu_out, t, d->n, d->n_slices, st);
+      p.mu_out_t = t;
+    } else if (d->has_out) {
+      p.mu_out_t = p.mu_in_t;
+    }
+    work = reinterpret_cast<char*>(work) + prefix;
+  }
   p.n = d->n; p.P = P; p.e = e; p.n_det = d->n_det; p.n_sub = d->n_sub;
   p.has_in = d->has_in; p.has_out = d->has_out; p.maps_dtype = d->maps_dtype; p.n_angles = d->n_angles;
   p.jobs_per_angle = (d->has_in ? 1 : 0) + (d->has_out ? d->n_det * d->n_sub : 0);
