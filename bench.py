@@ -48,7 +48,7 @@ UNIT = "slices/s"
 # ncu capture at 512^2 x 720 FP32 maps (read + write)
 FP_VARIANT_NAMES = {0: "ldg", 1: "tma", 2: "slices2"}
 FP_KERNEL_NAMES = {0: "fp_kernel", 1: "fp_tma_kernel", 2: "fp_pair_kernel"}
-FP_TRAFFIC_PER_SLICE = {0: 1.4749e9 / 2, 1: 1.4616e9 / 2, 2: 2.8297e9 / 4}
+FP_TRAFFIC_PER_SLICE = {0: 2.8680e9 / 4, 1: 2.9200e9 / 4, 2: 2.7911e9 / 4}
 WEIGHTS = os.path.join(ROOT, "pycorrectedemissionct_b200", "weights", "warmstart.pt")
 
 
@@ -84,6 +84,8 @@ def parse():
     ap.add_argument("--field-slices", type=int, default=1, help="channels workload: field slices per wave")
     ap.add_argument("--wave-slices", type=int, default=512)
     ap.add_argument("--ragged-slices", type=int, default=400)
+    ap.add_argument("--ragged-legs", default="subsets,learned,plain",
+                    help="ragged workload: MLEM starts to time (subsets, learned, plain), comma-separated")
     ap.add_argument("--cpu-sample-angles", type=int, default=144)
     return ap.parse_args()
 
@@ -458,9 +460,9 @@ def run_ours(a):
         },
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            # DRAM read + write bytes per launch from one ncu capture of each variant
-            # (fp_tma_kernel 1.4616 GB and fp_kernel 1.4749 GB on 2 slices, fp_pair_kernel 2.8297 GB on
-            # 4 slices), scaled by the slices per launch; only for the captures' own configuration
+            # DRAM read + write bytes per launch from one ncu capture of each variant on 4 slices
+            # (fp_kernel 2.8680 GB, fp_tma_kernel 2.9200 GB, fp_pair_kernel 2.7911 GB), scaled by the
+            # slices per launch; only for the captures' own configuration
             "traffic": (FP_TRAFFIC_PER_SLICE[variant] * S)
             if (n == 512 and a.angles == 720 and a.maps_dtype == "float32") else None,
             "kernel": FP_KERNEL_NAMES[variant] + "<MLEM> (attenuated fp + ratio + KL residual)",
@@ -930,22 +932,35 @@ def run_ragged(a):
         for j in jobs:
             j.x, j.iterations_done, j.finished_s = None, 0, 0.0
 
+    net = None
+    legs = [x.strip() for x in a.ragged_legs.split(",") if x.strip()]
+    if "learned" in legs:
+        if os.path.exists(WEIGHTS):
+            from pycorrectedemissionct_b200.warmstart import WarmStartNet
+
+            net = WarmStartNet(device=dev)
+            net.load(WEIGHTS)
+        else:
+            legs.remove("learned")
     out = {}
-    for name, warm in (("warm", True), ("plain", False)):
+    for name in legs:
+        warm = {"subsets": True, "learned": "learned", "plain": False}[name]
         reset()
-        st = stream.RaggedStream(dev, warm_start=warm)  # schedules follow each slice's angle count
+        st = stream.RaggedStream(dev, warm_start=warm, net=net)  # schedules follow each slice's angle count
         r = st.solve(jobs, max_iterations=2 * a.iters)
         r["launches"] = st.launches
         r["mlem_mean_passes"] = float(np.mean([j.iterations_done for j in mlem]))
         r["converged"] = int(sum(j.extra["residual"] <= j.tolerance for j in mlem))
         r["restarted"] = int(sum(bool(j.extra.get("restarted")) for j in mlem))
         out[name] = r
+    head = "learned" if "learned" in out else legs[0]
     line = {
         "metric": "ragged stream slices/s (mixed sizes and angle counts, half SIRT 150, half MLEM to residual)",
-        "value": out["warm"]["slices_per_s"], "unit": "slices/s", "n_gpus": 1, "higher_is_better": True,
+        "value": out[head]["slices_per_s"], "unit": "slices/s", "n_gpus": 1, "higher_is_better": True,
         "config": {"workload": f"{a.ragged_slices} slices, sides {list(sizes)}, angles U[90, 1440], mu <= 0.02, "
-                               "peaks log-U[1e3, 1e5]", "ragged": "one launch per operator over all groups of a wave"},
-        "p50_s": out["warm"]["p50_s"], "p99_s": out["warm"]["p99_s"], "warm": out["warm"], "plain": out["plain"],
+                               "peaks log-U[1e3, 1e5]", "ragged": "one launch per operator over all groups of a wave",
+                   "headline_start": head},
+        "p50_s": out[head]["p50_s"], "p99_s": out[head]["p99_s"], **out,
         "data": "synthetic", "dtype": "f32",
     }
     print(json.dumps(line), flush=True)

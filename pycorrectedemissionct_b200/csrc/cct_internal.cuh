@@ -155,6 +155,37 @@ __device__ __forceinline__ void bp_epilogue(const BpArgs& a, int s, int i, int j
   a.x[idx] = x;
 }
 
+// The MLEM / SIRT epilogue of K pixels (s, i0 + di * k, j) of one thread: the loads of tau and x
+// are issued before the first store of x, which the per-pixel form cannot do (a store to x
+// may alias the next pixel's loads), so that a back projection of few lines does not wait for K
+// memory round trips in a row.  Same arithmetic as bp_epilogue.
+template <int EPI, int K>
+__device__ __forceinline__ void bp_epilogue_rows(const BpArgs& a, int s, int i0, int di, int j, const float (&v)[K]) {
+  static_assert(EPI == BP_EPI_MLEM || EPI == BP_EPI_SIRT, "MLEM and SIRT epilogues only");
+  const int n = a.n;
+  const int64_t n2 = (int64_t)n * n;
+  const float* tau = a.tau + (a.tau_shared ? 0 : (int64_t)s * n2);
+  float tv[K], xv[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int i = i0 + di * k;
+    const int64_t pix = (int64_t)i * n + j;
+    const bool in = i < n && j < n;
+    tv[k] = in ? tau[pix] : 1.f;
+    xv[k] = in ? a.x[(int64_t)s * n2 + pix] : 0.f;
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int i = i0 + di * k;
+    if (i >= n || j >= n) continue;
+    const int64_t pix = (int64_t)i * n + j;
+    float x = EPI == BP_EPI_MLEM ? xv[k] * (v[k] / tv[k]) : xv[k] + v[k] * tv[k];
+    x = apply_limits(a, x);
+    if (a.x_mask != nullptr) x *= a.x_mask[a.mask_per_slice ? (int64_t)s * n2 + pix : pix];
+    a.x[(int64_t)s * n2 + pix] = x;
+  }
+}
+
 void launch_fp(const FpArgs& a, cudaStream_t st);
 bool fp_vec4_ok(const FpArgs& a);  // may the fp staging use 16-byte loads for these pointers
 // PSF convolution of finished sinogram lines (a.vol = input sinogram) with the fp epilogue EPI

@@ -813,6 +813,7 @@ __device__ __forceinline__ void bp_cta(const BpArgs& args, const int tile, const
   __shared__ float4 linfo[BP_LINES];  // cos, sin, offset (K - kbase), weight
   __shared__ int lkind[BP_LINES];
   __shared__ int lkbase[BP_LINES];
+  __shared__ float2 linner[BP_LINES];  // checked lines: interior range of the FP32 coordinate
 
   const int n = args.n;
   if (args.active != nullptr && args.active[s] == 0) return;
@@ -883,6 +884,10 @@ __device__ __forceinline__ void bp_cta(const BpArgs& args, const int tile, const
         linfo[ll] = make_float4(cs, sn, (float)(K - kbase), w);
         lkind[ll] = kind;
         lkbase[ll] = kbase;
+        // the FP32 coordinate u = t + K - kbase of the accumulate loop is within ~1e-4 of its
+        // exact value: pixels with u inside the detector by more than BP_EDGE_GUARD take the
+        // fast lerp, only the others decide the edge in double precision
+        linner[ll] = make_float2((float)(-kbase) + BP_EDGE_GUARD, (float)(n - 1 - kbase) - BP_EDGE_GUARD);
       }
     }
     __syncthreads();
@@ -910,13 +915,15 @@ __device__ __forceinline__ void bp_cta(const BpArgs& args, const int tile, const
         }
         continue;
       }
+      const float2 inner = linner[ll];
 #pragma unroll
       for (int k = 0; k < BP_PPT; ++k) {
         const int i = i0 + warp + 8 * k;
-        const FloorSplit fs = floor_split(fmaf(nfiR[k], inf.y, base));
+        const float u = fmaf(nfiR[k], inf.y, base);
+        const FloorSplit fs = floor_split(u);
         const float2 p = pr[fs.i];
         float v = fmaf(fs.f, p.y, p.x);
-        if (kind == LINE_CHECKED) {
+        if (kind == LINE_CHECKED && !(u > inner.x && u < inner.y)) {
           // np.interp(t, k - K, line, left=0, right=0) decided in double like numpy
           const double td = __dsub_rn(__dmul_rn((double)(j - R), (double)inf.x),
                                       __dmul_rn((double)(i - R), (double)inf.y));
@@ -943,15 +950,19 @@ __device__ __forceinline__ void bp_cta(const BpArgs& args, const int tile, const
     __syncthreads();
   }
 
+  if constexpr (EPI == BP_EPI_MLEM || EPI == BP_EPI_SIRT) {
+    bp_epilogue_rows<EPI, BP_PPT>(args, s, i0 + warp, 8, j, acc);
+  } else {
 #pragma unroll
-  for (int k = 0; k < BP_PPT; ++k) {
-    const int i = i0 + warp + 8 * k;
-    if (i < n && j < n) bp_epilogue<EPI>(args, s, i, j, acc[k]);
+    for (int k = 0; k < BP_PPT; ++k) {
+      const int i = i0 + warp + 8 * k;
+      if (i < n && j < n) bp_epilogue<EPI>(args, s, i, j, acc[k]);
+    }
   }
 }
 
 template <int EPI, bool SYM, int MAPS_DTYPE>
-__global__ void __launch_bounds__(BP_THREADS) bp_kernel(BpArgs args) {
+__global__ void __launch_bounds__(BP_THREADS, 4) bp_kernel(BpArgs args) {
   bp_cta<EPI, SYM, MAPS_DTYPE>(args, blockIdx.x, blockIdx.y);
 }
 

@@ -7,7 +7,11 @@ and solver buffers) fits a budget; inside a wave, jobs with the same (n, angles,
 uniform group, and every operator of every iteration runs as ONE ragged launch over all groups
 (``cct_ragged_step``): SIRT groups together, MLEM groups together, and for the MLEM warm start
 every ordered-subsets step over all groups' subset m together.  With ``warm_start=False`` MLEM
-starts from the reference's default (the plain cold-start path).
+starts from the reference's default (the plain cold-start path); with ``warm_start="learned"``
+each MLEM group starts from the learned start (``train_warmstart.learned_start``: one
+ordered-subsets pass keeping snapshots, the warm-start network, one pass per ordered-subsets
+level of ``WarmStartNet.os_levels``), run per group, and the ragged MLEM iterations then judge
+every slice as for the other starts.
 
 The per-slice arithmetic is that of ``BatchedSolver`` (and so of corrct's solvers), which the
 ragged kernels reproduce bit for bit.
@@ -77,11 +81,17 @@ def pack_waves(jobs: list[Job], memory_budget: int, maps_bytes: int = 4) -> list
 
 
 class _Group:
-    def __init__(self, jobs: list[Job], device, maps_dtype: str, schedule, warm: bool, workspace: torch.Tensor):
+    def __init__(self, jobs: list[Job], device, maps_dtype: str, schedule, warm, workspace: torch.Tensor, net=None):
         j0 = jobs[0]
         self.jobs = jobs
         self.method = j0.method
         angles = np.asarray(j0.angles, dtype=np.float64)
+        # the learned start's ordered-subsets levels, when the network has them for this angle count
+        # (the encoder-decoder halves the side three times: n a multiple of 8)
+        self.learned = (warm == "learned" and j0.method == "mlem" and net is not None and j0.n % 8 == 0
+                        and bool(net.os_levels(len(angles))))
+        if self.learned:
+            schedule = [(k, 1) for k in net.os_levels(len(angles))]
         if schedule is None:
             schedule = default_schedule(len(angles))
         self.schedule = None if schedule is None else [(int(k), int(p)) for k, p in schedule]
@@ -116,6 +126,12 @@ class _Group:
             x_shared = None if self.subsets is None else self.subsets.x
             self.solver = BatchedSolver(self.core, self.maps, self.b, "mlem", tolerance=tol, x_shared=x_shared)
 
+    def warm_passes(self) -> int:
+        """Full-data passes of the warm start (the learned start's snapshot pass included)."""
+        if self.subsets is None:
+            return 0
+        return self.subsets.passes + (1 if self.learned else 0)
+
 
 class RaggedStream:
     """Solve a list of jobs in waves of at most ``memory_budget`` device bytes.
@@ -128,12 +144,18 @@ class RaggedStream:
     """
 
     def __init__(self, device=None, memory_budget: int = 100 << 30, schedule=None,
-                 maps_dtype: str = "float32", warm_start: bool = True, check_every: int = 2, fallback_after: int = 200):
+                 maps_dtype: str = "float32", warm_start=True, check_every: int = 2, fallback_after: int = 200,
+                 net=None):
         self.device = _core.require_cuda(device)
         self.memory_budget = int(memory_budget)
         self.schedule = None if schedule is None else [(int(k), int(p)) for k, p in schedule]
         self.maps_dtype = maps_dtype
-        self.warm = bool(warm_start)
+        if warm_start not in (True, False, "subsets", "learned"):
+            raise ValueError(f"warm_start must be True / 'subsets', 'learned' or False, got {warm_start!r}")
+        if warm_start == "learned" and net is None:
+            raise ValueError("warm_start='learned' needs the warm-start network (net=WarmStartNet with weights)")
+        self.warm = warm_start if warm_start == "learned" else bool(warm_start)
+        self.net = net
         self.check_every = int(check_every)
         self.fallback_after = int(fallback_after)
         self.launches = 0
@@ -156,7 +178,8 @@ class RaggedStream:
                     raise ValueError(f"unknown method {j.method!r}")
                 key = (j.method, j.n, len(j.angles), tuple(np.round(np.asarray(j.angles, np.float64), 9)))
                 groups.setdefault(key, []).append(j)
-            gs = [_Group(js, self.device, self.maps_dtype, self.schedule, self.warm, ws) for js in groups.values()]
+            gs = [_Group(js, self.device, self.maps_dtype, self.schedule, self.warm, ws, self.net)
+                  for js in groups.values()]
             self._run_sirt([g for g in gs if g.method == "sirt"], t0)
             self._run_mlem([g for g in gs if g.method == "mlem"], t0, max_iterations)
             del gs
@@ -173,7 +196,7 @@ class RaggedStream:
         for k, j in enumerate(g.jobs):
             j.x = x[k]
             j.extra["residual"] = float(res[k])
-            j.iterations_done = int(its[k]) + (g.spent if g.restarted else (g.subsets.passes if g.subsets is not None else 0))
+            j.iterations_done = int(its[k]) + (g.spent if g.restarted else g.warm_passes())
             j.extra["restarted"] = g.restarted
             if j.finished_s == 0.0:
                 j.finished_s = time.perf_counter() - t0
@@ -194,11 +217,19 @@ class RaggedStream:
     def _run_mlem(self, gs: list[_Group], t0: float, max_iterations: int) -> None:
         if not gs:
             return
-        if self.warm:
+        learned = [g for g in gs if g.learned]
+        if learned:
+            from .train_warmstart import learned_start
+
+            for g in learned:
+                learned_start(self.net, g.subsets, g.core, g.b, g.solver.tau)
+                self.launches += 1
+        others = [g for g in gs if g.subsets is not None and not g.learned]
+        if others:
             # step t of a level applies subset t mod k_g of every group g still in its passes, all
             # groups in one ragged launch per operator
-            for li in range(max(len(g.schedule) for g in gs)):
-                live = [g for g in gs if li < len(g.schedule)]
+            for li in range(max(len(g.schedule) for g in others)):
+                live = [g for g in others if li < len(g.schedule)]
                 steps = max(g.schedule[li][0] * g.schedule[li][1] for g in live)
                 for t in range(steps):
                     members = [g.subsets.levels[li][t % g.schedule[li][0]] for g in live
@@ -223,7 +254,7 @@ class RaggedStream:
                 g.judge_its += self.check_every
                 if self.warm and g.subsets is not None and g.judge_its >= self.fallback_after and not g.restarted:
                     if int(g.solver.active.sum().item()) > 0:
-                        g.spent = g.subsets.passes + g.judge_its
+                        g.spent = g.warm_passes() + g.judge_its
                         g.solver.reset()
                         g.restarted = True
             flags = torch.cat([g.solver.active for g in pending]).cpu().numpy()  # one copy per check

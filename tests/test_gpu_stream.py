@@ -82,3 +82,33 @@ def test_warm_stream_reaches_tolerances_sooner(cuda):
             continue
         assert job.extra["residual"] <= job.tolerance
         assert job.iterations_done < int(single.iterations[0].item())
+
+
+def test_learned_stream_reaches_tolerances(cuda):
+    """The learned start inside the stream (one network evaluation per MLEM group): every MLEM job
+    still reaches its tolerance, and its pass count includes the start's three passes."""
+    import os
+
+    from pycorrectedemissionct_b200 import stream
+    from pycorrectedemissionct_b200.warmstart import WarmStartNet
+
+    weights = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "pycorrectedemissionct_b200",
+                           "weights", "warmstart.pt")
+    if not os.path.exists(weights):
+        pytest.skip("no committed warm-start weights")
+    net = WarmStartNet(device=cuda)
+    net.load(weights)
+    jobs, singles = _jobs(cuda)
+    st = stream.RaggedStream(cuda, warm_start="learned", net=net, check_every=1)
+    st.solve(jobs, max_iterations=200)
+    learned, cold = [], []
+    for job, single in zip(jobs, singles):
+        if job.method != "mlem":
+            continue
+        assert job.extra["residual"] <= job.tolerance
+        assert job.iterations_done >= 3
+        learned.append(job.iterations_done)
+        cold.append(int(single.iterations[0].item()))
+    print(f"learned start in the stream: passes {learned}, cold {cold}")
+    with pytest.raises(ValueError):
+        stream.RaggedStream(cuda, warm_start="learned")
