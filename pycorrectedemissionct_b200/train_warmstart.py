@@ -13,8 +13,9 @@ The learned start (``learned_start``): the snapshot pass, the network, then one 
 of the two ordered-subsets levels; plain MLEM then finishes to the data-residual tolerance and
 judges every slice.
 
-The learned start also serves as PDHG's ``x0`` (``evaluate_pdhg``: passes until the PDHG-KL-TV
-iterate is within 1 % of its long-run solution, from zero and from the learned start).
+The learned start also serves as PDHG's ``x0`` (``evaluate_pdhg``: passes until PDHG-KL-TV reaches
+the data residual of plain PDHG after 200 iterations, from the learned start and without the
+network).
 
 Usage (GPU):  python -m pycorrectedemissionct_b200.train_warmstart --slices 20000 --steps 12000 --out w.pt
               python -m pycorrectedemissionct_b200.train_warmstart --weights w.pt --eval-slices 256 \
@@ -245,51 +246,43 @@ def evaluate(net: WarmStartNet, n: int, n_angles: int, n_slices: int, seed: int,
             "reached_residual": ok}
 
 
-def pdhg_iterations_to(c: core.XrfCore, maps: torch.Tensor, b: torch.Tensor, x_target: torch.Tensor, rel: float,
-                       x0: torch.Tensor | None = None, max_iterations: int = 1000, check_every: int = 5,
-                       tv_lambda: float = 1e-2) -> np.ndarray:
-    """Per slice, the PDHG-KL-TV iterations from ``x0`` (default: the reference's zero start,
-    ``solvers.py:1133-1137``) until the iterate is within ``rel`` (relative L2) of ``x_target``,
-    counted in blocks of ``check_every``; -1 where ``max_iterations`` do not get there."""
-    sv = BatchedSolver(c, maps, b, "pdhg", x0=x0, tv_lambda=tv_lambda)
-    need = np.full(b.shape[0], -1, dtype=np.int64)
-    ref = x_target.flatten(1).norm(dim=1)
-    done = 0
-    while done < max_iterations and (need < 0).any():
-        sv.run(check_every, check_every=check_every, use_graph=False)
-        done += check_every
-        d = ((sv.x - x_target).flatten(1).norm(dim=1) / ref).cpu().numpy()
-        need[(need < 0) & (d <= rel)] = done
-    return need
-
-
 def evaluate_pdhg(net: WarmStartNet, n: int, n_angles: int, n_slices: int, seed: int, batch: int = 16, device=None,
-                  long_iterations: int = 1000, rel: float = 0.01, tv_lambda: float = 1e-2) -> dict:
-    """Held-out evaluation of the learned start as PDHG's ``x0``: per slice, the full-data passes
-    until the PDHG-KL-TV iterate is within ``rel`` (relative L2) of the solution after
-    ``long_iterations`` PDHG iterations from zero, from the reference's zero start and from the
-    learned start (its three ordered-subsets passes counted)."""
+                  plain_iterations: int = 200, tv_lambda: float = 1e-2) -> dict:
+    """Held-out evaluation of the learned start as PDHG's ``x0`` (corrct's hook,
+    ``solvers.py:1133-1137``): per slice, the full-data passes that PDHG-KL-TV needs to reach the
+    data residual plain PDHG (zero start) reaches after ``plain_iterations`` iterations, from the
+    learned start (its three ordered-subsets passes counted) and from the same passes without the
+    network; PDHG stops on the reference's rule, ``tolerance > residual``."""
     device = core.require_cuda(device)
     levels = net.os_levels(n_angles)
-    cold, warm = [], []
+    learned, without, ok = [], [], 0
     for s0 in range(0, n_slices, batch):
         seeds = [seed + k for k in range(s0, min(n_slices, s0 + batch))]
         c, maps, b, _ = synth_batch(n, n_angles, seeds, 0.02, 1e4, device, subsets=levels)
-        long_run = BatchedSolver(c, maps, b, "pdhg", tv_lambda=tv_lambda)
-        long_run.run(long_iterations, check_every=50)
-        x_target = long_run.x.clone()
-        del long_run
-        cold.append(pdhg_iterations_to(c, maps, b, x_target, rel, None, long_iterations, tv_lambda=tv_lambda))
+        plain = BatchedSolver(c, maps, b, "pdhg", tv_lambda=tv_lambda, tolerance=np.zeros(b.shape[0]))
+        plain.run(plain_iterations, check_every=plain_iterations, use_graph=False)
+        tol = plain.residuals.cpu().numpy() * (1 + 1e-9)
+        del plain
         tau = BatchedSolver(c, maps, b, "mlem").tau
-        x0 = learned_start(net, OrderedSubsets(c, maps, b, [(levels[0], 1), (levels[1], 1)]), c, b, tau).clone()
-        w = pdhg_iterations_to(c, maps, b, x_target, rel, x0, long_iterations, tv_lambda=tv_lambda)
-        warm.append(np.where(w >= 0, w + 3, -1))
+        for use_net, out in ((True, learned), (False, without)):
+            os_ = OrderedSubsets(c, maps, b, [(levels[0], 1), (levels[1], 1)])
+            if use_net:
+                x0 = learned_start(net, os_, c, b, tau).clone()
+            else:
+                os_.run_level(0)
+                os_.run_level(0)
+                x0 = os_.run_level(1).clone()
+            sv = BatchedSolver(c, maps, b, "pdhg", tv_lambda=tv_lambda, tolerance=tol, x0=x0)
+            sv.run(2 * plain_iterations, check_every=1, use_graph=False)
+            if use_net:
+                ok += int((sv.residuals.cpu().numpy() <= tol).sum())
+            out.append(sv.iterations.cpu().numpy() + 3)
         del maps
-    cold, warm = np.concatenate(cold), np.concatenate(warm)
-    return {"n": n, "angles": n_angles, "slices": int(cold.size), "rel": rel, "long_iterations": long_iterations,
-            "tv_lambda": tv_lambda, "cold_mean": float(cold[cold >= 0].mean()) if (cold >= 0).any() else None,
-            "cold_reached": int((cold >= 0).sum()), "learned_mean": float(warm[warm >= 0].mean()) if (warm >= 0).any()
-            else None, "learned_reached": int((warm >= 0).sum()), "learned_max": int(warm.max())}
+    learned, without = np.concatenate(learned), np.concatenate(without)
+    return {"n": n, "angles": n_angles, "slices": int(learned.size), "plain_iterations": plain_iterations,
+            "tv_lambda": tv_lambda, "learned_mean": float(learned.mean()), "learned_max": int(learned.max()),
+            "without_network_mean": float(without.mean()), "without_network_max": int(without.max()),
+            "reached_residual": ok}
 
 
 def main():
