@@ -399,15 +399,40 @@ def run_ours(a):
     if headline == "plain":
         fp_keep, bp_keep = list(fp_ms), list(bp_ms)
 
-    # ---- e2e: the headline step from pinned host buffers, copies inside the timed region
+    # ---- e2e: the headline step from pinned host buffers, copies inside the timed region.  A
+    # step's inputs (mu, copied once: mu_out = mu_in here, and the data) go host -> device on a side
+    # stream into staging buffers while the previous step computes; the step moves them into its
+    # working buffers with a device copy, and its reconstruction comes back to pinned memory.
     mu_h = torch.from_numpy(mus_h).pin_memory()
     b_h = b.cpu().pin_memory()
     x_h = torch.empty((S, n, n), dtype=torch.float32).pin_memory()
+    side = torch.cuda.Stream(dev)
+    mu_stage, b_stage = torch.empty_like(mu_in), torch.empty_like(b)
+    pipe = {"staged": None, "free": torch.cuda.Event(), "left": 0}
+    pipe["free"].record()
+
+    def stage_inputs():
+        side.wait_event(pipe["free"])
+        with torch.cuda.stream(side):
+            mu_stage.copy_(mu_h, non_blocking=True)
+            b_stage.copy_(b_h, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(side)
+        pipe["staged"] = ev
 
     def e2e_step(_timed):
-        mu_in.copy_(mu_h, non_blocking=True)
-        mu_out.copy_(mu_h, non_blocking=True)
-        b.copy_(b_h, non_blocking=True)
+        if pipe["staged"] is None:
+            stage_inputs()
+        cur = torch.cuda.current_stream(dev)
+        cur.wait_event(pipe["staged"])
+        mu_in.copy_(mu_stage)
+        mu_out.copy_(mu_stage)
+        b.copy_(b_stage)
+        pipe["free"].record(cur)
+        pipe["staged"] = None
+        pipe["left"] -= 1
+        if pipe["left"] > 0:
+            stage_inputs()  # the next step's inputs, overlapping this step's compute
         if headline == "subsets":
             torch.index_select(b, 2, perm_t, out=b_os)
             subsets.set_data(b_os)
@@ -415,10 +440,12 @@ def run_ours(a):
         x_h.copy_(result.x, non_blocking=True)
         return its
 
-    e2e_step(False)
+    pipe["left"] = 1
+    e2e_step(False)  # warm-up: no copy carried into the timed steps
+    pipe["left"] = a.steps
     e2e_s, _ = timed_steps(e2e_step, a.steps)
     e2e_s = distributed.max_over_ranks(e2e_s, dev)
-    h2d = S * (2 * n * n + a.angles * n) * 4
+    h2d = S * (n * n + a.angles * n) * 4
     d2h = S * n * n * 4
 
     extra = {}

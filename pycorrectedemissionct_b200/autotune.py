@@ -6,7 +6,8 @@ sharing the sample coordinates (``CCT_VARIANT_FP_SLICES2``).  Which is
 faster depends on n, the angle count, the map type, the batch and whether the maps are an
 angle range of a larger array (the TMA variant needs dense maps), so ``tune`` times every
 applicable variant on the actual call (CUDA events, a few launches over a batch of the real
-size) and caches the winner per (GPU, n, angles, detectors, slices, map dtype, layout) in a
+size, with the fused MLEM epilogue the solvers launch) and caches the winner per (GPU, n, angles,
+detectors, slices, map dtype, layout) in a
 JSON file (``$CCT_AUTOTUNE_CACHE`` or ``~/.cache/corrct_b200/autotune.json``).
 
 ``tune_maps`` does the same for ``compute_maps``: how many entries (angles, or half-turn pairs)
@@ -59,25 +60,45 @@ def _store(cache: dict) -> None:
 def key(core: XrfCore, n_slices: int, maps_dtype: torch.dtype, dense: bool = True) -> str:
     name = torch.cuda.get_device_name(core.device).replace(" ", "_")
     layout = "" if dense else "|strided"
-    return f"{name}|n{core.n}|a{core.n_angles}|d{core.n_det}|s{n_slices}|{str(maps_dtype).split('.')[-1]}{layout}"
+    return f"{name}|n{core.n}|a{core.n_angles}|d{core.n_det}|s{n_slices}|{str(maps_dtype).split('.')[-1]}{layout}|mlem-fp"
 
 
-def time_fp(core: XrfCore, vol: torch.Tensor, maps: torch.Tensor, variant: int, reps: int = 3) -> float:
-    """Mean fp launch time (ms) of one variant on the given batch."""
+def time_fp(core: XrfCore, vol: torch.Tensor, maps: torch.Tensor, variant: int, reps: int = 3,
+            epilogue: str = "mlem") -> float:
+    """Mean fp launch time (ms) of one variant on the given batch: the fused MLEM fp (ratio and KL
+    residual, ``cct_mlem_fp``, what the solvers launch) or the plain projection (``"store"``)."""
+    import ctypes
+
+    from .engine import BatchedSolver
+
     old = core.variant
     core.variant = variant
     try:
         out = core.fp(vol, maps)  # warm-up (also loads the kernel)
+        if epilogue == "mlem":
+            sv = BatchedSolver(core, maps, out, "mlem", x0=vol)
+            h = core_stream(core)
+
+            def launch():
+                _lib.call("cct_mlem_fp", ctypes.byref(sv.desc), sv._maps_ptr, ctypes.byref(sv.state), h)
+        else:
+            def launch():
+                core.fp(vol, maps, out=out)
+        launch()
         start = torch.cuda.Event(enable_timing=True)
         stop = torch.cuda.Event(enable_timing=True)
         start.record()
         for _ in range(reps):
-            core.fp(vol, maps, out=out)
+            launch()
         stop.record()
         stop.synchronize()
         return start.elapsed_time(stop) / reps
     finally:
         core.variant = old
+
+
+def core_stream(c: XrfCore):
+    return core.stream_handle(c.device)
 
 
 def tune(core: XrfCore, vol: torch.Tensor, maps: torch.Tensor, force: bool = False) -> int:
