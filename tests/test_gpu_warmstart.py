@@ -8,6 +8,8 @@
    the network, one pass per ordered-subsets level) followed by MLEM needs at most half the
    full-data passes of plain MLEM to reach plain MLEM's 200-iteration KL residual, and fewer than
    the same ordered-subsets passes without the network.
+3. The learned start as PDHG's x0: PDHG-KL-TV reaches plain PDHG's 200-iteration data residual in
+   at most half the passes.
 """
 
 import os
@@ -71,3 +73,21 @@ def test_committed_network_gains_over_the_method_without_it(cuda):
     assert r["reached_residual"] == 16
     assert r["learned_mean"] <= 0.5 * r["plain_passes"]
     assert r["learned_mean"] < r["without_network_mean"]
+
+
+def test_committed_network_warm_starts_pdhg(cuda):
+    """The learned start as PDHG's x0 (corrct's hook): on held-out config-4 slices (256 x 256, 360
+    angles), PDHG-KL-TV from the learned start reaches the data residual that plain PDHG (zero
+    start) reaches after 200 iterations in at most half the full-data passes."""
+    if not os.path.exists(WEIGHTS):
+        pytest.skip("no committed warm-start weights")
+    from pycorrectedemissionct_b200 import train_warmstart as tw
+    from pycorrectedemissionct_b200.warmstart import WarmStartNet
+
+    net = WarmStartNet(device=cuda)
+    net.load(WEIGHTS)
+    r = tw.evaluate_pdhg(net, 256, 360, 8, seed=975_000, batch=8, device=cuda)
+    print(f"PDHG from the learned start: {r['learned_mean']:.1f} passes (max {r['learned_max']}), without the "
+          f"network {r['without_network_mean']:.1f}, plain {r['plain_iterations']}")
+    assert r["reached_residual"] == 8
+    assert r["learned_mean"] <= 0.5 * r["plain_iterations"]
