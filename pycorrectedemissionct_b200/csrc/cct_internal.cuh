@@ -130,8 +130,9 @@ __device__ __forceinline__ void bp_epilogue(const BpArgs& a, int s, int i, int j
   const float tau = a.tau[(a.tau_shared ? 0 : (int64_t)s * n2) + pix];
   float x = a.x[idx];
   if (EPI == BP_EPI_MLEM) {
-    // x *= upd / tau  (corrct solvers.py:798-803)
-    x = x * (v / tau);
+    // x *= upd / tau  (corrct solvers.py:798-803); a pixel that no line reaches (tau = 0, which an
+    // ordered subset of few angles can leave in the corners) keeps its value
+    x = tau != 0.f ? x * (v / tau) : x;
   } else if (EPI == BP_EPI_SIRT) {
     // x += upd * tau  (corrct solvers.py:977)
     x = x + v * tau;
@@ -179,7 +180,8 @@ __device__ __forceinline__ void bp_epilogue_rows(const BpArgs& a, int s, int i0,
     const int i = i0 + di * k;
     if (i >= n || j >= n) continue;
     const int64_t pix = (int64_t)i * n + j;
-    float x = EPI == BP_EPI_MLEM ? xv[k] * (v[k] / tv[k]) : xv[k] + v[k] * tv[k];
+    // MLEM: a pixel that no line reaches (tau = 0) keeps its value, as in bp_epilogue
+    float x = EPI == BP_EPI_MLEM ? (tv[k] != 0.f ? xv[k] * (v[k] / tv[k]) : xv[k]) : xv[k] + v[k] * tv[k];
     x = apply_limits(a, x);
     if (a.x_mask != nullptr) x *= a.x_mask[a.mask_per_slice ? (int64_t)s * n2 + pix : pix];
     a.x[(int64_t)s * n2 + pix] = x;

@@ -589,3 +589,34 @@ def test_quarter_turn_quads():
     assert geometry.quarter_turn_quads(rad32, geometry.half_turn_pairs(rad32), np.pi / 3) is None
     assert geometry.quarter_turn_quads(rad32, None, np.pi / 2) is None
 
+
+
+@pytest.mark.parametrize("deg", [0.0, 23.0, 45.0, 90.0, 137.5, 301.0])
+def test_quarter_turn_row_cumsum_identity(deg):
+    """The quad maps scan one rotated lattice per quad (csrc/cct_maps.cu, maps_rowscan_kernel and
+    maps_resample_quad_kernel): with F = rotate(pad(mu), -phi), the column roll + cumsum of F gives
+    the line integral of phi (the reference's compute_attenuation), the same along rows,
+    V[r][c] = sum_{c' < c} F[r][c'] + F[r][c] / 2 + F[r][P - 1] / 2, gives that of phi + pi / 2 and
+    Kr - V (Kr = sum F[r] + F[r][0] / 2 + F[r][P - 1] / 2) that of phi + 3 pi / 2, all three read
+    back at phi's rotate(+phi) positions.  And which of a quad's two other angles is phi + pi / 2
+    follows from the rotate(+angle) matrices: m0(a) m3(phi) - m3(a) m0(phi) = -1 for a = phi + pi / 2."""
+    from oracle import port
+    from oracle import skimage_restated as skr
+    from pycorrectedemissionct_b200 import geometry
+
+    n = 40
+    mu = np.random.default_rng(int(deg * 10) + 1).random((n, n)) * 0.02
+    edge, _ = port.padded_size(n)
+    F = skr.rotate(np.pad(mu, ((edge, edge), (edge, edge))), -deg, order=1, clip=False)
+    W = np.cumsum(F, axis=0) - F / 2 + F[-1:, :] / 2
+    V = np.cumsum(F, axis=1) - F / 2 + F[:, -1:] / 2
+    Kr = F.sum(axis=1, keepdims=True) + F[:, :1] / 2 + F[:, -1:] / 2
+    phi = np.deg2rad(deg)
+    for arr, ang in ((W, phi), (V, phi + np.pi / 2), (Kr - V, phi + 1.5 * np.pi)):
+        back = skr.rotate(arr, deg, order=1, clip=False)[edge:-edge, edge:-edge]
+        ref = -np.log(port.compute_attenuation(mu, ang))
+        assert np.abs(back - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+    m_phi = geometry.rotate_matrix(deg, 2 * edge + n)
+    for off, sign in ((90.0, -1.0), (-90.0, 1.0), (270.0, 1.0)):
+        m = geometry.rotate_matrix(deg + off, 2 * edge + n)
+        assert abs((m[0] * m_phi[3] - m[3] * m_phi[0]) - sign) < 1e-12
