@@ -246,9 +246,7 @@ __device__ __forceinline__ void column_support(double ax, double bx, double ay, 
 // One thread per column; the 32 columns of a warp walk the rows in lockstep (coalesced W
 // stores), with warp-uniform row ranges: no lane samples before the warp's first support row or
 // after its last, and rows where every lane's four taps are inside mu skip the per-tap tests.
-// QROWS (quarter-turn quads): job ai scans quad a0 + ai's first entry into plane 2 ai and also
-// stores the sampled lattice U into plane 2 ai + 1, whose rows maps_rowscan_kernel then sums.
-template <bool PAIRS, bool QROWS = false>
+template <bool PAIRS>
 __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
   const int P = p.P, n = p.n;
   const int cpr_raw = blockIdx.x * blockDim.x + threadIdx.x;  // rotated-frame column c'
@@ -259,7 +257,7 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
   const int ai = job_lin / p.jobs_per_angle;
   const int job = job_lin - ai * p.jobs_per_angle;
   int a, b;
-  entry_angles(p, QROWS ? p.quads[6 * (p.a0 + ai)] : slot_entry(p, ai), &a, &b);
+  entry_angles(p, slot_entry(p, ai), &a, &b);
   if (a < 0) return;  // the whole CTA
   const double* Md = job_matrix(p, a, job, 0);  // rotate(-phi)
   const bool incident = p.has_in && job == 0;
@@ -294,9 +292,7 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
   if (wilo > wihi) { wilo = whi + 1; wihi = whi; }  // no row is inside for every lane
   const float fc = (float)cpr;
   const float xc = fmaf(m00, fc, m02), yc = fmaf(m10, fc, m12);
-  const int plane = QROWS ? 2 * ai : ai;
-  float* W = p.work + (((int64_t)s * p.na + plane) * p.jobs_per_angle + job) * (int64_t)P * P + cpr;
-  float* U = QROWS ? W + (int64_t)P * P : nullptr;  // jobs_per_angle == 1 with quads
+  float* W = p.work + (((int64_t)s * p.na + ai) * p.jobs_per_angle + job) * (int64_t)P * P + cpr;
 
   // wrap-around term U[P-1] / 2 of roll + cumsum
   double wrap = 0.0;
@@ -304,19 +300,16 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
     const float fr = (float)(P - 1);
     wrap = 0.5 * (double)bilin_zero_mu(mu, n, sy, sx, fmaf(m01, fr, xc), fmaf(m11, fr, yc));
   }
-  // W[r] = acc + U[r]/2 + wrap with acc = sum_{k<r} U[k] (FP64); U = 0 outside [lo, hi]
+  // W[r] = acc + U[r]/2 + wrap with acc = sum_{k<r} U[k] (FP64); U = 0 outside [lo, hi].  Only
+  // the warp's rows [wlo, whi] are stored: outside them W is constant per column and the
+  // resample, whose positions all map back into the image, never reads it there
+  // (tests/test_host.py::test_maps_resample_reads_only_scanned_rows mirrors that arithmetic).
   double acc = 0.0;
-  int r = 0;
-  const float w_before = (float)wrap;
-  for (; r < wlo; ++r) {
-    if (valid) W[(int64_t)r * P] = w_before;
-    if (QROWS && valid) U[(int64_t)r * P] = 0.f;
-  }
+  int r = wlo;
   for (; r < wilo; ++r) {
     const float fr = (float)r;
     const float u = (r >= lo && r <= hi) ? bilin_zero_mu(mu, n, sy, sx, fmaf(m01, fr, xc), fmaf(m11, fr, yc)) : 0.f;
     if (valid) W[(int64_t)r * P] = (float)(acc + 0.5 * (double)u + wrap);
-    if (QROWS && valid) U[(int64_t)r * P] = u;
     acc += (double)u;
   }
   for (; r + 3 <= wihi; r += 4) {
@@ -329,7 +322,6 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       if (valid) W[(int64_t)(r + k) * P] = (float)(acc + 0.5 * (double)u[k] + wrap);
-      if (QROWS && valid) U[(int64_t)(r + k) * P] = u[k];
       acc += (double)u[k];
     }
   }
@@ -337,20 +329,13 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
     const float fr = (float)r;
     const float u = bilin_inside_mu(mu, n, sy, sx, fmaf(m01, fr, xc), fmaf(m11, fr, yc));
     if (valid) W[(int64_t)r * P] = (float)(acc + 0.5 * (double)u + wrap);
-    if (QROWS && valid) U[(int64_t)r * P] = u;
     acc += (double)u;
   }
   for (; r <= whi; ++r) {
     const float fr = (float)r;
     const float u = (r >= lo && r <= hi) ? bilin_zero_mu(mu, n, sy, sx, fmaf(m01, fr, xc), fmaf(m11, fr, yc)) : 0.f;
     if (valid) W[(int64_t)r * P] = (float)(acc + 0.5 * (double)u + wrap);
-    if (QROWS && valid) U[(int64_t)r * P] = u;
     acc += (double)u;
-  }
-  const float w_after = (float)(acc + wrap);
-  for (; r < P; ++r) {
-    if (valid) W[(int64_t)r * P] = w_after;
-    if (QROWS && valid) U[(int64_t)r * P] = 0.f;
   }
   if (PAIRS && b >= 0 && valid) {
     // the partner angle (phi + pi) rotates by a half turn more: its frame is this one turned
@@ -358,7 +343,7 @@ __global__ void __launch_bounds__(128) maps_scan_kernel(MapsPass p) {
     // K = sum_k U[k] + U[0]/2 + U[P-1]/2 (the reverse roll + cumsum of the same column)
     double first = 0.0;
     if (0 >= lo && 0 <= hi) first = 0.5 * (double)bilin_zero_mu(mu, n, sy, sx, xc, yc);
-    p.kcol[(((int64_t)s * p.na + plane) * p.jobs_per_angle + job) * P + cpr] = (float)(acc + first + wrap);
+    p.kcol[(((int64_t)s * p.na + ai) * p.jobs_per_angle + job) * P + cpr] = (float)(acc + first + wrap);
   }
 }
 
@@ -505,98 +490,15 @@ __global__ void __launch_bounds__(256, PAIRS ? 5 : 1) maps_resample_kernel(MapsP
   }
 }
 
-// Rows of a quad's lattice U (plane 2 q + 1, written by maps_scan_kernel<true, true>) summed in
-// place into V[r][c] = sum_{c' < c} U[r][c'] + U[r][c] / 2 + U[r][P - 1] / 2, the roll + cumsum of
-// the reference taken along rows, and the row constants Kr[r] = sum U[r] + U[r][0] / 2 +
-// U[r][P - 1] / 2 (kcol slot 2 q + 1).  The lattice of angle phi + pi / 2 is phi's turned by a
-// quarter turn (np.rot90(F_phi, -1)), so its roll + cumsum along its own columns is V, read at
-// phi's positions (and phi + 3 pi / 2's is Kr - V).  One warp per row: 32 columns per step, an
-// FP64 inclusive warp scan and a running carry.
-__global__ void __launch_bounds__(256) maps_rowscan_kernel(MapsPass p) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int P = p.P;
-  const int r = blockIdx.x * 8 + warp;
-  const int q = blockIdx.y, s = blockIdx.z;
-  if (r >= P) return;  // whole warps
-  const int plane = 2 * q + 1;
-  float* row = p.work + ((int64_t)s * p.na + plane) * (int64_t)P * P + (int64_t)r * P;
-  const double wrap = 0.5 * (double)row[P - 1];
-  const double first = 0.5 * (double)row[0];
-  __syncwarp();
-  double carry = 0.0;
-  for (int c0 = 0; c0 < P; c0 += 32) {
-    const int c = c0 + lane;
-    const double u = c < P ? (double)row[c] : 0.0;
-    double incl = u;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const double t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    if (c < P) row[c] = (float)(carry + (incl - u) + 0.5 * u + wrap);
-    carry += __shfl_sync(0xffffffffu, incl, 31);
-  }
-  if (lane == 0) p.kcol[((int64_t)s * p.na + plane) * P + r] = (float)(carry + first + wrap);
-}
-
-// Bilinear samples at (x, y) of a quad's column sums W and row sums V (P x P, zero outside the
-// frame) and of their partner fields Kc[c] - W[r][c] and Kr[r] - V[r][c]; the same four taps
-// serve both planes.  As in bilin_square_pair, inside the frame a partner is its interpolated
-// constant minus the sample, at the frame edge its four taps are interpolated.
-__device__ __forceinline__ void bilin_square_quad(const float* wf, const float* vf, const float* kc, const float* kr,
-                                                  int P, float x, float y, float (&L)[4]) {
-  const FloorSplit fx = floor_split(x), fy = floor_split(y);
-  const int x0 = fx.i, y0 = fy.i;
-  float w00, w01, w10, w11, v00, v01, v10, v11;
-  if ((unsigned)x0 < (unsigned)(P - 1) && (unsigned)y0 < (unsigned)(P - 1)) {
-    const int64_t o = (int64_t)y0 * P + x0;
-    w00 = __ldg(wf + o); w01 = __ldg(wf + o + 1); w10 = __ldg(wf + o + P); w11 = __ldg(wf + o + P + 1);
-    v00 = __ldg(vf + o); v01 = __ldg(vf + o + 1); v10 = __ldg(vf + o + P); v11 = __ldg(vf + o + P + 1);
-    const float c0 = __ldg(kc + x0), c1 = __ldg(kc + x0 + 1), r0 = __ldg(kr + y0), r1 = __ldg(kr + y0 + 1);
-    float top = fmaf(fx.f, w01 - w00, w00), bot = fmaf(fx.f, w11 - w10, w10);
-    L[0] = fmaf(fy.f, bot - top, top);
-    L[1] = fmaf(fx.f, c1 - c0, c0) - L[0];
-    top = fmaf(fx.f, v01 - v00, v00);
-    bot = fmaf(fx.f, v11 - v10, v10);
-    L[2] = fmaf(fy.f, bot - top, top);
-    L[3] = fmaf(fy.f, r1 - r0, r0) - L[2];
-    return;
-  }
-  const bool xin0 = x0 >= 0 && x0 < P, xin1 = x0 + 1 >= 0 && x0 + 1 < P;
-  const bool yin0 = y0 >= 0 && y0 < P, yin1 = y0 + 1 >= 0 && y0 + 1 < P;
-  const float c0 = xin0 ? __ldg(kc + x0) : 0.f, c1 = xin1 ? __ldg(kc + x0 + 1) : 0.f;
-  const float r0 = yin0 ? __ldg(kr + y0) : 0.f, r1 = yin1 ? __ldg(kr + y0 + 1) : 0.f;
-  const int64_t o = (int64_t)y0 * P + x0;
-  const bool i00 = yin0 && xin0, i01 = yin0 && xin1, i10 = yin1 && xin0, i11 = yin1 && xin1;
-  w00 = i00 ? __ldg(wf + o) : 0.f;
-  w01 = i01 ? __ldg(wf + o + 1) : 0.f;
-  w10 = i10 ? __ldg(wf + o + P) : 0.f;
-  w11 = i11 ? __ldg(wf + o + P + 1) : 0.f;
-  v00 = i00 ? __ldg(vf + o) : 0.f;
-  v01 = i01 ? __ldg(vf + o + 1) : 0.f;
-  v10 = i10 ? __ldg(vf + o + P) : 0.f;
-  v11 = i11 ? __ldg(vf + o + P + 1) : 0.f;
-  auto lerp2 = [&](float a00, float a01, float a10, float a11) {
-    const float top = fmaf(fx.f, a01 - a00, a00), bot = fmaf(fx.f, a11 - a10, a10);
-    return fmaf(fy.f, bot - top, top);
-  };
-  L[0] = lerp2(w00, w01, w10, w11);
-  L[1] = lerp2(i00 ? c0 - w00 : 0.f, i01 ? c1 - w01 : 0.f, i10 ? c0 - w10 : 0.f, i11 ? c1 - w11 : 0.f);
-  L[2] = lerp2(v00, v01, v10, v11);
-  L[3] = lerp2(i00 ? r0 - v00 : 0.f, i01 ? r0 - v01 : 0.f, i10 ? r1 - v10 : 0.f, i11 ? r1 - v11 : 0.f);
-}
-
 // Quarter-turn quads (one point detector whose emitted direction is the incident direction of
-// another angle of the set, mu_out = emitted_scale * mu_in): the pass scanned one incident
-// lattice per quad, entry e's angle phi, into its column sums W (plane 2q, constants Kc) and row
-// sums V (plane 2q + 1, constants Kr).  At every pixel one position in phi's frame gives the
-// incident line integrals of the quad's four angles: phi (W), phi + pi (Kc - W), phi + pi / 2 (V)
-// and phi + 3 pi / 2 (Kr - V); which of entry e''s angle and partner is phi + pi / 2 follows from
-// their rotate(+angle) matrices (m0(a) m3(phi) - m3(a) m0(phi) = -1 for a = phi + pi / 2).  The map
-// of angle k is exp(-L[k]) * exp(-emitted_scale * L[src[k]]), src[k] naming which of the four
-// angles the emitted direction of angle k is (the three derived angles are phi + k pi / 2
-// exactly, where the reference rotates by their float32 angles, like a half-turn partner).  Four
-// maps from one gather of two planes per pixel.
+// another angle of the set, mu_out = emitted_scale * mu_in): the pass scanned only incident
+// fields, two per quad (slots 2q, 2q + 1), each a half-turn pair of angles.  At every pixel the two
+// pair samples give the incident line integrals L[0..3] of the quad's four angles (entry e's angle
+// and partner, entry e''s angle and partner); the map of angle k is
+// exp(-L[k]) * exp(-emitted_scale * L[src[k]]), src[k] naming which of the four angles the
+// emitted direction of angle k is (its rotation angle differs from the reference's emitted angle
+// only by the float32 rounding of the angles, like a half-turn partner's).  Four maps from two
+// gathers per pixel, where the per-pair resample needs two gathers for two maps.
 __global__ void __launch_bounds__(256, 5) maps_resample_quad_kernel(MapsPass p) {
   __shared__ float qm[2][6];  // rotate(+phi) matrices of the two entries' angles
   __shared__ int qa[4];       // the four angles
@@ -631,25 +533,20 @@ __global__ void __launch_bounds__(256, 5) maps_resample_quad_kernel(MapsPass p) 
   const float X = (float)(j + p.e);
   const int64_t n2 = (int64_t)n * n;
   const float sc = p.emitted_scale;
-  const float* m = qm[0];
-  const float* wf = p.work + ((int64_t)s * p.na + 2 * qi) * (int64_t)P * P;
-  const float* vf = wf + (int64_t)P * P;
-  const float* kc = p.kcol + ((int64_t)s * p.na + 2 * qi) * (int64_t)P;
-  const float* kr = kc + P;
-  // entry e''s angle is phi + pi / 2 (V) or phi + 3 pi / 2 (Kr - V)
-  const bool plus = qm[1][0] * m[3] - qm[1][3] * m[0] < 0.f;
   float L[4][RS_PIX];
 #pragma unroll
-  for (int k = 0; k < RS_PIX; ++k) {
-    const float Y = (float)(i0 + 8 * k + p.e);
-    const float x = fmaf(m[1], Y, fmaf(m[0], X, m[2]));
-    const float y = fmaf(m[4], Y, fmaf(m[3], X, m[5]));
-    float l[4];
-    bilin_square_quad(wf, vf, kc, kr, P, x, y, l);
-    L[0][k] = l[0];
-    L[1][k] = l[1];
-    L[2][k] = plus ? l[2] : l[3];
-    L[3][k] = plus ? l[3] : l[2];
+  for (int w = 0; w < 2; ++w) {
+    const float* m = qm[w];
+    const int slot = 2 * qi + w;
+    const float* wf = p.work + ((int64_t)s * p.na + slot) * (int64_t)P * P;
+    const float* kc = p.kcol + ((int64_t)s * p.na + slot) * (int64_t)P;
+#pragma unroll
+    for (int k = 0; k < RS_PIX; ++k) {
+      const float Y = (float)(i0 + 8 * k + p.e);
+      const float x = fmaf(m[1], Y, fmaf(m[0], X, m[2]));
+      const float y = fmaf(m[4], Y, fmaf(m[3], X, m[5]));
+      bilin_square_pair(wf, kc, P, x, y, &L[2 * w][k], &L[2 * w + 1][k]);
+    }
   }
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
@@ -727,9 +624,8 @@ int64_t maps_bytes_per_angle(const cct_maps_desc* d) {
   return jobs * (P * P + P) * (int64_t)sizeof(float) * d->n_slices;  // W planes + partner constants
 }
 
-// Quarter-turn quads: per pass, one incident lattice per quad, summed along columns (the scan) and
-// rows (the row scan) into two planes (a quad takes the workspace of one entry with incident and
-// emitted jobs), then one quad resample.
+// Quarter-turn quads: per pass, the incident fields of 2 entries per quad (one job each, so a quad
+// takes the workspace of one entry with incident and emitted jobs), then one quad resample.
 static int launch_maps_quads(const cct_maps_desc* d, const float* mu_in, void* maps, void* work, size_t work_bytes,
                              cudaStream_t st) {
   const int e = padded_edge(d->n);
@@ -757,9 +653,8 @@ static int launch_maps_quads(const cct_maps_desc* d, const float* mu_in, void* m
   for (int q0 = 0; q0 < d->n_quads; q0 += per_pass) {
     const int nq = std::min(per_pass, d->n_quads - q0);
     p.a0 = q0;
-    p.na = 2 * nq;  // planes: W and V of every quad
-    maps_scan_kernel<true, true><<<dim3((P + 127) / 128, nq, d->n_slices), 128, 0, st>>>(p);
-    maps_rowscan_kernel<<<dim3((P + 7) / 8, nq, d->n_slices), 256, 0, st>>>(p);
+    p.na = 2 * nq;
+    maps_scan_kernel<true><<<dim3((P + 127) / 128, p.na, d->n_slices), 128, 0, st>>>(p);
     maps_resample_quad_kernel<<<dim3((unsigned)(tiles * tiles), nq, d->n_slices), 256, 0, st>>>(p);
   }
   return CCT_OK;

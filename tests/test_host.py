@@ -325,6 +325,52 @@ def test_maps_scan_fast_rows_stay_inside(n, n_angles):
     assert checked > 0 or n < 64
 
 
+@pytest.mark.parametrize("n,n_angles", [(2, 16), (3, 16), (16, 40), (33, 36), (130, 24), (512, 12)])
+def test_maps_resample_reads_only_scanned_rows(n, n_angles):
+    """The scan kernel stores a column's W only on its warp's support rows [min lo, max hi] (the
+    rows outside are constant and never read); mirror the resample's FP32 positions (rotate(+phi)
+    of every map pixel) and check that each of its bilinear taps inside the frame lies on a row the
+    scan stored for the tap's column, for the incident and emitted rotations."""
+    from pycorrectedemissionct_b200 import geometry
+
+    e, P = geometry.padded_size(n)
+    angles = np.concatenate([np.linspace(0, 2 * np.pi, n_angles, endpoint=False), [np.pi / 4, np.pi / 2, 1e-7, np.pi - 1e-7]])
+    rot_in, rot_out, _ = geometry.attenuation_rotations(np.array(angles, dtype=np.float32), [np.pi / 2, 1.0], n)
+    pairs = [rot_in[a] for a in range(len(angles))] + [rot_out[a, d, 0] for a in range(len(angles)) for d in range(2)]
+
+    def fma32(a, b, c):
+        return (np.float64(a) * np.float64(b) + np.float64(c)).astype(np.float32)
+
+    ii, jj = np.meshgrid(np.arange(n, dtype=np.float32), np.arange(n, dtype=np.float32), indexing="ij")
+    X, Y = jj + np.float32(e), ii + np.float32(e)
+    for mats in pairs:
+        Md, Mb = mats[0], mats[1]  # rotate(-phi) of the scan, rotate(+phi) of the resample
+        # rows the scan stores per column: its warp's [min lo, max hi]
+        wlo = np.full(P, P, dtype=np.int64)
+        whi = np.full(P, -1, dtype=np.int64)
+        for w0 in range(0, P, 32):
+            los, his = [], []
+            for c in range(w0, min(w0 + 32, P)):
+                ax, ay = Md[0] * c + Md[2] - e, Md[3] * c + Md[5] - e
+                lo, hi = _column_range(ax, Md[1], ay, Md[4], -1.0, float(n), P, True)
+                if lo <= hi:
+                    los.append(lo)
+                    his.append(hi)
+            if los:
+                wlo[w0:w0 + 32] = min(los)
+                whi[w0:w0 + 32] = max(his)
+        m = [np.float32(v) for v in Mb]
+        x = fma32(m[1], Y, fma32(m[0], X, m[2]))
+        y = fma32(m[4], Y, fma32(m[3], X, m[5]))
+        x0, y0 = np.floor(x).astype(np.int64), np.floor(y).astype(np.int64)
+        for dx in (0, 1):
+            for dy in (0, 1):
+                c, r = (x0 + dx).ravel(), (y0 + dy).ravel()
+                inside = (c >= 0) & (c < P) & (r >= 0) & (r < P)
+                c, r = c[inside], r[inside]
+                assert np.all((r >= wlo[c]) & (r <= whi[c])), (n, np.count_nonzero((r < wlo[c]) | (r > whi[c])))
+
+
 @pytest.mark.parametrize("n", [64, 130, 512])
 def test_fp_chunk_boxes_hold_every_tap(n):
     """The forward projection stages a box per 64-bin x 64-row chunk (chunk_box in
@@ -588,35 +634,3 @@ def test_quarter_turn_quads():
     rad32 = np.array(phantoms.angles(40), dtype=np.float32)
     assert geometry.quarter_turn_quads(rad32, geometry.half_turn_pairs(rad32), np.pi / 3) is None
     assert geometry.quarter_turn_quads(rad32, None, np.pi / 2) is None
-
-
-
-@pytest.mark.parametrize("deg", [0.0, 23.0, 45.0, 90.0, 137.5, 301.0])
-def test_quarter_turn_row_cumsum_identity(deg):
-    """The quad maps scan one rotated lattice per quad (csrc/cct_maps.cu, maps_rowscan_kernel and
-    maps_resample_quad_kernel): with F = rotate(pad(mu), -phi), the column roll + cumsum of F gives
-    the line integral of phi (the reference's compute_attenuation), the same along rows,
-    V[r][c] = sum_{c' < c} F[r][c'] + F[r][c] / 2 + F[r][P - 1] / 2, gives that of phi + pi / 2 and
-    Kr - V (Kr = sum F[r] + F[r][0] / 2 + F[r][P - 1] / 2) that of phi + 3 pi / 2, all three read
-    back at phi's rotate(+phi) positions.  And which of a quad's two other angles is phi + pi / 2
-    follows from the rotate(+angle) matrices: m0(a) m3(phi) - m3(a) m0(phi) = -1 for a = phi + pi / 2."""
-    from oracle import port
-    from oracle import skimage_restated as skr
-    from pycorrectedemissionct_b200 import geometry
-
-    n = 40
-    mu = np.random.default_rng(int(deg * 10) + 1).random((n, n)) * 0.02
-    edge, _ = port.padded_size(n)
-    F = skr.rotate(np.pad(mu, ((edge, edge), (edge, edge))), -deg, order=1, clip=False)
-    W = np.cumsum(F, axis=0) - F / 2 + F[-1:, :] / 2
-    V = np.cumsum(F, axis=1) - F / 2 + F[:, -1:] / 2
-    Kr = F.sum(axis=1, keepdims=True) + F[:, :1] / 2 + F[:, -1:] / 2
-    phi = np.deg2rad(deg)
-    for arr, ang in ((W, phi), (V, phi + np.pi / 2), (Kr - V, phi + 1.5 * np.pi)):
-        back = skr.rotate(arr, deg, order=1, clip=False)[edge:-edge, edge:-edge]
-        ref = -np.log(port.compute_attenuation(mu, ang))
-        assert np.abs(back - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
-    m_phi = geometry.rotate_matrix(deg, 2 * edge + n)
-    for off, sign in ((90.0, -1.0), (-90.0, 1.0), (270.0, 1.0)):
-        m = geometry.rotate_matrix(deg + off, 2 * edge + n)
-        assert abs((m[0] * m_phi[3] - m[3] * m_phi[0]) - sign) < 1e-12
