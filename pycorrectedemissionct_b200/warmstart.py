@@ -241,12 +241,15 @@ class WarmStartNet:
         """NHWC bf16 input (B, H, W, 16) from FP32 planar images (B, H, W), one per channel, each
         slice divided by its ``slice_scale``."""
         b, hh, ww = planes[0].shape
-        planes = [p.contiguous() for p in planes]
-        ptrs = torch.tensor([p.data_ptr() for p in planes], dtype=torch.int64, device=self.device)
+        # the planes stacked and their pointer table built on the device: no host copy or wait, so
+        # the call can be captured in a CUDA graph (the stream orders the kernel before any reuse
+        # of these buffers)
+        stacked = torch.stack([p.float() for p in planes])
+        step = stacked[0].numel() * stacked.element_size()
+        ptrs = torch.arange(len(planes), dtype=torch.int64, device=self.device) * step + stacked.data_ptr()
         out = torch.empty((b, hh, ww, IN_CHANNELS), dtype=BF16, device=self.device)
         _lib.check(self.lib.cct_net_pack_nhwc(ptrs.data_ptr(), len(planes), out.data_ptr(), b * hh * ww, IN_CHANNELS,
                                               _p(slice_scale), hh * ww, stream_handle(self.device)))
-        torch.cuda.current_stream(self.device).synchronize()  # keep `planes` / `ptrs` alive until read
         return out
 
     def predict(self, planes: list[torch.Tensor], base: torch.Tensor, slice_scale: torch.Tensor,
