@@ -9,7 +9,7 @@ reaches after 200 iterations (calibrated once, untimed).  Paths:
 * plain: MLEM from the default start;
 * subsets (the headline): ordered-subsets EM passes (90 subsets x 2 passes, then 18 x 1; each pass
   costs one MLEM iteration), then MLEM to the residual, which judges every slice;
-* learned: on the learned part's own data (config 4's textured slices at 1e4 counts), the learned
+* learned: on the learned part's own data (textured slices at 1e4 peak counts), the learned
   start (one ordered-subsets pass keeping 10 snapshots, the tensor-core encoder-decoder, one pass
   per ordered-subsets level) then MLEM to the residual, timed beside plain MLEM and the
   ordered-subsets passes on the same slices.
@@ -23,8 +23,8 @@ data copied in, the reconstruction copied out inside the timed region); ``dropin
 call a corrct user makes (projector from mu + MLEM with a tolerance, numpy in and out).
 ``--impl reference`` times the reference algorithm's CPU implementation (the oracle port in
 ``oracle/``) on the host cores on a bounded sample of the same workload.  Other workloads:
-``--workload ragged`` (mixed sizes), ``waves`` (config 2: 512 slices of plain MLEM, FP32 and BF16
-maps), ``channels`` (config 3: 8 fluorescence channels, PDHG-TV).
+``--workload ragged`` (mixed sizes), ``waves`` (512 slices of plain MLEM in HBM-sized waves, FP32
+and BF16 maps), ``channels`` (8 fluorescence channels of 1024x1024x1440 slices, PDHG-TV).
 """
 
 from __future__ import annotations
@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=20240)
     ap.add_argument("--method", default="auto", choices=["auto", "plain", "subsets"],
                     help="headline path (auto: ordered subsets); the others are timed beside it")
-    ap.add_argument("--learned-peak", type=float, default=1e4, help="learned leg: Poisson peak counts (config 4)")
+    ap.add_argument("--learned-peak", type=float, default=1e4, help="learned leg: Poisson peak counts of its textured slices")
     ap.add_argument("--subsets", default="90:2,18:1", help="ordered-subsets schedule subsets:passes,...")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra-legs", action="store_true",
@@ -528,8 +528,8 @@ def run_ours(a):
 
 
 def run_learned_leg(a, dev, rank, world, maps, ws, variant, schedule) -> dict:
-    """The learned warm start on the learned part's own data (config 4's slices at the benchmark
-    shape): seeded textured phantoms (5-20 ellipses with a Gaussian-random-field texture), disk
+    """The learned warm start on the learned part's own data at the benchmark shape: seeded textured
+    phantoms (5-20 ellipses with a Gaussian-random-field texture), disk
     attenuation with mu in [0, 0.02] and emitted mu = 0.7 incident mu, Poisson data at 1e4 peak
     counts, held-out seeds.  Three paths on the same slices, each step = compute_maps + the solve
     until every slice reaches the KL residual plain MLEM reaches after 200 iterations: plain MLEM,
@@ -642,7 +642,7 @@ def run_learned_leg(a, dev, rank, world, maps, ws, variant, schedule) -> dict:
         "solver": (f"learned start (one ordered-subsets pass over {levels[0]} subsets keeping 10 snapshots, the "
                    f"encoder-decoder, one pass over {levels[0]} and one over {levels[1]} subsets), then MLEM to the "
                    "plain residual"),
-        "data": (f"config 4 slices at {n}x{n}x{A}: {S} held-out seeds, textured phantoms, mu in [0, 0.02], "
+        "data": (f"textured slices at {n}x{n}x{A}: {S} held-out seeds, textured phantoms, mu in [0, 0.02], "
                  f"emitted mu 0.7 incident, Poisson {a.learned_peak:g} peak counts"),
         "same_data": {"plain": out["plain"], "subsets": dict(out["subsets"], schedule=[(levels[0], 2), (levels[1], 1)])},
         "learned_over_plain": out["learned"]["value"] / out["plain"]["value"],
@@ -787,7 +787,7 @@ def extra_legs(a, dev, c, maps, mus_h, xs_h, b, tol_np, max_iters, variant) -> d
 
 
 def run_waves(a):
-    """Config 2 as stated: --wave-slices independent 512x512 slices over 720 angles, plain MLEM for
+    """Independent slices in HBM-sized waves: --wave-slices independent 512x512 slices over 720 angles, plain MLEM for
     200 iterations with all slices of a wave in one launch per operator and each block of
     iterations in a CUDA graph; waves sized to HBM; FP32 and BF16 maps.  Data synthesis is
     untimed; each wave's timed work is compute_maps + 200 MLEM iterations."""
@@ -840,14 +840,14 @@ def run_waves(a):
         torch.cuda.empty_cache()
     line = {"metric": f"plain MLEM slices/s, {a.wave_slices} slices of {n}x{n}x{A} in HBM-sized waves",
             "value": out["float32"]["slices_per_s"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
-            "config": {"workload": "config 2: independent slices, 200 MLEM iterations, FP32 vs BF16 maps",
+            "config": {"workload": "independent 512x512x720 slices in HBM-sized waves, 200 MLEM iterations, FP32 vs BF16 maps",
                        "iterations": a.iters}, "float32": out["float32"], "bfloat16": out["bfloat16"],
             "data": "synthetic", "dtype": "f32"}
     print(json.dumps(line), flush=True)
 
 
 def run_channels(a):
-    """Config 3: fluorescence channels c = 0..7 whose emitted attenuation is s_c times the incident
+    """Fluorescence channels c = 0..7 whose emitted attenuation is s_c times the incident
     one (s_c in {0.5, 0.75, 1, 1.25, 1.5, 2, 2.5, 3}), 1024 x 1024 slices over 1440 angles, Poisson
     data at 1e4 peak counts, PDHG with the KL data term and isotropic TV (lambda 1e-2) for 300
     iterations.  The maps are line-integral fields (L_in and L_out: two planes per angle and
@@ -932,7 +932,7 @@ def run_channels(a):
         "metric": "slices x channels per s, PDHG-KL-TV 300 iterations, 1024x1024x1440, 8 channels",
         "value": S / secs, "unit": "slice-channels/s", "n_gpus": 1, "higher_is_better": True,
         "ms_per_step": secs * 1e3, "dtype": "f32", "data": "synthetic (seeded ellipse phantoms, disk attenuation)",
-        "config": {"workload": f"config 3: {F} field slice(s) x {C} channels per wave (the full 64 field slices run as "
+        "config": {"workload": f"{F} field slice(s) x {C} channels per wave (the full 64 field slices run as "
                                f"{-(-64 // F)} waves)", "n": n, "angles": A, "channel_scales": scales.tolist(),
                    "iterations": iters, "tv_lambda": 1e-2, "maps": "line-integral fields, 2 planes per angle"},
         "fp_roofline": {"fp_launch_us": fp_s * 1e6, "algorithmic_bytes": map_once + per_channel,

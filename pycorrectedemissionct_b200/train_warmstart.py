@@ -221,7 +221,7 @@ def warm_started_solve(net: WarmStartNet, c: core.XrfCore, maps: torch.Tensor, b
 
 def evaluate(net: WarmStartNet, n: int, n_angles: int, n_slices: int, seed: int, batch: int = 32, device=None,
              plain_iterations: int = 200) -> dict:
-    """Held-out evaluation on config-4-style slices: per slice, the full-data passes that plain
+    """Held-out evaluation on textured slices (mu up to 0.02, 1e4 peak counts): per slice, the full-data passes that plain
     MLEM (cold start), the learned start + MLEM, and the same passes without the network need to
     reach the KL residual plain MLEM reaches after ``plain_iterations`` iterations."""
     device = core.require_cuda(device)

@@ -3,7 +3,7 @@
 1. The training path end to end at a small size: pairs from the GPU MLEM, a few hundred steps with
    the project's tensor-core kernels, and the learned start + MLEM reaching the plain solver's
    final KL residual on held-out seeds (the plain solver judges every slice).
-2. What the committed network gains: on held-out config-4 slices (textured phantoms, mu up to 0.02,
+2. What the committed network gains: on held-out textured slices (textured phantoms, mu up to 0.02,
    1e4 peak counts, 256 x 256 over 360 angles), the learned start (a snapshot ordered-subsets pass,
    the network, one pass per ordered-subsets level) followed by MLEM needs at most half the
    full-data passes of plain MLEM to reach plain MLEM's 200-iteration KL residual, and fewer than
@@ -76,7 +76,7 @@ def test_committed_network_gains_over_the_method_without_it(cuda):
 
 
 def test_committed_network_warm_starts_pdhg(cuda):
-    """The learned start as PDHG's x0 (corrct's hook): on held-out config-4 slices (256 x 256, 360
+    """The learned start as PDHG's x0 (corrct's hook): on held-out textured slices (256 x 256, 360
     angles), PDHG-KL-TV from the learned start reaches the data residual that plain PDHG (zero
     start) reaches after 200 iterations in at most half the full-data passes."""
     if not os.path.exists(WEIGHTS):
